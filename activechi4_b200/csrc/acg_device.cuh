@@ -1,0 +1,188 @@
+// Device-side data layout, constants and helpers of the activechi4 B200 engine.
+//
+// Layout in HBM (all systems of a batch concatenated; one system = batch of 1):
+//   particle slots  [poff_r, poff_r + n_r) per system r, poff_r a multiple of 32.
+//     Between rebuilds the slots are in cell order (counting sort by cell,
+//     ascending original index inside a cell), so neighbour gathers hit L1/L2.
+//     pos  : double4 {x, y, z, type}   reduced coordinates in [0,1) + type as a
+//            double, 32 B aligned -> one sector per neighbour gather
+//     ux/uy/uz, vx/vy/vz, fx/fy/fz, ox/oy/oz : FP64 SoA (unfolded position,
+//            momentum, force, unfolded position at the last rebuild)
+//     id   : original particle index inside its system
+//     act  : -1 or index into the system's direction array
+//     cellof: cell of the slot at the last rebuild
+//     nbn / nbl : full neighbour list, row-major, `maxnb` entries per slot
+//   cells           [coff_r, coff_r + ncell_r): cstart (slot offset inside the
+//                   system), ccount
+//   directions      [aoff_r, aoff_r + nact_r): char4 {kx, ky, kz, 0}
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace acg {
+
+constexpr int NHC_M = 3;
+constexpr int BLOCK_A = 256;    // kick+drift: one thread per particle
+constexpr int BLOCK_L = 256;    // list build: one warp per particle
+constexpr int PART_L = BLOCK_L / 32;
+constexpr int BLOCK_R = 256;    // per-slot rebuild kernels (tiles of BLOCK_A)
+constexpr int CELLS_PER_TILE = 8;
+constexpr int BLOCK_SCAN = 512;
+
+// KA pair constants (MDcode/cell_list+forces.c:19-20, MDcode/global.h:26,39-40)
+constexpr double KA_C0 = 0.0162665594880;
+constexpr double KA_C2 = -0.001949973872640;
+constexpr double KA_RC2 = 6.25;  // (r/sigma)^2 cut
+
+struct SysDesc {
+  int n, nact, poff, aoff;
+  int coff, ncell, nc, pad0;
+  int tile0_b, ntile_b, tau_p, thermostat;
+  int shuffle, list_mode, precision, pad1;
+  double L, invL, inv_cell;  // inv_cell: cells per unit reduced length (InvCellSize)
+  double T, f0, dt, half_dt, skin2, rebuild_factor, dof;
+  double q[NHC_M];
+  double lcut2[3];           // list cut^2 (absolute units) for type sums 0 (AA), 1 (AB), 2 (BB)
+  unsigned long long seed;
+};
+
+struct SysState {
+  double eta_end[NHC_M], p_eta_end[NHC_M];  // chain at the step boundary
+  double eta_cur[NHC_M], p_eta_cur[NHC_M];  // chain after the next step's first half
+  double s1, s2;             // pending velocity scales (next first-half, last second-half)
+  double ke_end;             // 0.5 sum p^2 at the boundary
+  double pe, virial, vir_act;
+  double maxD_last;
+  unsigned long long maxd_bits;  // running max of |xu - xold|^2 (as bits) for this step
+  long long step;
+  long long rebuilds;
+  int rebuild;               // rebuild this step
+  int force_rebuild;         // host request
+  int prime;                 // host request: recompute forces + thermostat pre-half
+  int status;                // 1 = non-finite kinetic energy seen
+  unsigned int counter_b;    // last-block counter of the force kernel
+  int overflow;
+};
+
+struct View {
+  const SysDesc *desc;
+  SysState *st;
+  double4 *pos;
+  double *ux, *uy, *uz, *vx, *vy, *vz, *fx, *fy, *fz, *ox, *oy, *oz;
+  int *id, *act, *cellof, *nbn, *nbl;
+  char4 *kdir;
+  double4 *pos_s;
+  double *ux_s, *uy_s, *uz_s, *vx_s, *vy_s, *vz_s, *fx_s, *fy_s, *fz_s;
+  int *id_s, *act_s;
+  int *cell_tmp, *perm_u, *perm;
+  int *ccount_b, *cfill, *cstart, *ccount;
+  const int2 *tiles_a, *tiles_b, *tiles_l, *tiles_c;
+  double4 *part_b;
+  unsigned int *counter_a;
+  double *stage_d;  // [9n] x, xu, p interleaved per system (original order)
+  int *stage_i;     // [2n] type, act
+  double *stage_f;  // [3n] forces
+  int ntiles_a, ntiles_b, ntiles_l, ntiles_c, nsys, maxnb;
+};
+
+// minimum image in reduced units, as MDcode/cell_list+forces.c:177-182
+__device__ __forceinline__ double min_image(double d) {
+  if (d < -0.5) d += 1.0;
+  if (d > 0.5) d -= 1.0;
+  return d;
+}
+
+// applypbc1 (MDcode/time_evolve.c:15-26) for a displacement far below one box:
+// the while loops run at most once.  A coordinate still outside [0,1) (only
+// possible for non-finite or absurd velocities) is folded with floor so that
+// no loop can run unbounded.
+__device__ __forceinline__ double wrap_unit(double x) {
+  if (x >= 1.0) {
+    x = __dadd_rn(x, -1.0);
+    if (x >= 1.0) x = x - floor(x);
+  } else if (x < 0.0) {
+    x = __dadd_rn(x, 1.0);
+    if (x < 0.0) x = x - floor(x);
+  }
+  return x;
+}
+
+__device__ __forceinline__ int cell_coord(double x, double inv, int nc) {
+  double f = floor(__dmul_rn(x, inv));
+  int c = (int)f;  // NaN converts to 0
+  c = c < 0 ? 0 : c;
+  return c >= nc ? nc - 1 : c;
+}
+
+// per-dimension neighbour-cell offsets without repeats: {-1,0,1} when there
+// are >= 3 cells on a side, {0,1} for 2, {0} for 1
+__device__ __forceinline__ int stencil_lo(int nc) { return nc >= 3 ? -1 : 0; }
+__device__ __forceinline__ int stencil_hi(int nc) { return nc >= 2 ? 1 : 0; }
+__device__ __forceinline__ int wrap_cell(int c, int nc) {
+  c += nc;
+  return c >= nc ? (c >= 2 * nc ? c - 2 * nc : c - nc) : c;
+}
+
+// U4Propagator (MDcode/time_evolve.c:578-609): one chain sweep jStart..jEnd,
+// `ksum` = sum p^2 for the j == 0 link.
+__device__ inline void nhc_u4(double *p_eta, const double *q, double T, double dof, double t,
+                              int j0, int j1, double ksum) {
+  int dj = j0 > j1 ? -1 : 1;
+  int j = j0;
+  double gj;
+  do {
+    if (j == 0)
+      gj = ksum - dof * T;
+    else
+      gj = (p_eta[j - 1] * p_eta[j - 1]) / q[j - 1] - T;
+    if (j == NHC_M - 1) {
+      p_eta[j] = p_eta[j] + t * gj;
+    } else {
+      double x = t * p_eta[j + 1] / q[j + 1];
+      double e = exp(-x);
+      p_eta[j] = p_eta[j] * e + t * gj * (1.0 - e) / x;
+    }
+    j += dj;
+  } while (j - dj != j1);
+}
+
+// U4(t/2..) U3 U4 half of the NHC Trotter split (MDcode/time_evolve.c:499-501)
+// applied to chain (eta, p_eta) with sum p^2 = ksum; returns the velocity
+// scale of U3.
+__device__ inline double nhc_half(double *eta, double *p_eta, const double *q, double T,
+                                  double dof, double dt, double ksum) {
+  const double t4 = dt * 0.25, t3 = dt * 0.50;
+  nhc_u4(p_eta, q, T, dof, t4, NHC_M - 1, 0, ksum);
+  double s = exp(-t3 * p_eta[0] / q[0]);
+  for (int i = 0; i < NHC_M; i++) eta[i] = eta[i] + t3 * p_eta[i] / q[i];
+  double s2k = (s * s) * ksum;
+  nhc_u4(p_eta, q, T, dof, t4, 0, NHC_M - 1, s2k);
+  return s;
+}
+
+// keyed bijection of 32-bit integers (4-round Feistel network): distinct
+// inputs give distinct keys, which makes rank-by-key an exact permutation
+__device__ __forceinline__ uint32_t feistel32(uint32_t v, uint64_t key) {
+  uint32_t L = v >> 16, R = v & 0xffffu;
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    uint32_t k = (uint32_t)(key >> (16 * r)) * 0x9E3779B1u + (uint32_t)r * 0x7F4A7C15u;
+    uint32_t f = (R ^ k) * 0x85EBCA6Bu;
+    f ^= f >> 13;
+    f *= 0xC2B2AE35u;
+    f ^= f >> 16;
+    uint32_t nl = R, nr = (L ^ f) & 0xffffu;
+    L = nl;
+    R = nr;
+  }
+  return (L << 16) | R;
+}
+
+__device__ __forceinline__ uint64_t splitmix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+}  // namespace acg

@@ -1,0 +1,899 @@
+// Host side of the activechi4 B200 engine: device memory arena, tiling,
+// CUDA-graph construction (with a device-decided conditional for the list
+// rebuild) and the C ABI declared in include/activechi4.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/activechi4.h"
+#include "acg_kernels.cuh"
+
+using namespace acg;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CK(call)                                                                              \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess)                                                                    \
+      return fail(ACG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));         \
+  } while (0)
+
+constexpr double TAU_T = 0.20;  // MDcode/time_evolve.c:477
+constexpr int GRAPH_STEPS = 32;
+
+struct Layout {
+  int nsys = 0, nslots = 0, ncells = 0, nact = 0, maxnb = 0;
+  std::vector<SysDesc> desc;
+  size_t bytes = 0;
+};
+
+double sigma_of(int tsum) { return tsum == 0 ? 1.00 : (tsum == 1 ? 0.80 : 0.88); }
+
+int resolve(const acg_params &p, SysDesc &d) {
+  if (p.n < 2) return fail(ACG_ERR_INVALID, "n must be >= 2");
+  memset(&d, 0, sizeof(d));
+  d.n = p.n;
+  d.nact = p.nact < 0 ? (int)((double)p.n * 0.1) : p.nact;
+  if (d.nact > d.n) return fail(ACG_ERR_INVALID, "nact > n");
+  double L = p.L > 0 ? p.L : std::pow((double)p.n / p.density, 0.33333333);
+  if (!(L > 0) || !std::isfinite(L)) return fail(ACG_ERR_INVALID, "bad box length");
+  const double cell_cut = 2.5 * 1.00 + p.skin;  // Cell_cut (MDcode/global.h:29)
+  // Ncell = (int)Lpp / Cell_cut with the cast on Lpp (MDcode/Parallel.c:72)
+  int nc = (int)((double)(int)L / cell_cut);
+  if (nc < 2)
+    return fail(ACG_ERR_INVALID, "box too small: need at least 2 cells of size >= 2.5+skin per side");
+  double cs = L / (double)nc;
+  d.nc = nc;
+  d.ncell = nc * nc * nc;
+  d.L = L;
+  d.invL = 1.0 / L;
+  d.inv_cell = L / cs;  // InvCellSize (MDcode/Parallel.c:78)
+  d.T = p.T;
+  d.f0 = p.f0;
+  d.dt = p.dt;
+  d.half_dt = p.dt * 0.5;
+  d.skin2 = p.skin * p.skin;
+  d.rebuild_factor = p.rebuild_factor;
+  d.dof = 3.0 * (double)p.n - 3.0;  // DOF (MDcode/global.h:35)
+  for (int i = 0; i < NHC_M; i++) d.q[i] = p.T * TAU_T * TAU_T;
+  d.q[0] = d.dof * p.T * TAU_T * TAU_T;
+  for (int t = 0; t < 3; t++) {
+    double rl = p.list_mode == 0 ? cell_cut : 2.5 * sigma_of(t) + p.skin;
+    d.lcut2[t] = rl * rl;
+  }
+  d.tau_p = p.tau_p_steps;
+  d.thermostat = p.thermostat ? 1 : 0;
+  d.shuffle = p.shuffle ? 1 : 0;
+  d.list_mode = p.list_mode;
+  d.precision = p.precision;
+  d.seed = p.seed;
+  if (p.dt <= 0 || p.skin <= 0 || p.rebuild_factor <= 0)
+    return fail(ACG_ERR_INVALID, "dt, skin and rebuild_factor must be positive");
+  if (p.thermostat && !(p.T > 0)) return fail(ACG_ERR_INVALID, "thermostat needs T > 0");
+  if (p.shuffle && p.tau_p_steps <= 0) return fail(ACG_ERR_INVALID, "shuffle needs tau_p_steps > 0");
+  return ACG_OK;
+}
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+int plan(const acg_params *params, int nsys, Layout &lay) {
+  if (!params || nsys < 1) return fail(ACG_ERR_INVALID, "need at least one system");
+  lay = Layout();
+  lay.nsys = nsys;
+  lay.desc.resize(nsys);
+  double dens_max = 0;
+  for (int r = 0; r < nsys; r++) {
+    int rc = resolve(params[r], lay.desc[r]);
+    if (rc) return fail(rc, "system " + std::to_string(r) + ": " + g_err);
+    if (params[r].precision != params[0].precision)
+      return fail(ACG_ERR_INVALID, "all systems of an engine share one precision");
+    SysDesc &d = lay.desc[r];
+    d.poff = lay.nslots;
+    d.coff = lay.ncells;
+    d.aoff = lay.nact;
+    lay.nslots += (int)align_up((size_t)d.n, 32);
+    lay.ncells += d.ncell;
+    lay.nact += d.nact;
+    dens_max = std::max(dens_max, (double)d.n / (d.L * d.L * d.L));
+  }
+  // neighbour-row capacity: 1.45x the ideal-gas count within the widest list
+  // cut plus margin; rare denser particles fall back to the cell scan
+  const double rl = 2.5 + params[0].skin;
+  double expect = dens_max * 4.0 / 3.0 * M_PI * rl * rl * rl;
+  lay.maxnb = (int)align_up((size_t)(1.45 * expect + 16.0), 32);
+  lay.maxnb = std::max(lay.maxnb, 64);
+  if (params[0].nb_capacity > 0) lay.maxnb = (int)align_up((size_t)params[0].nb_capacity, 32);
+  const size_t S = (size_t)lay.nslots, Cn = (size_t)lay.ncells;
+  size_t b = 0;
+  auto add = [&](size_t n) { b += align_up(n, 256); };
+  add(sizeof(SysDesc) * nsys);
+  add(sizeof(SysState) * nsys);
+  add(32 * S);                    // pos
+  for (int k = 0; k < 12; k++) add(8 * S);
+  for (int k = 0; k < 4; k++) add(4 * S);  // id act cellof nbn
+  add(4 * S * (size_t)lay.maxnb); // nbl
+  add(4 * (size_t)std::max(lay.nact, 1));
+  add(32 * S);                    // pos_s
+  for (int k = 0; k < 9; k++) add(8 * S);
+  for (int k = 0; k < 5; k++) add(4 * S);  // id_s act_s cell_tmp perm_u perm
+  for (int k = 0; k < 4; k++) add(4 * Cn);
+  add(8 * (S / BLOCK_A + nsys + 1));      // tiles_a
+  add(8 * (S / 4 + nsys + 1));            // tiles_b (>= 4 particles per block)
+  add(8 * (S / PART_L + nsys + 1));       // tiles_l
+  add(8 * (Cn / CELLS_PER_TILE + nsys + 1));
+  add(32 * (S / 4 + nsys + 1));           // part_b
+  add(64);                                // counters
+  add(72 * S);                            // stage_d
+  add(8 * S);                             // stage_i
+  add(24 * S);                            // stage_f
+  lay.bytes = b;
+  return ACG_OK;
+}
+
+}  // namespace
+
+struct acg_engine {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  Layout lay;
+  void *arena = nullptr;
+  View v{};
+  SysDesc *d_desc = nullptr;
+  int tpp = 4, block = 128;
+  int ntiles_a = 0, ntiles_b = 0, ntiles_l = 0, ntiles_c = 0;
+  int2 *d_tiles_b = nullptr;
+  std::vector<int> dirty;  // systems whose forces/lists must be recomputed
+  bool any_dirty = false;
+  cudaGraphExec_t gexec = nullptr;
+  cudaGraph_t graph = nullptr;
+  int gsteps = 0;
+  cudaGraphExec_t gexec1 = nullptr;
+  cudaGraph_t graph1 = nullptr;
+  void *flush = nullptr;  // bench-only L2 flush buffer
+  size_t flush_bytes = 0;
+};
+
+namespace {
+
+using ForceFn = void (*)(View, int);
+
+ForceFn force_fn(int tpp, int prec) {
+#define F(T)                                                                     \
+  case T:                                                                        \
+    return prec ? (ForceFn)k_force_kick<T, 1> : (ForceFn)k_force_kick<T, 0>;
+  switch (tpp) {
+    F(1) F(2) F(4) F(8) F(16) F(32)
+  }
+#undef F
+  return nullptr;
+}
+
+int build_tiles_b(acg_engine *e) {
+  const int pb = e->block / e->tpp;
+  std::vector<int2> tb;
+  for (int r = 0; r < e->lay.nsys; r++) {
+    SysDesc &d = e->lay.desc[r];
+    d.tile0_b = (int)tb.size();
+    for (int s = 0; s < d.n; s += pb) tb.push_back(make_int2(r, s));
+    d.ntile_b = (int)tb.size() - d.tile0_b;
+  }
+  e->ntiles_b = (int)tb.size();
+  const size_t cap = e->lay.nslots / 4 + e->lay.nsys + 1;
+  if (tb.size() > cap) return fail(ACG_ERR_INVALID, "launch shape needs >= 4 particles per block");
+  CK(cudaMemcpyAsync(e->d_tiles_b, tb.data(), tb.size() * sizeof(int2), cudaMemcpyHostToDevice,
+                     e->stream));
+  CK(cudaMemcpyAsync(e->d_desc, e->lay.desc.data(), sizeof(SysDesc) * e->lay.nsys,
+                     cudaMemcpyHostToDevice, e->stream));
+  e->v.ntiles_b = e->ntiles_b;
+  return ACG_OK;
+}
+
+void drop_graphs(acg_engine *e) {
+  if (e->gexec) cudaGraphExecDestroy(e->gexec);
+  if (e->graph) cudaGraphDestroy(e->graph);
+  if (e->gexec1) cudaGraphExecDestroy(e->gexec1);
+  if (e->graph1) cudaGraphDestroy(e->graph1);
+  e->gexec = e->gexec1 = nullptr;
+  e->graph = e->graph1 = nullptr;
+  e->gsteps = 0;
+}
+
+// ---- launches --------------------------------------------------------------
+int launch_rebuild(acg_engine *e) {
+  View v = e->v;
+  cudaStream_t s = e->stream;
+  k_cells_count<<<e->ntiles_a, BLOCK_R, 0, s>>>(v);
+  k_cells_scan<<<e->lay.nsys, BLOCK_SCAN, 0, s>>>(v);
+  k_cells_scatter<<<e->ntiles_a, BLOCK_R, 0, s>>>(v);
+  k_cells_order<<<e->ntiles_c, 32 * CELLS_PER_TILE, 0, s>>>(v);
+  k_permute<<<e->ntiles_a, BLOCK_R, 0, s>>>(v);
+  k_build_list<<<e->ntiles_l, BLOCK_L, 0, s>>>(v);
+  CK(cudaGetLastError());
+  return ACG_OK;
+}
+
+int launch_force(acg_engine *e, int mode) {
+  ForceFn f = force_fn(e->tpp, e->lay.desc[0].precision);
+  f<<<e->ntiles_b, e->block, 0, e->stream>>>(e->v, mode);
+  CK(cudaGetLastError());
+  return ACG_OK;
+}
+
+int launch_step_eager(acg_engine *e) {
+  k_kick_drift<<<e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, 0, e->stream>>>(e->v, 0, 0);
+  CK(cudaGetLastError());
+  int rc = launch_rebuild(e);
+  if (rc) return rc;
+  return launch_force(e, 0);
+}
+
+// forces (and lists) for every system flagged dirty
+int prime(acg_engine *e) {
+  if (!e->any_dirty) return ACG_OK;
+  for (int r = 0; r < e->lay.nsys; r++) {
+    if (!e->dirty[r]) continue;
+    int one = 1;
+    CK(cudaMemcpyAsync(&e->v.st[r].prime, &one, sizeof(int), cudaMemcpyHostToDevice, e->stream));
+    e->dirty[r] = 0;
+  }
+  k_flag_rebuild<<<1, 256, 0, e->stream>>>(e->v, 0);
+  CK(cudaGetLastError());
+  int rc = launch_rebuild(e);
+  if (rc) return rc;
+  rc = launch_force(e, 1);
+  if (rc) return rc;
+  e->any_dirty = false;
+  return ACG_OK;
+}
+
+// ---- graphs ----------------------------------------------------------------
+int add_kernel(cudaGraph_t g, const cudaGraphNode_t *dep, size_t ndep, cudaGraphNode_t *out,
+               void *fn, int grid, int block, void **args) {
+  cudaKernelNodeParams p = {};
+  p.func = fn;
+  p.gridDim = dim3(grid);
+  p.blockDim = dim3(block);
+  p.sharedMemBytes = 0;
+  p.kernelParams = args;
+  CK(cudaGraphAddKernelNode(out, g, dep, ndep, &p));
+  return ACG_OK;
+}
+
+int build_graph(acg_engine *e, int K, cudaGraph_t *gout, cudaGraphExec_t *xout) {
+  cudaGraph_t g;
+  CK(cudaGraphCreate(&g, 0));
+  View v = e->v;
+  ForceFn ff = force_fn(e->tpp, e->lay.desc[0].precision);
+  cudaGraphNode_t prev = nullptr;
+  int mode0 = 0, use_cond = 1;
+  for (int s = 0; s < K; s++) {
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+    cudaGraphNode_t na, nc, nb;
+    void *aa[] = {&v, &use_cond, &h};
+    int rc = add_kernel(g, prev ? &prev : nullptr, prev ? 1 : 0, &na, (void *)k_kick_drift,
+                        e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, aa);
+    if (rc) return rc;
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    CK(cudaGraphAddNode(&nc, g, &na, 1, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    void *va[] = {&v};
+    struct {
+      void *fn;
+      int grid, block;
+    } rb[] = {{(void *)k_cells_count, e->ntiles_a, BLOCK_R},
+              {(void *)k_cells_scan, e->lay.nsys, BLOCK_SCAN},
+              {(void *)k_cells_scatter, e->ntiles_a, BLOCK_R},
+              {(void *)k_cells_order, e->ntiles_c, 32 * CELLS_PER_TILE},
+              {(void *)k_permute, e->ntiles_a, BLOCK_R},
+              {(void *)k_build_list, e->ntiles_l, BLOCK_L}};
+    cudaGraphNode_t bp = nullptr;
+    for (auto &k : rb) {
+      cudaGraphNode_t nn;
+      rc = add_kernel(body, bp ? &bp : nullptr, bp ? 1 : 0, &nn, k.fn, k.grid, k.block, va);
+      if (rc) return rc;
+      bp = nn;
+    }
+    void *ba[] = {&v, &mode0};
+    rc = add_kernel(g, &nc, 1, &nb, (void *)ff, e->ntiles_b, e->block, ba);
+    if (rc) return rc;
+    prev = nb;
+  }
+  cudaGraphExec_t x;
+  CK(cudaGraphInstantiate(&x, g, 0));
+  *gout = g;
+  *xout = x;
+  return ACG_OK;
+}
+
+int check_sys(acg_engine *e, int sys) {
+  if (!e) return fail(ACG_ERR_INVALID, "null engine");
+  if (sys < 0 || sys >= e->lay.nsys) return fail(ACG_ERR_INVALID, "system index out of range");
+  return ACG_OK;
+}
+
+}  // namespace
+
+// ============================================================================
+extern "C" {
+
+const char *acg_last_error(void) { return g_err.c_str(); }
+const char *acg_version(void) { return "activechi4-b200 0.1 (sm_100a)"; }
+
+int acg_params_default(acg_params *p, int n) {
+  if (!p) return fail(ACG_ERR_INVALID, "null params");
+  memset(p, 0, sizeof(*p));
+  p->n = n;
+  p->nact = -1;
+  p->L = 0.0;
+  p->density = 1.2;
+  p->T = 0.45;
+  p->f0 = 1.0;
+  p->tau_p_steps = 200;     // TAU_per (MDcode/global.h:58)
+  p->dt = 0.005;            // time_step (MDcode/global.h:32)
+  p->skin = 0.35 * 1.00;    // skin (MDcode/global.h:28)
+  p->rebuild_factor = 3.0;  // MDcode/time_evolve.c:508
+  p->list_mode = 0;
+  p->thermostat = 1;
+  p->shuffle = 1;
+  p->precision = ACG_PREC_FP64;
+  p->seed = 12345;
+  return ACG_OK;
+}
+
+int acg_footprint(const acg_params *params, int nsys, size_t *bytes) {
+  Layout lay;
+  int rc = plan(params, nsys, lay);
+  if (rc) return rc;
+  if (bytes) *bytes = lay.bytes;
+  return ACG_OK;
+}
+
+int acg_create(const acg_params *params, int nsys, int device, acg_engine **out) {
+  if (!out) return fail(ACG_ERR_INVALID, "null out");
+  *out = nullptr;
+  acg_engine *e = new acg_engine();
+  int rc = plan(params, nsys, e->lay);
+  if (rc) {
+    delete e;
+    return rc;
+  }
+  e->device = device;
+  cudaError_t ce = cudaSetDevice(device);
+  if (ce != cudaSuccess) {
+    delete e;
+    return fail(ACG_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(ce));
+  }
+  ce = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+  if (ce == cudaSuccess) ce = cudaMalloc(&e->arena, e->lay.bytes);
+  if (ce != cudaSuccess) {
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+    return fail(ce == cudaErrorMemoryAllocation ? ACG_ERR_NOMEM : ACG_ERR_CUDA,
+                std::string("device allocation: ") + cudaGetErrorString(ce));
+  }
+  const Layout &L = e->lay;
+  const size_t S = L.nslots, Cn = L.ncells;
+  char *p = (char *)e->arena;
+  auto take = [&](size_t n) {
+    void *q = p;
+    p += align_up(n, 256);
+    return q;
+  };
+  View &v = e->v;
+  e->d_desc = (SysDesc *)take(sizeof(SysDesc) * nsys);
+  v.desc = e->d_desc;
+  v.st = (SysState *)take(sizeof(SysState) * nsys);
+  v.pos = (double4 *)take(32 * S);
+  double **dd[] = {&v.ux, &v.uy, &v.uz, &v.vx, &v.vy, &v.vz, &v.fx, &v.fy, &v.fz, &v.ox, &v.oy, &v.oz};
+  for (auto q : dd) *q = (double *)take(8 * S);
+  v.id = (int *)take(4 * S);
+  v.act = (int *)take(4 * S);
+  v.cellof = (int *)take(4 * S);
+  v.nbn = (int *)take(4 * S);
+  v.nbl = (int *)take(4 * S * (size_t)L.maxnb);
+  v.kdir = (char4 *)take(4 * (size_t)std::max(L.nact, 1));
+  v.pos_s = (double4 *)take(32 * S);
+  double **ds[] = {&v.ux_s, &v.uy_s, &v.uz_s, &v.vx_s, &v.vy_s, &v.vz_s, &v.fx_s, &v.fy_s, &v.fz_s};
+  for (auto q : ds) *q = (double *)take(8 * S);
+  v.id_s = (int *)take(4 * S);
+  v.act_s = (int *)take(4 * S);
+  v.cell_tmp = (int *)take(4 * S);
+  v.perm_u = (int *)take(4 * S);
+  v.perm = (int *)take(4 * S);
+  v.ccount_b = (int *)take(4 * Cn);
+  v.cfill = (int *)take(4 * Cn);
+  v.cstart = (int *)take(4 * Cn);
+  v.ccount = (int *)take(4 * Cn);
+  int2 *ta = (int2 *)take(8 * (S / BLOCK_A + nsys + 1));
+  e->d_tiles_b = (int2 *)take(8 * (S / 4 + nsys + 1));
+  int2 *tl = (int2 *)take(8 * (S / PART_L + nsys + 1));
+  int2 *tc = (int2 *)take(8 * (Cn / CELLS_PER_TILE + nsys + 1));
+  v.part_b = (double4 *)take(32 * (S / 4 + nsys + 1));
+  v.counter_a = (unsigned int *)take(64);
+  v.stage_d = (double *)take(72 * S);
+  v.stage_i = (int *)take(8 * S);
+  v.stage_f = (double *)take(24 * S);
+  v.tiles_a = ta;
+  v.tiles_b = e->d_tiles_b;
+  v.tiles_l = tl;
+  v.tiles_c = tc;
+  v.nsys = nsys;
+  v.maxnb = L.maxnb;
+
+  std::vector<int2> h_a, h_l, h_c;
+  for (int r = 0; r < nsys; r++) {
+    const SysDesc &d = L.desc[r];
+    for (int s = 0; s < d.n; s += BLOCK_A) h_a.push_back(make_int2(r, s));
+    for (int s = 0; s < d.n; s += PART_L) h_l.push_back(make_int2(r, s));
+    for (int s = 0; s < d.ncell; s += CELLS_PER_TILE) h_c.push_back(make_int2(r, s));
+  }
+  e->ntiles_a = (int)h_a.size();
+  e->ntiles_l = (int)h_l.size();
+  e->ntiles_c = (int)h_c.size();
+  v.ntiles_a = e->ntiles_a;
+  v.ntiles_l = e->ntiles_l;
+  v.ntiles_c = e->ntiles_c;
+  auto cleanup_fail = [&](int code) {
+    acg_destroy(e);
+    return code;
+  };
+  if (cudaMemsetAsync(e->arena, 0, L.bytes, e->stream) != cudaSuccess ||
+      cudaMemcpyAsync(ta, h_a.data(), h_a.size() * sizeof(int2), cudaMemcpyHostToDevice, e->stream) !=
+          cudaSuccess ||
+      cudaMemcpyAsync(tl, h_l.data(), h_l.size() * sizeof(int2), cudaMemcpyHostToDevice, e->stream) !=
+          cudaSuccess ||
+      cudaMemcpyAsync(tc, h_c.data(), h_c.size() * sizeof(int2), cudaMemcpyHostToDevice, e->stream) !=
+          cudaSuccess)
+    return cleanup_fail(fail(ACG_ERR_CUDA, "initial upload failed"));
+  std::vector<SysState> st(nsys);
+  memset(st.data(), 0, sizeof(SysState) * nsys);
+  for (auto &s : st) {
+    s.s1 = s.s2 = 1.0;
+  }
+  if (cudaMemcpyAsync(v.st, st.data(), sizeof(SysState) * nsys, cudaMemcpyHostToDevice, e->stream) !=
+      cudaSuccess)
+    return cleanup_fail(fail(ACG_ERR_CUDA, "state upload failed"));
+  rc = build_tiles_b(e);
+  if (rc) return cleanup_fail(rc);
+  e->dirty.assign(nsys, 1);
+  e->any_dirty = true;
+  if (cudaStreamSynchronize(e->stream) != cudaSuccess)
+    return cleanup_fail(fail(ACG_ERR_CUDA, "set-up synchronisation failed"));
+  *out = e;
+  return ACG_OK;
+}
+
+int acg_destroy(acg_engine *e) {
+  if (!e) return ACG_OK;
+  cudaSetDevice(e->device);
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  drop_graphs(e);
+  if (e->flush) cudaFree(e->flush);
+  if (e->arena) cudaFree(e->arena);
+  if (e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+  return ACG_OK;
+}
+
+int acg_num_systems(acg_engine *e) { return e ? e->lay.nsys : 0; }
+
+int acg_system_size(acg_engine *e, int sys, int *n, int *nact) {
+  int rc = check_sys(e, sys);
+  if (rc) return rc;
+  if (n) *n = e->lay.desc[sys].n;
+  if (nact) *nact = e->lay.desc[sys].nact;
+  return ACG_OK;
+}
+
+void *acg_stream(acg_engine *e) { return e ? (void *)e->stream : nullptr; }
+
+int acg_set_state(acg_engine *e, int sys, const double *x, const double *xu, const double *p,
+                  const int *type, const int *act_tag) {
+  int rc = check_sys(e, sys);
+  if (rc) return rc;
+  if (!x || !p || !type || !act_tag) return fail(ACG_ERR_INVALID, "x, p, type and act_tag are required");
+  const SysDesc &d = e->lay.desc[sys];
+  const size_t n = d.n;
+  for (size_t i = 0; i < n; i++) {
+    if (type[i] != 0 && type[i] != 1) return fail(ACG_ERR_INVALID, "type must be 0 or 1");
+    if (act_tag[i] < -1 || act_tag[i] >= d.nact) return fail(ACG_ERR_INVALID, "act_tag out of range");
+    for (int c = 0; c < 3; c++)
+      if (!(x[3 * i + c] >= 0.0 && x[3 * i + c] < 1.0))
+        return fail(ACG_ERR_INVALID, "x must be wrapped reduced coordinates in [0,1)");
+  }
+  CK(cudaSetDevice(e->device));
+  double *sd = e->v.stage_d + 9 * (size_t)d.poff;
+  int *si = e->v.stage_i + 2 * (size_t)d.poff;
+  CK(cudaMemcpyAsync(sd, x, 24 * n, cudaMemcpyHostToDevice, e->stream));
+  CK(cudaMemcpyAsync(sd + 3 * n, xu ? xu : x, 24 * n, cudaMemcpyHostToDevice, e->stream));
+  CK(cudaMemcpyAsync(sd + 6 * n, p, 24 * n, cudaMemcpyHostToDevice, e->stream));
+  CK(cudaMemcpyAsync(si, type, 4 * n, cudaMemcpyHostToDevice, e->stream));
+  CK(cudaMemcpyAsync(si + n, act_tag, 4 * n, cudaMemcpyHostToDevice, e->stream));
+  k_load<<<std::max(1, std::min((int)((n + 255) / 256), 1024)), 256, 0, e->stream>>>(e->v, sys);
+  CK(cudaGetLastError());
+  double one = 1.0;
+  CK(cudaMemcpyAsync(&e->v.st[sys].s1, &one, sizeof(double), cudaMemcpyHostToDevice, e->stream));
+  CK(cudaMemcpyAsync(&e->v.st[sys].s2, &one, sizeof(double), cudaMemcpyHostToDevice, e->stream));
+  CK(cudaStreamSynchronize(e->stream));  // host buffers may be freed on return
+  e->dirty[sys] = 1;
+  e->any_dirty = true;
+  return ACG_OK;
+}
+
+int acg_get_state(acg_engine *e, int sys, double *x, double *xu, double *p, double *F) {
+  int rc = check_sys(e, sys);
+  if (rc) return rc;
+  CK(cudaSetDevice(e->device));
+  rc = prime(e);
+  if (rc) return rc;
+  const SysDesc &d = e->lay.desc[sys];
+  const size_t n = d.n;
+  k_unload<<<std::max(1, std::min((int)((n + 255) / 256), 1024)), 256, 0, e->stream>>>(e->v, sys);
+  CK(cudaGetLastError());
+  double *sd = e->v.stage_d + 9 * (size_t)d.poff;
+  double *sf = e->v.stage_f + 3 * (size_t)d.poff;
+  if (x) CK(cudaMemcpyAsync(x, sd, 24 * n, cudaMemcpyDeviceToHost, e->stream));
+  if (xu) CK(cudaMemcpyAsync(xu, sd + 3 * n, 24 * n, cudaMemcpyDeviceToHost, e->stream));
+  if (p) CK(cudaMemcpyAsync(p, sd + 6 * n, 24 * n, cudaMemcpyDeviceToHost, e->stream));
+  if (F) CK(cudaMemcpyAsync(F, sf, 24 * n, cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  return ACG_OK;
+}
+
+int acg_set_directions(acg_engine *e, int sys, const int *k) {
+  int rc = check_sys(e, sys);
+  if (rc) return rc;
+  const SysDesc &d = e->lay.desc[sys];
+  if (d.nact == 0) return ACG_OK;
+  if (!k) return fail(ACG_ERR_INVALID, "null directions");
+  std::vector<char4> h(d.nact);
+  for (int a = 0; a < d.nact; a++) {
+    int kx = k[a], ky = k[d.nact + a], kz = k[2 * d.nact + a];
+    if (std::abs(kx) > 1 || std::abs(ky) > 1 || std::abs(kz) > 1)
+      return fail(ACG_ERR_INVALID, "direction components must be -1, 0 or +1");
+    h[a] = make_char4((signed char)kx, (signed char)ky, (signed char)kz, 0);
+  }
+  CK(cudaSetDevice(e->device));
+  CK(cudaMemcpyAsync(e->v.kdir + d.aoff, h.data(), 4 * (size_t)d.nact, cudaMemcpyHostToDevice, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  return ACG_OK;
+}
+
+int acg_get_directions(acg_engine *e, int sys, int *k) {
+  int rc = check_sys(e, sys);
+  if (rc) return rc;
+  const SysDesc &d = e->lay.desc[sys];
+  if (d.nact == 0) return ACG_OK;
+  std::vector<char4> h(d.nact);
+  CK(cudaSetDevice(e->device));
+  CK(cudaMemcpyAsync(h.data(), e->v.kdir + d.aoff, 4 * (size_t)d.nact, cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  for (int a = 0; a < d.nact; a++) {
+    k[a] = h[a].x;
+    k[d.nact + a] = h[a].y;
+    k[2 * d.nact + a] = h[a].z;
+  }
+  return ACG_OK;
+}
+
+int acg_shuffle_directions(acg_engine *e, int sys) {
+  int rc = check_sys(e, sys);
+  if (rc) return rc;
+  if (e->lay.desc[sys].nact == 0) return ACG_OK;
+  CK(cudaSetDevice(e->device));
+  k_shuffle_now<<<3, 256, 0, e->stream>>>(e->v, sys);
+  CK(cudaGetLastError());
+  return ACG_OK;
+}
+
+int acg_set_nhc(acg_engine *e, int sys, const double *eta3, const double *p_eta3) {
+  int rc = check_sys(e, sys);
+  if (rc) return rc;
+  if (!eta3 || !p_eta3) return fail(ACG_ERR_INVALID, "null chain");
+  CK(cudaSetDevice(e->device));
+  SysState *s = e->v.st + sys;
+  CK(cudaMemcpyAsync(s->eta_end, eta3, 3 * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+  CK(cudaMemcpyAsync(s->p_eta_end, p_eta3, 3 * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+  if (e->dirty[sys]) {
+    // the prime pass computes the first half once forces and KE are known
+    CK(cudaStreamSynchronize(e->stream));
+    return ACG_OK;
+  }
+  k_prehalf<<<1, 1, 0, e->stream>>>(e->v, sys);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(e->stream));
+  return ACG_OK;
+}
+
+int acg_set_temperature(acg_engine *e, int sys, double T) {
+  int rc = check_sys(e, sys);
+  if (rc) return rc;
+  if (!(T > 0)) return fail(ACG_ERR_INVALID, "T must be positive");
+  SysDesc &d = e->lay.desc[sys];
+  d.T = T;
+  for (int i = 0; i < NHC_M; i++) d.q[i] = T * TAU_T * TAU_T;
+  d.q[0] = d.dof * T * TAU_T * TAU_T;
+  CK(cudaSetDevice(e->device));
+  CK(cudaMemcpyAsync(e->d_desc + sys, &d, sizeof(SysDesc), cudaMemcpyHostToDevice, e->stream));
+  if (!e->dirty[sys]) k_prehalf<<<1, 1, 0, e->stream>>>(e->v, sys);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(e->stream));
+  return ACG_OK;
+}
+
+int acg_rebuild(acg_engine *e) {
+  if (!e) return fail(ACG_ERR_INVALID, "null engine");
+  CK(cudaSetDevice(e->device));
+  int rc = prime(e);
+  if (rc) return rc;
+  k_flag_rebuild<<<1, 256, 0, e->stream>>>(e->v, 1);
+  CK(cudaGetLastError());
+  rc = launch_rebuild(e);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(e->stream));
+  return ACG_OK;
+}
+
+int acg_compute_forces(acg_engine *e) {
+  if (!e) return fail(ACG_ERR_INVALID, "null engine");
+  CK(cudaSetDevice(e->device));
+  int rc = prime(e);
+  if (rc) return rc;
+  k_flag_rebuild<<<1, 256, 0, e->stream>>>(e->v, 1);
+  CK(cudaGetLastError());
+  rc = launch_rebuild(e);
+  if (rc) return rc;
+  rc = launch_force(e, 2);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(e->stream));
+  return ACG_OK;
+}
+
+int acg_step(acg_engine *e, int nsteps) {
+  if (!e) return fail(ACG_ERR_INVALID, "null engine");
+  if (nsteps < 0) return fail(ACG_ERR_INVALID, "nsteps < 0");
+  CK(cudaSetDevice(e->device));
+  int rc = prime(e);
+  if (rc) return rc;
+  if (nsteps >= GRAPH_STEPS && !e->gexec) {
+    rc = build_graph(e, GRAPH_STEPS, &e->graph, &e->gexec);
+    if (rc) return rc;
+    e->gsteps = GRAPH_STEPS;
+  }
+  if (nsteps % GRAPH_STEPS && !e->gexec1) {
+    rc = build_graph(e, 1, &e->graph1, &e->gexec1);
+    if (rc) return rc;
+  }
+  int left = nsteps;
+  while (left >= GRAPH_STEPS) {
+    CK(cudaGraphLaunch(e->gexec, e->stream));
+    left -= GRAPH_STEPS;
+  }
+  while (left-- > 0) CK(cudaGraphLaunch(e->gexec1, e->stream));
+  return ACG_OK;
+}
+
+int acg_step_eager(acg_engine *e, int nsteps) {
+  if (!e) return fail(ACG_ERR_INVALID, "null engine");
+  CK(cudaSetDevice(e->device));
+  int rc = prime(e);
+  if (rc) return rc;
+  for (int s = 0; s < nsteps; s++) {
+    rc = launch_step_eager(e);
+    if (rc) return rc;
+  }
+  return ACG_OK;
+}
+
+int acg_sync(acg_engine *e) {
+  if (!e) return fail(ACG_ERR_INVALID, "null engine");
+  CK(cudaSetDevice(e->device));
+  CK(cudaStreamSynchronize(e->stream));
+  return ACG_OK;
+}
+
+int acg_get_thermo(acg_engine *e, int sys, acg_thermo *out) {
+  int rc = check_sys(e, sys);
+  if (rc) return rc;
+  if (!out) return fail(ACG_ERR_INVALID, "null out");
+  CK(cudaSetDevice(e->device));
+  rc = prime(e);
+  if (rc) return rc;
+  SysState s;
+  CK(cudaMemcpyAsync(&s, e->v.st + sys, sizeof(s), cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  const SysDesc &d = e->lay.desc[sys];
+  memset(out, 0, sizeof(*out));
+  out->pe = s.pe;
+  out->ke = s.ke_end;
+  out->virial = s.virial;
+  out->vir_act = s.vir_act;
+  out->inst_T = 2.0 * s.ke_end / d.dof;
+  out->maxD = s.maxD_last;
+  for (int i = 0; i < NHC_M; i++) {
+    out->eta[i] = s.eta_end[i];
+    out->p_eta[i] = s.p_eta_end[i];
+    out->q[i] = d.q[i];
+  }
+  // Heff (MDcode/print.c:85-87)
+  double h = s.ke_end + s.pe + s.eta_end[0] * d.T * d.dof;
+  for (int i = 0; i < NHC_M; i++) h += s.p_eta_end[i] * s.p_eta_end[i] / (2.0 * d.q[i]);
+  for (int i = 1; i < NHC_M; i++) h += d.T * s.eta_end[i];
+  out->heff = h;
+  out->step = s.step;
+  out->rebuilds = s.rebuilds;
+  out->overflow = s.overflow;
+  out->status = s.status ? ACG_ERR_NONFINITE : 0;
+  if (s.status) return fail(ACG_ERR_NONFINITE, "system " + std::to_string(sys) + ": non-finite kinetic energy");
+  return ACG_OK;
+}
+
+int acg_get_cells(acg_engine *e, int sys, int *dims, int *ncell, int *counts, int *members) {
+  int rc = check_sys(e, sys);
+  if (rc) return rc;
+  CK(cudaSetDevice(e->device));
+  rc = prime(e);
+  if (rc) return rc;
+  const SysDesc &d = e->lay.desc[sys];
+  if (dims) dims[0] = dims[1] = dims[2] = d.nc;
+  if (ncell) *ncell = d.ncell;
+  if (counts)
+    CK(cudaMemcpyAsync(counts, e->v.ccount + d.coff, 4 * (size_t)d.ncell, cudaMemcpyDeviceToHost, e->stream));
+  if (members) {
+    // slots are in cell order after the rebuild: the member list is the id
+    // array of the system's slots
+    CK(cudaMemcpyAsync(members, e->v.id + d.poff, 4 * (size_t)d.n, cudaMemcpyDeviceToHost, e->stream));
+  }
+  CK(cudaStreamSynchronize(e->stream));
+  return ACG_OK;
+}
+
+int acg_set_launch(acg_engine *e, int tpp, int block) {
+  if (!e) return fail(ACG_ERR_INVALID, "null engine");
+  if (!force_fn(tpp, 0)) return fail(ACG_ERR_INVALID, "tpp must be 1, 2, 4, 8, 16 or 32");
+  if (block < 32 || block > 512 || block % 32 || block / tpp < 4)
+    return fail(ACG_ERR_INVALID, "block must be a multiple of 32 in [32,512] with >= 4 particles");
+  CK(cudaSetDevice(e->device));
+  CK(cudaStreamSynchronize(e->stream));
+  e->tpp = tpp;
+  e->block = block;
+  drop_graphs(e);
+  int rc = build_tiles_b(e);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(e->stream));
+  return ACG_OK;
+}
+
+int acg_get_launch(acg_engine *e, int *tpp, int *block) {
+  if (!e) return fail(ACG_ERR_INVALID, "null engine");
+  if (tpp) *tpp = e->tpp;
+  if (block) *block = e->block;
+  return ACG_OK;
+}
+
+int acg_time_stage(acg_engine *e, int stage, int reps, double *ms) {
+  if (!e || reps < 1 || !ms) return fail(ACG_ERR_INVALID, "bad arguments");
+  CK(cudaSetDevice(e->device));
+  int rc = prime(e);
+  if (rc) return rc;
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  // stage 1 evaluates forces only (mode 2) and stage 2 rebuilds at the
+  // current positions, so neither changes the trajectory; stage 0 drifts the
+  // particles and is meant for a scratch engine.
+  CK(cudaEventRecord(a, e->stream));
+  for (int i = 0; i < reps; i++) {
+    if (stage == 0) {
+      k_kick_drift<<<e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, 0, e->stream>>>(e->v, 0, 0);
+    } else if (stage == 1) {
+      rc = launch_force(e, 2);
+    } else {
+      k_flag_rebuild<<<1, 256, 0, e->stream>>>(e->v, 1);
+      rc = launch_rebuild(e);
+    }
+    if (rc) return rc;
+  }
+  CK(cudaEventRecord(b, e->stream));
+  CK(cudaEventSynchronize(b));
+  float t = 0;
+  CK(cudaEventElapsedTime(&t, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *ms = (double)t / reps;
+  return ACG_OK;
+}
+
+int acg_bench_steps(acg_engine *e, int nchunks, size_t flush_bytes, double *ms, int64_t *launches) {
+  if (!e || nchunks < 1 || !ms) return fail(ACG_ERR_INVALID, "bad arguments");
+  CK(cudaSetDevice(e->device));
+  int rc = prime(e);
+  if (rc) return rc;
+  if (!e->gexec) {
+    rc = build_graph(e, GRAPH_STEPS, &e->graph, &e->gexec);
+    if (rc) return rc;
+    e->gsteps = GRAPH_STEPS;
+  }
+  if (flush_bytes > e->flush_bytes) {
+    if (e->flush) cudaFree(e->flush);
+    e->flush = nullptr;
+    e->flush_bytes = 0;
+    CK(cudaMalloc(&e->flush, flush_bytes));
+    e->flush_bytes = flush_bytes;
+  }
+  std::vector<long long> rb0(e->lay.nsys);
+  for (int r = 0; r < e->lay.nsys; r++)
+    CK(cudaMemcpyAsync(&rb0[r], &e->v.st[r].rebuilds, sizeof(long long), cudaMemcpyDeviceToHost, e->stream));
+  std::vector<cudaEvent_t> ev(2 * nchunks);
+  for (auto &x : ev) CK(cudaEventCreate(&x));
+  for (int c = 0; c < nchunks; c++) {
+    if (flush_bytes) CK(cudaMemsetAsync(e->flush, c & 0xff, flush_bytes, e->stream));
+    CK(cudaEventRecord(ev[2 * c], e->stream));
+    CK(cudaGraphLaunch(e->gexec, e->stream));
+    CK(cudaEventRecord(ev[2 * c + 1], e->stream));
+  }
+  CK(cudaStreamSynchronize(e->stream));
+  double tot = 0;
+  for (int c = 0; c < nchunks; c++) {
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, ev[2 * c], ev[2 * c + 1]));
+    tot += t;
+  }
+  for (auto &x : ev) cudaEventDestroy(x);
+  std::vector<long long> rb1(e->lay.nsys);
+  for (int r = 0; r < e->lay.nsys; r++)
+    CK(cudaMemcpy(&rb1[r], &e->v.st[r].rebuilds, sizeof(long long), cudaMemcpyDeviceToHost));
+  // every step launches the kick/drift and force kernels; a step whose
+  // conditional fires also launches the six rebuild kernels
+  long long steps_with_rebuild = 0;
+  for (int r = 0; r < e->lay.nsys; r++) steps_with_rebuild = std::max(steps_with_rebuild, rb1[r] - rb0[r]);
+  *ms = tot;
+  if (launches) *launches = 2LL * GRAPH_STEPS * nchunks + 6LL * steps_with_rebuild;
+  return ACG_OK;
+}
+
+int acg_measure_fp64_peak(int device, double *tflops) {
+  if (!tflops) return fail(ACG_ERR_INVALID, "null out");
+  CK(cudaSetDevice(device));
+  int sms = 0;
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  const int blocks = sms * 8, threads = 256, iters = 4096;
+  double *out = nullptr;
+  CK(cudaMalloc(&out, sizeof(double) * blocks * threads));
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  k_fp64_fma<<<blocks, threads>>>(out, iters, 1.0000001);
+  CK(cudaEventRecord(a));
+  for (int r = 0; r < 5; r++) k_fp64_fma<<<blocks, threads>>>(out, iters, 1.0000001);
+  CK(cudaEventRecord(b));
+  CK(cudaEventSynchronize(b));
+  float t = 0;
+  CK(cudaEventElapsedTime(&t, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(out);
+  const double flops = 5.0 * blocks * threads * (double)iters * 8 * 2;
+  *tflops = flops / (t * 1e-3) / 1e12;
+  return ACG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,721 @@
+// Kernels of one MD timestep (all systems of a batch in one launch each).
+//
+// Step s, for every system r (MDcode/time_evolve.c:495-526 restated):
+//   k_kick_drift   v = (v*s2)*s1 + F*dt/2 ; x,xu += v*dt/L ; wrap ; max|xu-xold|^2
+//                  (U3 of the previous step's second half, U3+U2 of this step's
+//                  first half, U1).  Extra blocks re-randomise the direction
+//                  arrays when the step is a shuffle step.  The last block to
+//                  finish decides, per system, whether the lists are rebuilt
+//                  and sets the CUDA-graph conditional that guards the rebuild.
+//   rebuild (conditional):
+//     k_cells_count    cell of every slot + per-cell counts
+//     k_cells_scan     per-system exclusive scan -> cell starts
+//     k_cells_scatter  slot -> position in its cell (unordered)
+//     k_cells_order    per cell: order members by original index (stable
+//                      counting sort, so InCell order is reproduced exactly)
+//     k_permute        gather all per-particle arrays into cell order (scratch)
+//     k_build_list     full neighbour list per particle (warp per particle,
+//                      ballot compaction) and copy-back of the scratch arrays
+//   k_force_kick   pair forces from the list (TPP threads per particle, shuffle
+//                  reduction), active force, second kick v += F dt/2, block
+//                  sums of pe/virial/KE; the last block of each system finishes
+//                  the sums in a fixed order and runs the thermostat chain
+//                  (U4 U3 U4) for the end of this step and the first half of
+//                  the next one.
+#pragma once
+#include "acg_device.cuh"
+
+namespace acg {
+
+// ---------------------------------------------------------------------------
+// block reductions (fixed order => deterministic)
+template <int NWARP>
+__device__ __forceinline__ double block_sum(double v, double *sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < NWARP; i++) t += sh[i];
+  return t;  // valid in thread 0
+}
+
+__device__ __forceinline__ double block_sum_dyn(double v, double *sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < nw; i++) t += sh[i];
+  return t;
+}
+
+// ---------------------------------------------------------------------------
+// direction shuffle: new k = +1 for the `count(+1)` smallest keyed ranks
+__device__ inline int kcomp(char4 k, int c) { return c == 0 ? k.x : (c == 1 ? k.y : k.z); }
+__device__ inline void kset(char4 *p, int c, int v) {
+  signed char *b = reinterpret_cast<signed char *>(p);
+  b[c] = (signed char)v;
+}
+
+__device__ void shuffle_component(const View &v, int r, int comp, long long step) {
+  __shared__ unsigned int hist[256];
+  __shared__ unsigned int s_cnt, s_prefix, s_mask, s_want;
+  const SysDesc &d = v.desc[r];
+  const int nact = d.nact;
+  char4 *kd = v.kdir + d.aoff;
+  if (threadIdx.x == 0) s_cnt = 0;
+  __syncthreads();
+  unsigned int c = 0;
+  for (int a = threadIdx.x; a < nact; a += blockDim.x) c += kcomp(kd[a], comp) > 0;
+  atomicAdd(&s_cnt, c);
+  __syncthreads();
+  const unsigned int plus = s_cnt;
+  if (plus == 0 || plus == (unsigned)nact) return;  // nothing to permute
+  const uint64_t key = splitmix64(d.seed ^ splitmix64((uint64_t)step * 3ull + (uint64_t)comp));
+  unsigned int prefix = 0, mask = 0, want = plus;
+  for (int shift = 24; shift >= 0; shift -= 8) {
+    for (int b = threadIdx.x; b < 256; b += blockDim.x) hist[b] = 0;
+    __syncthreads();
+    for (int a = threadIdx.x; a < nact; a += blockDim.x) {
+      uint32_t kk = feistel32((uint32_t)a, key);
+      if ((kk & mask) == prefix) atomicAdd(&hist[(kk >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned int cum = 0, sel = 255;
+      for (unsigned int b = 0; b < 256; b++) {
+        if (cum + hist[b] > want) {
+          sel = b;
+          break;
+        }
+        cum += hist[b];
+      }
+      s_want = want - cum;
+      s_prefix = prefix | (sel << shift);
+      s_mask = mask | (255u << shift);
+    }
+    __syncthreads();
+    prefix = s_prefix;
+    mask = s_mask;
+    want = s_want;
+    __syncthreads();
+  }
+  // exactly `plus` keys are below the key of rank `plus`
+  for (int a = threadIdx.x; a < nact; a += blockDim.x)
+    kset(&kd[a], comp, feistel32((uint32_t)a, key) < prefix ? 1 : -1);
+}
+
+// ---------------------------------------------------------------------------
+// stage 1: kick + drift (+ shuffle blocks) + rebuild decision
+__global__ void __launch_bounds__(BLOCK_A) k_kick_drift(View v, int use_cond,
+                                                        cudaGraphConditionalHandle h) {
+  __shared__ double sm[BLOCK_A / 32];
+  __shared__ int s_last;
+  const int b = blockIdx.x;
+  double mymax = 0.0;
+  int r = -1;
+  if (b < v.ntiles_a) {
+    int2 t = v.tiles_a[b];
+    r = t.x;
+    const SysDesc &d = v.desc[r];
+    int loc = t.y + threadIdx.x;
+    if (loc < d.n) {
+      const int i = d.poff + loc;
+      const double s2 = v.st[r].s2, s1 = v.st[r].s1;
+      const double hdt = d.half_dt, dt = d.dt, il = d.invL;
+      // v_b * s1 + F dt/2, in the reference's order of roundings
+      double px = __dadd_rn(__dmul_rn(__dmul_rn(v.vx[i], s2), s1), __dmul_rn(v.fx[i], hdt));
+      double py = __dadd_rn(__dmul_rn(__dmul_rn(v.vy[i], s2), s1), __dmul_rn(v.fy[i], hdt));
+      double pz = __dadd_rn(__dmul_rn(__dmul_rn(v.vz[i], s2), s1), __dmul_rn(v.fz[i], hdt));
+      double ddx = __dmul_rn(__dmul_rn(px, dt), il);
+      double ddy = __dmul_rn(__dmul_rn(py, dt), il);
+      double ddz = __dmul_rn(__dmul_rn(pz, dt), il);
+      double4 p = v.pos[i];
+      double ux = __dadd_rn(v.ux[i], ddx), uy = __dadd_rn(v.uy[i], ddy), uz = __dadd_rn(v.uz[i], ddz);
+      p.x = wrap_unit(__dadd_rn(p.x, ddx));
+      p.y = wrap_unit(__dadd_rn(p.y, ddy));
+      p.z = wrap_unit(__dadd_rn(p.z, ddz));
+      double ex = __dadd_rn(ux, -v.ox[i]), ey = __dadd_rn(uy, -v.oy[i]), ez = __dadd_rn(uz, -v.oz[i]);
+      mymax = __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
+      v.vx[i] = px;
+      v.vy[i] = py;
+      v.vz[i] = pz;
+      v.ux[i] = ux;
+      v.uy[i] = uy;
+      v.uz[i] = uz;
+      v.pos[i] = p;
+    }
+    // per-system block max (a tile never straddles systems)
+    for (int o = 16; o > 0; o >>= 1) mymax = fmax(mymax, __shfl_down_sync(0xffffffffu, mymax, o));
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = mymax;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double m = sm[0];
+      for (int w = 1; w < BLOCK_A / 32; w++) m = fmax(m, sm[w]);
+      if (m > 0.0)
+        atomicMax(&v.st[r].maxd_bits, (unsigned long long)__double_as_longlong(m));
+    }
+  } else {
+    int q = b - v.ntiles_a;
+    int rs = q / 3, comp = q % 3;
+    const SysDesc &d = v.desc[rs];
+    long long step = v.st[rs].step;
+    if (d.shuffle && d.nact > 0 && d.tau_p > 0 && (step % d.tau_p) == 0)
+      shuffle_component(v, rs, comp, step);
+  }
+  // the last block to finish takes the per-system rebuild decisions
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(v.counter_a, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  int any = 0;
+  for (int s = threadIdx.x; s < v.nsys; s += blockDim.x) {
+    const SysDesc &d = v.desc[s];
+    SysState &st = v.st[s];
+    unsigned long long bits = atomicExch(&st.maxd_bits, 0ull);
+    double m = __dmul_rn(__dmul_rn(__longlong_as_double((long long)bits), d.L), d.L);
+    st.maxD_last = m;
+    int rb = (__dmul_rn(d.rebuild_factor, m) > d.skin2) || st.force_rebuild;
+    st.rebuild = rb;
+    st.force_rebuild = 0;
+    any |= rb;
+  }
+  any = __syncthreads_or(any);
+  if (threadIdx.x == 0) {
+    *v.counter_a = 0;
+    if (use_cond) cudaGraphSetConditional(h, any ? 1u : 0u);
+  }
+}
+
+// host request: rebuild the systems flagged `prime` (all < 0: rebuild all)
+__global__ void k_flag_rebuild(View v, int all) {
+  for (int s = threadIdx.x; s < v.nsys; s += blockDim.x) {
+    SysState &st = v.st[s];
+    st.rebuild = all ? 1 : st.prime;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// rebuild stage (runs only for systems with st.rebuild set)
+__global__ void __launch_bounds__(BLOCK_R) k_cells_count(View v) {
+  int2 t = v.tiles_a[blockIdx.x];
+  const int r = t.x;
+  if (!v.st[r].rebuild) return;
+  const SysDesc &d = v.desc[r];
+  int loc = t.y + threadIdx.x;
+  if (loc >= d.n) return;
+  const int i = d.poff + loc;
+  double4 p = v.pos[i];
+  // cell = floor(x*Inv) + floor(y*Inv)*Nc + floor(z*Inv)*Nc*Nc
+  // (MDcode/cell_list+forces.c:73-74), clamped to the grid
+  int cx = cell_coord(p.x, d.inv_cell, d.nc), cy = cell_coord(p.y, d.inv_cell, d.nc),
+      cz = cell_coord(p.z, d.inv_cell, d.nc);
+  int c = cx + cy * d.nc + cz * d.nc * d.nc;
+  v.cell_tmp[i] = c;
+  atomicAdd(&v.ccount_b[d.coff + c], 1);
+}
+
+__global__ void __launch_bounds__(BLOCK_SCAN) k_cells_scan(View v) {
+  __shared__ int sh[BLOCK_SCAN];
+  const int r = blockIdx.x;
+  SysState &st = v.st[r];
+  if (!st.rebuild) return;
+  const SysDesc &d = v.desc[r];
+  const int nc = d.ncell, B = blockDim.x;
+  const int chunk = (nc + B - 1) / B;
+  const int beg = min(threadIdx.x * chunk, nc), end = min(beg + chunk, nc);
+  int sum = 0;
+  for (int c = beg; c < end; c++) sum += v.ccount_b[d.coff + c];
+  sh[threadIdx.x] = sum;
+  __syncthreads();
+  for (int o = 1; o < B; o <<= 1) {  // inclusive Hillis-Steele scan
+    int x = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
+    __syncthreads();
+    sh[threadIdx.x] += x;
+    __syncthreads();
+  }
+  int run = sh[threadIdx.x] - sum;
+  for (int c = beg; c < end; c++) {
+    int k = v.ccount_b[d.coff + c];
+    v.cstart[d.coff + c] = run;
+    v.ccount[d.coff + c] = k;
+    v.ccount_b[d.coff + c] = 0;
+    v.cfill[d.coff + c] = 0;
+    run += k;
+  }
+  if (threadIdx.x == 0) {
+    st.rebuilds += 1;
+    st.overflow = 0;
+  }
+}
+
+__global__ void __launch_bounds__(BLOCK_R) k_cells_scatter(View v) {
+  int2 t = v.tiles_a[blockIdx.x];
+  const int r = t.x;
+  if (!v.st[r].rebuild) return;
+  const SysDesc &d = v.desc[r];
+  int loc = t.y + threadIdx.x;
+  if (loc >= d.n) return;
+  const int i = d.poff + loc;
+  int c = v.cell_tmp[i];
+  int k = atomicAdd(&v.cfill[d.coff + c], 1);
+  v.perm_u[d.poff + v.cstart[d.coff + c] + k] = i;
+}
+
+// one warp per cell: order the members by original particle index
+__global__ void __launch_bounds__(32 * CELLS_PER_TILE) k_cells_order(View v) {
+  int2 t = v.tiles_c[blockIdx.x];
+  const int r = t.x;
+  if (!v.st[r].rebuild) return;
+  const SysDesc &d = v.desc[r];
+  const int c = t.y + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (c >= d.ncell) return;
+  const int m = v.ccount[d.coff + c];
+  const int base = d.poff + v.cstart[d.coff + c];
+  for (int a = lane; a < m; a += 32) {
+    int sa = v.perm_u[base + a];
+    int ida = v.id[sa];
+    int rank = 0;
+    for (int b = 0; b < m; b++) rank += v.id[v.perm_u[base + b]] < ida;
+    v.perm[base + rank] = sa;
+    v.cellof[base + rank] = c;
+  }
+}
+
+__global__ void __launch_bounds__(BLOCK_R) k_permute(View v) {
+  int2 t = v.tiles_a[blockIdx.x];
+  const int r = t.x;
+  if (!v.st[r].rebuild) return;
+  const SysDesc &d = v.desc[r];
+  int loc = t.y + threadIdx.x;
+  if (loc >= d.n) return;
+  const int i = d.poff + loc;
+  const int o = v.perm[i];
+  v.pos_s[i] = v.pos[o];
+  v.ux_s[i] = v.ux[o];
+  v.uy_s[i] = v.uy[o];
+  v.uz_s[i] = v.uz[o];
+  v.vx_s[i] = v.vx[o];
+  v.vy_s[i] = v.vy[o];
+  v.vz_s[i] = v.vz[o];
+  v.fx_s[i] = v.fx[o];
+  v.fy_s[i] = v.fy[o];
+  v.fz_s[i] = v.fz[o];
+  v.id_s[i] = v.id[o];
+  v.act_s[i] = v.act[o];
+}
+
+__device__ __forceinline__ double lcut2_of(const SysDesc &d, int tsum) {
+  return tsum == 0 ? d.lcut2[0] : (tsum == 1 ? d.lcut2[1] : d.lcut2[2]);
+}
+
+// one warp per particle (sorted slot): scan the neighbour cells of its cell
+// and append every slot closer than the list cut (MDcode/cell_list+forces.c:
+// 82-140, here as a full list: each pair appears in both particles' rows)
+__global__ void __launch_bounds__(BLOCK_L) k_build_list(View v) {
+  int2 t = v.tiles_l[blockIdx.x];
+  const int r = t.x;
+  if (!v.st[r].rebuild) return;
+  const SysDesc &d = v.desc[r];
+  const int loc = t.y + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (loc >= d.n) return;
+  const int i = d.poff + loc;
+  const double4 pi = v.pos_s[i];
+  const int ti = (int)pi.w;
+  const double L = d.L;
+  const int nc = d.nc, c = v.cellof[i];
+  const int cx = c % nc, cy = (c / nc) % nc, cz = c / (nc * nc);
+  const int lo = stencil_lo(nc), hi = stencil_hi(nc);
+  const int maxnb = v.maxnb;
+  int *row = v.nbl + (size_t)i * maxnb;
+  int cnt = 0;
+  for (int oz = lo; oz <= hi; oz++)
+    for (int oy = lo; oy <= hi; oy++)
+      for (int ox = lo; ox <= hi; ox++) {
+        int c2 = wrap_cell(cx + ox, nc) + wrap_cell(cy + oy, nc) * nc + wrap_cell(cz + oz, nc) * nc * nc;
+        const int s0 = d.poff + v.cstart[d.coff + c2], m = v.ccount[d.coff + c2];
+        for (int k0 = 0; k0 < m; k0 += 32) {
+          const int k = k0 + lane;
+          bool ok = false;
+          int j = s0 + k;
+          if (k < m && j != i) {
+            double4 pj = v.pos_s[j];
+            double dx = min_image(pi.x - pj.x), dy = min_image(pi.y - pj.y), dz = min_image(pi.z - pj.z);
+            double dr2 = (dx * dx + dy * dy + dz * dz) * L * L;
+            ok = dr2 < lcut2_of(d, ti + (int)pj.w);
+          }
+          unsigned int mask = __ballot_sync(0xffffffffu, ok);
+          if (ok) {
+            int pos = cnt + __popc(mask & ((1u << lane) - 1u));
+            if (pos < maxnb) row[pos] = j;
+          }
+          cnt += __popc(mask);
+        }
+      }
+  if (lane == 0) {
+    if (cnt > maxnb) {
+      v.nbn[i] = -1;  // served from the cell list by the force kernel
+      atomicAdd(&v.st[r].overflow, 1);
+    } else {
+      v.nbn[i] = cnt;
+    }
+    v.pos[i] = pi;
+    v.ux[i] = v.ux_s[i];
+    v.uy[i] = v.uy_s[i];
+    v.uz[i] = v.uz_s[i];
+    v.ox[i] = v.ux_s[i];
+    v.oy[i] = v.uy_s[i];
+    v.oz[i] = v.uz_s[i];
+    v.vx[i] = v.vx_s[i];
+    v.vy[i] = v.vy_s[i];
+    v.vz[i] = v.vz_s[i];
+    v.fx[i] = v.fx_s[i];
+    v.fy[i] = v.fy_s[i];
+    v.fz[i] = v.fz_s[i];
+    v.id[i] = v.id_s[i];
+    v.act[i] = v.act_s[i];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// pair term (MDcode/cell_list+forces.c:174-203).  dr2/sigma^2 and 1/dr2 use
+// the precomputed 1/sigma^2 instead of the reference's two divisions; the
+// results agree to rounding.
+struct PairAcc {
+  double fx, fy, fz, pe, vir;
+};
+
+__device__ __forceinline__ void pair_fp64(PairAcc &a, const double4 &pi, int ti, const double4 &pj,
+                                          double L, double L2) {
+  const int tp = ti + (int)pj.w;
+  double dx = min_image(pi.x - pj.x), dy = min_image(pi.y - pj.y), dz = min_image(pi.z - pj.z);
+  double dr2 = (dx * dx + dy * dy + dz * dz) * L2;
+  // 1/sigma^2, 4 eps, 8 eps/sigma^2 for AA / AB / BB
+  const double is2 = tp == 0 ? 1.0 : (tp == 1 ? 1.5625 : 1.0 / (0.88 * 0.88));
+  double rs2 = dr2 * is2;
+  if (rs2 < KA_RC2) {
+    const double e4 = tp == 0 ? 4.0 : (tp == 1 ? 6.0 : 2.0);
+    double s2 = 1.0 / rs2;
+    double s6 = s2 * s2 * s2;
+    a.pe += e4 * ((s6 * (s6 - 1.0)) + KA_C0 + KA_C2 * rs2);
+    double g = (2.0 * e4 * is2) * (6.0 * s6 * (s6 - 0.5) * s2 - KA_C2);
+    double gl = g * L;
+    a.fx += gl * dx;
+    a.fy += gl * dy;
+    a.fz += gl * dz;
+    a.vir += g * dr2;
+  }
+}
+
+__device__ __forceinline__ void pair_fp32(PairAcc &a, const double4 &pi, int ti, const double4 &pj,
+                                          double L, double) {
+  const int tp = ti + (int)pj.w;
+  // the separation is formed in FP64 (positions stay FP64), the pair math in FP32
+  const float Lf = (float)L;
+  float dx = (float)min_image(pi.x - pj.x) * Lf, dy = (float)min_image(pi.y - pj.y) * Lf,
+        dz = (float)min_image(pi.z - pj.z) * Lf;
+  float dr2 = dx * dx + dy * dy + dz * dz;
+  const float is2 = tp == 0 ? 1.0f : (tp == 1 ? 1.5625f : (float)(1.0 / (0.88 * 0.88)));
+  float rs2 = dr2 * is2;
+  if (rs2 < (float)KA_RC2) {
+    const float e4 = tp == 0 ? 4.0f : (tp == 1 ? 6.0f : 2.0f);
+    float s2 = __frcp_rn(rs2);
+    float s6 = s2 * s2 * s2;
+    a.pe += (double)(e4 * ((s6 * (s6 - 1.0f)) + (float)KA_C0 + (float)KA_C2 * rs2));
+    float g = (2.0f * e4 * is2) * (6.0f * s6 * (s6 - 0.5f) * s2 - (float)KA_C2);
+    a.fx += (double)(g * dx);
+    a.fy += (double)(g * dy);
+    a.fz += (double)(g * dz);
+    a.vir += (double)(g * dr2);
+  }
+}
+
+// finish one system after its last force block: fixed-order sums, then the
+// thermostat chain (runs in a single block)
+__device__ void finalize_system(const View &v, int r, int mode) {
+  __shared__ double sh[32];
+  const SysDesc &d = v.desc[r];
+  SysState &st = v.st[r];
+  double pe = 0.0, vir = 0.0, ke = 0.0, va = 0.0;
+  for (int k = threadIdx.x; k < d.ntile_b; k += blockDim.x) {
+    const double2 *pp = reinterpret_cast<const double2 *>(&v.part_b[d.tile0_b + k]);
+    const double2 p0 = __ldcg(pp), p1 = __ldcg(pp + 1);
+    pe += p0.x;
+    vir += p0.y;
+    ke += p1.x;
+    va += p1.y;
+  }
+  pe = block_sum_dyn(pe, sh);
+  vir = block_sum_dyn(vir, sh);
+  ke = block_sum_dyn(ke, sh);
+  va = block_sum_dyn(va, sh);
+  if (threadIdx.x != 0) return;
+  st.pe = 0.5 * pe;
+  st.virial = (0.5 * vir) / 3.0;
+  st.vir_act = va;
+  if (mode == 2) {  // force evaluation only (calculate_forces)
+    __threadfence();
+    st.counter_b = 0;
+    return;
+  }
+  double eta[NHC_M], pet[NHC_M];
+  double kb;
+  if (mode == 0) {
+    if (d.thermostat) {
+      for (int k = 0; k < NHC_M; k++) {
+        eta[k] = st.eta_cur[k];
+        pet[k] = st.p_eta_cur[k];
+      }
+      double s2 = nhc_half(eta, pet, d.q, d.T, d.dof, d.dt, ke);
+      for (int k = 0; k < NHC_M; k++) {
+        st.eta_end[k] = eta[k];
+        st.p_eta_end[k] = pet[k];
+      }
+      st.s2 = s2;
+      kb = (s2 * s2) * ke;
+    } else {
+      st.s2 = 1.0;
+      kb = ke;
+    }
+    st.step += 1;
+  } else {
+    st.s2 = 1.0;  // velocities were materialised by the prime pass
+    kb = ke;
+  }
+  st.ke_end = kb * 0.5;
+  if (d.thermostat) {
+    for (int k = 0; k < NHC_M; k++) {
+      eta[k] = st.eta_end[k];
+      pet[k] = st.p_eta_end[k];
+    }
+    double s1 = nhc_half(eta, pet, d.q, d.T, d.dof, d.dt, kb);
+    for (int k = 0; k < NHC_M; k++) {
+      st.eta_cur[k] = eta[k];
+      st.p_eta_cur[k] = pet[k];
+    }
+    st.s1 = s1;
+  } else {
+    st.s1 = 1.0;
+  }
+  if (!(ke == ke) || ke > 1.0e300) st.status = 1;
+  st.prime = 0;
+  __threadfence();
+  st.counter_b = 0;
+}
+
+// stage 2: forces + second kick.  mode 0 = step; 1 = prime (forces at the
+// current positions for systems flagged `prime`, pending velocity scale
+// applied, thermostat first half recomputed); 2 = forces only, velocities and
+// thermostat untouched (calculate_forces)
+template <int TPP, int PREC>
+__global__ void __launch_bounds__(512) k_force_kick(View v, int mode) {
+  __shared__ double sh[32];
+  __shared__ int s_last;
+  const int2 t = v.tiles_b[blockIdx.x];
+  const int r = t.x;
+  SysState &st = v.st[r];
+  if (mode == 1 && !st.prime) return;
+  const SysDesc &d = v.desc[r];
+  const int grp = threadIdx.x / TPP, lane = threadIdx.x % TPP;
+  const int loc = t.y + grp;
+  const bool valid = loc < d.n;
+  const int i = d.poff + (valid ? loc : 0);
+  const double L = d.L, L2 = d.L * d.L;
+  PairAcc a = {0.0, 0.0, 0.0, 0.0, 0.0};
+  if (valid) {
+    const double4 pi = v.pos[i];
+    const int ti = (int)pi.w;
+    const int nn = v.nbn[i];
+    if (nn >= 0) {
+      const int *row = v.nbl + (size_t)i * v.maxnb;
+      for (int k = lane; k < nn; k += TPP) {
+        const double4 pj = v.pos[__ldg(row + k)];
+        if (PREC == 0)
+          pair_fp64(a, pi, ti, pj, L, L2);
+        else
+          pair_fp32(a, pi, ti, pj, L, L2);
+      }
+    } else {
+      // neighbour-list overflow: scan the cells around the cell of the last
+      // rebuild (every pair within the cut is there since displacements stay
+      // below the skin)
+      const int nc = d.nc, c = v.cellof[i];
+      const int cx = c % nc, cy = (c / nc) % nc, cz = c / (nc * nc);
+      const int lo = stencil_lo(nc), hi = stencil_hi(nc);
+      for (int oz = lo; oz <= hi; oz++)
+        for (int oy = lo; oy <= hi; oy++)
+          for (int ox = lo; ox <= hi; ox++) {
+            int c2 = wrap_cell(cx + ox, nc) + wrap_cell(cy + oy, nc) * nc + wrap_cell(cz + oz, nc) * nc * nc;
+            const int s0 = d.poff + v.cstart[d.coff + c2], m = v.ccount[d.coff + c2];
+            for (int k = lane; k < m; k += TPP) {
+              const int j = s0 + k;
+              if (j == i) continue;
+              const double4 pj = v.pos[j];
+              if (PREC == 0)
+                pair_fp64(a, pi, ti, pj, L, L2);
+              else
+                pair_fp32(a, pi, ti, pj, L, L2);
+            }
+          }
+    }
+  }
+#pragma unroll
+  for (int o = TPP / 2; o > 0; o >>= 1) {
+    a.fx += __shfl_xor_sync(0xffffffffu, a.fx, o);
+    a.fy += __shfl_xor_sync(0xffffffffu, a.fy, o);
+    a.fz += __shfl_xor_sync(0xffffffffu, a.fz, o);
+    a.pe += __shfl_xor_sync(0xffffffffu, a.pe, o);
+    a.vir += __shfl_xor_sync(0xffffffffu, a.vir, o);
+  }
+  double ke = 0.0, va = 0.0, pe = 0.0, vir = 0.0;
+  if (valid && lane == 0) {
+    double fx = a.fx, fy = a.fy, fz = a.fz;
+    const int ai = v.act[i];
+    if (ai >= 0) {  // active force (MDcode/cell_list+forces.c:207-218)
+      const char4 k = v.kdir[d.aoff + ai];
+      const double kx = (double)k.x, ky = (double)k.y, kz = (double)k.z;
+      fx += d.f0 * kx;
+      fy += d.f0 * ky;
+      fz += d.f0 * kz;
+      va = d.f0 * (kx * v.ux[i] + ky * v.uy[i] + kz * v.uz[i]);
+    }
+    v.fx[i] = fx;
+    v.fy[i] = fy;
+    v.fz[i] = fz;
+    double px, py, pz;
+    if (mode == 2) {
+      px = py = pz = 0.0;
+    } else if (mode == 0) {  // U2 (MDcode/time_evolve.c:558-567)
+      px = __dadd_rn(v.vx[i], __dmul_rn(fx, d.half_dt));
+      py = __dadd_rn(v.vy[i], __dmul_rn(fy, d.half_dt));
+      pz = __dadd_rn(v.vz[i], __dmul_rn(fz, d.half_dt));
+    } else {
+      const double s2 = st.s2;
+      px = __dmul_rn(v.vx[i], s2);
+      py = __dmul_rn(v.vy[i], s2);
+      pz = __dmul_rn(v.vz[i], s2);
+    }
+    if (mode != 2) {
+      v.vx[i] = px;
+      v.vy[i] = py;
+      v.vz[i] = pz;
+    }
+    ke = px * px + py * py + pz * pz;
+    pe = a.pe;
+    vir = a.vir;
+  }
+  pe = block_sum_dyn(pe, sh);
+  vir = block_sum_dyn(vir, sh);
+  ke = block_sum_dyn(ke, sh);
+  va = block_sum_dyn(va, sh);
+  if (threadIdx.x == 0) {
+    v.part_b[blockIdx.x] = make_double4(pe, vir, ke, va);
+    __threadfence();
+    s_last = atomicAdd(&st.counter_b, 1u) == (unsigned)(d.ntile_b - 1);
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  finalize_system(v, r, mode);
+}
+
+// ---------------------------------------------------------------------------
+// state upload / download (caller order <-> slots)
+__global__ void k_load(View v, int r) {
+  const SysDesc &d = v.desc[r];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < d.n; k += gridDim.x * blockDim.x) {
+    const int i = d.poff + k;
+    const double *s = v.stage_d + 9 * (size_t)d.poff;
+    const int *si = v.stage_i + 2 * (size_t)d.poff;
+    v.pos[i] = make_double4(s[3 * k], s[3 * k + 1], s[3 * k + 2], (double)si[k]);
+    const double *u = s + 3 * (size_t)d.n, *p = s + 6 * (size_t)d.n;
+    v.ux[i] = u[3 * k];
+    v.uy[i] = u[3 * k + 1];
+    v.uz[i] = u[3 * k + 2];
+    v.ox[i] = u[3 * k];
+    v.oy[i] = u[3 * k + 1];
+    v.oz[i] = u[3 * k + 2];
+    v.vx[i] = p[3 * k];
+    v.vy[i] = p[3 * k + 1];
+    v.vz[i] = p[3 * k + 2];
+    v.fx[i] = v.fy[i] = v.fz[i] = 0.0;
+    v.id[i] = k;
+    v.act[i] = si[d.n + k];
+    v.nbn[i] = 0;
+    v.cellof[i] = 0;
+  }
+}
+
+__global__ void k_unload(View v, int r) {
+  const SysDesc &d = v.desc[r];
+  const double s2 = v.st[r].s2;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < d.n; k += gridDim.x * blockDim.x) {
+    const int i = d.poff + k;
+    const int o = v.id[i];
+    double *s = v.stage_d + 9 * (size_t)d.poff;
+    double *u = s + 3 * (size_t)d.n, *p = s + 6 * (size_t)d.n;
+    double *f = v.stage_f + 3 * (size_t)d.poff;
+    const double4 q = v.pos[i];
+    s[3 * o] = q.x;
+    s[3 * o + 1] = q.y;
+    s[3 * o + 2] = q.z;
+    u[3 * o] = v.ux[i];
+    u[3 * o + 1] = v.uy[i];
+    u[3 * o + 2] = v.uz[i];
+    p[3 * o] = __dmul_rn(v.vx[i], s2);
+    p[3 * o + 1] = __dmul_rn(v.vy[i], s2);
+    p[3 * o + 2] = __dmul_rn(v.vz[i], s2);
+    f[3 * o] = v.fx[i];
+    f[3 * o + 1] = v.fy[i];
+    f[3 * o + 2] = v.fz[i];
+    v.stage_i[2 * (size_t)d.poff + k] = o;  // slot order -> original index (cells)
+  }
+}
+
+// recompute the next step's first thermostat half after a host change of the
+// chain or temperature (single thread per system)
+__global__ void k_prehalf(View v, int r) {
+  const SysDesc &d = v.desc[r];
+  SysState &st = v.st[r];
+  if (!d.thermostat) {
+    st.s1 = 1.0;
+    return;
+  }
+  double eta[NHC_M], pet[NHC_M];
+  for (int k = 0; k < NHC_M; k++) {
+    eta[k] = st.eta_end[k];
+    pet[k] = st.p_eta_end[k];
+  }
+  double s1 = nhc_half(eta, pet, d.q, d.T, d.dof, d.dt, 2.0 * st.ke_end);
+  for (int k = 0; k < NHC_M; k++) {
+    st.eta_cur[k] = eta[k];
+    st.p_eta_cur[k] = pet[k];
+  }
+  st.s1 = s1;
+}
+
+__global__ void k_shuffle_now(View v, int r) { shuffle_component(v, r, blockIdx.x, v.st[r].step); }
+
+// FP64 pipe probe: 8 independent FMA chains per thread
+__global__ void k_fp64_fma(double *out, int iters, double m) {
+  double a[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) a[k] = 1.0 + 1e-3 * (threadIdx.x + k);
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) a[k] = fma(a[k], m, 1e-9);
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < 8; k++) s += a[k];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+}  // namespace acg

@@ -1,0 +1,196 @@
+"""Python mirror of the C ABI: an Engine holds one or many systems on a GPU.
+
+The names follow the reference's routines (MDcode/subroutine.h): ``rebuild``
+is update_cell_list, ``compute_forces`` is calculate_forces, ``step`` is the
+run() loop body (ShuffleActDirec when due + AdvanceTimeNVTNoseHoover),
+``shuffle`` is ShuffleActDirec, ``set_nhc`` is the chain set-up of
+InitialiseNoseHoover.  Arrays are numpy, in the caller's particle order and the
+reference's units.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Sequence
+
+import numpy as np
+
+from . import _abi
+from ._abi import acg_params, acg_thermo, check
+
+
+def default_params(n: int, **kw) -> acg_params:
+    p = acg_params()
+    check(_abi.lib().acg_params_default(C.byref(p), int(n)))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise AttributeError(f"acg_params has no field {k}")
+        setattr(p, k, v)
+    return p
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _f64(a, shape):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(shape))
+
+
+def _i32(a, shape):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.int32).reshape(shape))
+
+
+def measure_fp64_peak(device: int = 0) -> float:
+    """FP64 FMA throughput of the device in TFLOP/s."""
+    t = C.c_double()
+    check(_abi.lib().acg_measure_fp64_peak(int(device), C.byref(t)))
+    return t.value
+
+
+def footprint(params: Sequence[acg_params]) -> int:
+    arr = (acg_params * len(params))(*params)
+    out = C.c_size_t(0)
+    check(_abi.lib().acg_footprint(arr, len(params), C.byref(out)))
+    return int(out.value)
+
+
+class Engine:
+    """A batch of independent systems resident on one GPU."""
+
+    def __init__(self, params: acg_params | Sequence[acg_params], device: int = 0):
+        if isinstance(params, acg_params):
+            params = [params]
+        self.params = list(params)
+        self._lib = _abi.lib()
+        arr = (acg_params * len(self.params))(*self.params)
+        h = C.c_void_p()
+        check(self._lib.acg_create(arr, len(self.params), int(device), C.byref(h)))
+        self.h = h
+        self.sizes = []
+        for r in range(len(self.params)):
+            n, na = C.c_int(), C.c_int()
+            check(self._lib.acg_system_size(self.h, r, C.byref(n), C.byref(na)))
+            self.sizes.append((n.value, na.value))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._lib.acg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def nsys(self) -> int:
+        return len(self.params)
+
+    def n(self, sys: int = 0) -> int:
+        return self.sizes[sys][0]
+
+    def nact(self, sys: int = 0) -> int:
+        return self.sizes[sys][1]
+
+    # -- state -----------------------------------------------------------
+    def set_state(self, sys: int, state, set_directions: bool = True):
+        n = self.n(sys)
+        x = _f64(state.x, (n, 3))
+        xu = _f64(state.xu, (n, 3))
+        p = _f64(state.p, (n, 3))
+        t = _i32(state.type, (n,))
+        a = _i32(state.act_tag, (n,))
+        check(self._lib.acg_set_state(self.h, sys, _ptr(x), _ptr(xu), _ptr(p), _ptr(t), _ptr(a)))
+        if set_directions and self.nact(sys):
+            self.set_directions(sys, state.k)
+
+    def get_state(self, sys: int = 0):
+        n = self.n(sys)
+        x, xu, p, F = (np.empty((n, 3)) for _ in range(4))
+        check(self._lib.acg_get_state(self.h, sys, _ptr(x), _ptr(xu), _ptr(p), _ptr(F)))
+        return x, xu, p, F
+
+    def set_directions(self, sys: int, k):
+        na = self.nact(sys)
+        kk = _i32(k, (3 * na,))
+        check(self._lib.acg_set_directions(self.h, sys, _ptr(kk)))
+
+    def get_directions(self, sys: int = 0):
+        na = self.nact(sys)
+        k = np.zeros(3 * max(na, 1), dtype=np.int32)
+        check(self._lib.acg_get_directions(self.h, sys, _ptr(k)))
+        return k[: 3 * na].reshape(3, na)
+
+    def shuffle(self, sys: int = 0):
+        check(self._lib.acg_shuffle_directions(self.h, sys))
+
+    def set_nhc(self, sys: int, eta, p_eta):
+        e = _f64(eta, (3,))
+        pe = _f64(p_eta, (3,))
+        check(self._lib.acg_set_nhc(self.h, sys, _ptr(e), _ptr(pe)))
+
+    def set_temperature(self, sys: int, T: float):
+        check(self._lib.acg_set_temperature(self.h, sys, float(T)))
+
+    # -- stepping --------------------------------------------------------
+    def rebuild(self):
+        check(self._lib.acg_rebuild(self.h))
+
+    def compute_forces(self):
+        check(self._lib.acg_compute_forces(self.h))
+
+    def step(self, nsteps: int):
+        check(self._lib.acg_step(self.h, int(nsteps)))
+
+    def step_eager(self, nsteps: int):
+        check(self._lib.acg_step_eager(self.h, int(nsteps)))
+
+    def sync(self):
+        check(self._lib.acg_sync(self.h))
+
+    def thermo(self, sys: int = 0) -> dict:
+        t = acg_thermo()
+        rc = self._lib.acg_get_thermo(self.h, sys, C.byref(t))
+        out = {f: getattr(t, f) for f, _ in acg_thermo._fields_}
+        for f in ("eta", "p_eta", "q"):
+            out[f] = np.array(list(out[f]))
+        check(rc)
+        return out
+
+    def cells(self, sys: int = 0):
+        dims = np.zeros(3, dtype=np.int32)
+        nc = C.c_int()
+        check(self._lib.acg_get_cells(self.h, sys, _ptr(dims), C.byref(nc), None, None))
+        counts = np.zeros(nc.value, dtype=np.int32)
+        members = np.zeros(self.n(sys), dtype=np.int32)
+        check(self._lib.acg_get_cells(self.h, sys, _ptr(dims), C.byref(nc), _ptr(counts), _ptr(members)))
+        return dims, counts, members
+
+    # -- tuning / timing -------------------------------------------------
+    def set_launch(self, tpp: int, block: int):
+        check(self._lib.acg_set_launch(self.h, int(tpp), int(block)))
+
+    def get_launch(self):
+        t, b = C.c_int(), C.c_int()
+        check(self._lib.acg_get_launch(self.h, C.byref(t), C.byref(b)))
+        return t.value, b.value
+
+    def time_stage(self, stage: int, reps: int = 20) -> float:
+        ms = C.c_double()
+        check(self._lib.acg_time_stage(self.h, int(stage), int(reps), C.byref(ms)))
+        return ms.value
+
+    def bench_steps(self, nchunks: int, flush_bytes: int = 256 << 20):
+        """(device ms summed over the timed 32-step launches, kernel launches)"""
+        ms = C.c_double()
+        nl = C.c_int64()
+        check(self._lib.acg_bench_steps(self.h, int(nchunks), int(flush_bytes), C.byref(ms), C.byref(nl)))
+        return ms.value, nl.value
+
+    @property
+    def stream(self) -> int:
+        return int(self._lib.acg_stream(self.h) or 0)

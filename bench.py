@@ -1,0 +1,370 @@
+#!/usr/bin/env python
+"""Throughput of the active Kob-Andersen MD timestep (particle-steps/s).
+
+Workload (default): the plain method at scale — one KA 80:20 system,
+N = 100000 at density 1.2, T = 0.45, f0 = 1.0, tau_p = 1.0 (200 steps),
+active fraction 0.1, dt = 0.005, FP64 throughout, Nose-Hoover chain NVT.
+Synthetic data: a seeded random lattice melted on the device (T = 2.0, then
+T = 0.45) before the timed region.  One bench step is one MD timestep of the
+whole system; timed iterations are CUDA-graph launches of 32 steps with a
+256 MiB write between them (untimed) so every launch starts from a cold L2.
+
+--gpus N under torchrun runs one independent replica per GPU (replicas only:
+the path does not shard), value = all ranks' particle-steps / max time.
+--impl reference times the reference's own CPU code (compiled from its
+sources into oracle/_ref) on all host cores as independent single-rank
+processes.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+B_ALG = 148.0             # algorithmic bytes per particle-step (x, xu, v, type read + x, xu, v written)
+PAIRS_PER_PARTICLE = 32.6  # interacting pairs per particle (each pair once), ideal-gas estimate
+FLOPS_PER_PAIR = 30.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=32000, help="timed MD steps (rounded up to 32)")
+    ap.add_argument("--warmup", type=int, default=512, help="untimed MD steps before timing (>= 3)")
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=100000)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--equil", type=int, default=2048, help="melt steps at T=2.0 and again at T=0.45")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# CPU side: the reference (or the oracle restatement) on host cores
+def _cpu_worker(n, seed, seconds, max_steps, kind, barrier, q):
+    import numpy as np
+
+    from activechi4_b200.init import lattice_state
+    st = lattice_state(n, 0.45, seed=seed)
+    p_eta = np.array([0.1, -0.1, 0.05])
+    if kind == "reference":
+        from oracle import Reference
+        sysm = Reference(n)
+        sysm.setup(st, 0.45, 1.0, p_eta=p_eta)
+        sysm.seed_rng(seed + 1)
+    else:
+        from oracle import Oracle
+        sysm = Oracle.from_state(st, 0.45, 1.0, p_eta=p_eta)
+        sysm.seed_rng(seed + 1)
+    t0 = time.perf_counter()
+    sysm.run(2, start=0, shuffle=True)  # warm-up and per-step estimate
+    t1 = (time.perf_counter() - t0) / 2
+    steps = int(max(3, min(max_steps, seconds / max(t1, 1e-9))))
+    if barrier is not None:
+        barrier.wait()
+    t0 = time.perf_counter()
+    sysm.run(steps, start=2, shuffle=True)
+    q.put((steps, time.perf_counter() - t0))
+
+
+def cpu_run(n, nproc, seconds, max_steps):
+    from oracle import reference_available
+    kind = "reference" if reference_available(n) else "port"
+    ctx = mp.get_context("spawn")  # never fork a process that holds a CUDA context
+    q = ctx.Queue()
+    bar = ctx.Barrier(nproc) if nproc > 1 else None
+    procs = [ctx.Process(target=_cpu_worker, args=(n, 100 + i, seconds, max_steps, kind, bar, q))
+             for i in range(nproc)]
+    for p in procs:
+        p.start()
+    res = [q.get() for _ in procs]
+    for p in procs:
+        p.join()
+    steps = [r[0] for r in res]
+    wall = max(r[1] for r in res)
+    return kind, sum(n * s for s in steps) / wall, steps, wall
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.p is not None:
+            time.sleep(0.15)
+            self.p.terminate()
+            try:
+                self.out, _ = self.p.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+                self.out = ""
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (self.out or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """dram bytes per force launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "force_kernel_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+# ---------------------------------------------------------------------------
+def make_engine(n, precision, seed, device, equil):
+    import numpy as np
+
+    from activechi4_b200 import Engine, default_params
+    from activechi4_b200.init import lattice_state
+    prec = 1 if precision == "fp32" else 0
+    p = default_params(n, T=2.0, f0=1.0, tau_p_steps=200, precision=prec, seed=seed)
+    e = Engine(p, device=device)
+    st = lattice_state(n, 2.0, seed=seed)
+    e.set_state(0, st)
+    rng = np.random.default_rng(seed)
+    q = e.thermo(0)["q"]
+    e.set_nhc(0, np.zeros(3), np.sqrt(2.0 * q) * rng.standard_normal(3))
+    e.step(equil)
+    e.set_temperature(0, 0.45)
+    q = e.thermo(0)["q"]
+    e.set_nhc(0, np.zeros(3), np.sqrt(0.45 * q) * rng.standard_normal(3))
+    e.step(equil)
+    e.sync()
+    return e, st
+
+
+def e2e_run(e, st, nchunks):
+    """Through the public C ABI with host buffers: load the state from pinned
+    host memory, run nchunks x 32 steps reading the thermodynamic scalars back
+    after every launch (the reference prints them at its frame cadence), read
+    the final state back."""
+    import numpy as np
+    import torch
+    n = st.n
+    x, xu, p, F = e.get_state(0)
+    pin = {k: torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for k, a in
+           (("x", x), ("xu", xu), ("p", p), ("F", F))}
+    from activechi4_b200.init import State
+    hs = State(st.L, pin["x"].numpy(), pin["xu"].numpy(), pin["p"].numpy(), st.type, st.act_tag,
+               e.get_directions(0))
+    out = {k: torch.empty_like(v).pin_memory() for k, v in pin.items()}
+    import ctypes as C
+
+    from activechi4_b200 import _abi
+    lib = _abi.lib()
+    ptr = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    e.sync()
+    t0 = time.perf_counter()
+    e.set_state(0, hs)
+    for _ in range(nchunks):
+        e.step(32)
+        e.thermo(0)
+    _abi.check(lib.acg_get_state(e.h, 0, ptr(out["x"]), ptr(out["xu"]), ptr(out["p"]), ptr(out["F"])))
+    wall = time.perf_counter() - t0
+    steps = 32 * nchunks
+    state_bytes = n * (3 * 8 * 3 + 4 + 4)
+    thermo_bytes = C.sizeof(_abi.acg_thermo)
+    return n * steps / wall, state_bytes / steps, (state_bytes + 24 * n + thermo_bytes * nchunks) / steps
+
+
+def run_ours(args):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from activechi4_b200 import build
+    build.build()
+    from activechi4_b200.engine import measure_fp64_peak
+
+    n = args.n
+    nchunks = max(1, math.ceil(args.steps / 32))
+    warm = max(3, args.warmup)
+    e, st = make_engine(n, args.precision, 1000 + rank, local, args.equil)
+    e.step(32 * math.ceil(warm / 32))
+    e.sync()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(local)
+        e.sync()
+
+    barrier()
+    with ClockSampler(local) as clk:
+        dev_ms, launches = e.bench_steps(nchunks, 256 << 20)
+    barrier()
+    t = torch.tensor([dev_ms], dtype=torch.float64, device=f"cuda:{local}")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    steps = 32 * nchunks
+    value = world * n * steps / (max_ms * 1e-3)
+
+    # dominant kernel: pair forces (timed alone, force-only mode, warm L2)
+    t_force = e.time_stage(1, reps=64)
+    t_kick = None
+    t_rebuild = e.time_stage(2, reps=8)
+    peak_gbs, peak_src = measured_peaks()
+    achieved = B_ALG * n / (t_force * 1e-3) / 1e9
+    fp64_peak = measure_fp64_peak(local)
+    fp64_ach = PAIRS_PER_PARTICLE * FLOPS_PER_PAIR * n / (t_force * 1e-3) / 1e12
+    traffic = ncu_traffic()
+    th = e.thermo(0)
+
+    e2e_val, h2d, d2h = e2e_run(e, st, nchunks)
+    if dist is not None:
+        te = torch.tensor([e2e_val], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(te, op=dist.ReduceOp.MIN)
+        e2e_val = float(te.item()) * world
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        kind, cval, csteps, cwall = cpu_run(n, 1, args.cpu_seconds, 10 ** 6)
+        cpu = {"value": cval, "unit": "particle-steps/s", "cores": 1, "kind": kind,
+               "sample": f"{csteps[0]} NVT steps of one N={n} system from a T=0.45 lattice start, "
+                         f"single rank, {cwall:.1f} s"}
+    if rank == 0:
+        line = {
+            "metric": "particle-steps/s",
+            "value": value,
+            "unit": "particle-steps/s",
+            "n_gpus": world,
+            "steps": steps,
+            "warmup": warm,
+            "ms_per_step": max_ms / steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32-pair/f64-state",
+            "data": "synthetic: seeded random lattice melted on the device (T=2.0 then 0.45)",
+            "config": {"workload": f"plain KA active glass, N={n} one system, rho=1.2, T=0.45, f0=1.0, "
+                                   f"tau_p=200 steps, dt=0.005, NHC NVT, {args.precision} pair forces",
+                       "n": n, "systems_per_gpu": 1, "parallelism": f"replicas x{world}",
+                       "l2": "256 MiB write between timed 32-step graph launches (cold L2 each launch)"},
+            "e2e": {"value": e2e_val, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak_gbs, "unit": "GB/s",
+                         "frac": achieved / peak_gbs, "traffic": traffic.get("bytes_per_launch") if traffic else None,
+                         "kernel": "k_force_kick", "peak_source": peak_src,
+                         "alg_bytes_per_particle": B_ALG, "kernel_ms": t_force,
+                         "fp64": {"achieved_tflops": fp64_ach, "peak_tflops_measured": fp64_peak,
+                                  "frac": fp64_ach / fp64_peak,
+                                  "pairs_per_particle": PAIRS_PER_PARTICLE, "flops_per_pair": FLOPS_PER_PAIR}},
+            "stages_ms": {"force": t_force, "rebuild": t_rebuild, "kick_drift": t_kick},
+            "rebuilds": int(th["rebuilds"]),
+            "clocks": clk.summary(),
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    e.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    n = args.n
+    cores = host_cores()
+    kind, value, steps, wall = cpu_run(n, cores, args.cpu_seconds, max(3, args.steps))
+    line = {
+        "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "impl": "reference",
+        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": int(min(steps)),
+        "warmup": 2, "ms_per_step": wall * 1e3 / max(1, min(steps)), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: seeded random lattice at T=0.45",
+        "config": {"workload": f"plain KA active glass, N={n} one system per process, rho=1.2, T=0.45, "
+                               f"f0=1.0, tau_p=200 steps, dt=0.005, NHC NVT, fp64", "n": n,
+                   "parallelism": f"{cores} independent single-rank processes"},
+        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores, "kind": kind,
+                         "sample": f"{cores} processes x {min(steps)}-{max(steps)} NVT steps of N={n}, "
+                                   f"{wall:.1f} s wall"},
+        "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

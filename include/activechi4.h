@@ -1,0 +1,198 @@
+/*
+ * activechi4.h — C ABI of the B200 (sm_100a) MD timestep for the active
+ * Kob-Andersen glass.
+ *
+ * The reference engine (AnoopMut/activeChi4, MDcode/) keeps all state in
+ * process globals and exposes argument-less C routines (MDcode/subroutine.h).
+ * This library keeps the state resident on one GPU behind an opaque handle
+ * that may hold many independent systems ("a batch"); one system is simply a
+ * batch of one.  The reference routines are re-implemented on top of this ABI
+ * in activechi4_b200/legacy/*.c, which a C host program links in place of
+ * MDcode/cell_list+forces.c, MDcode/active.c and the NVT part of
+ * MDcode/time_evolve.c.
+ *
+ * Units and layouts follow the reference: positions are reduced coordinates
+ * (box = unit cube; x in [0,1) wrapped, xu unfolded), momenta and forces are
+ * absolute (unit mass).  Per-particle arrays are interleaved [n][3] doubles in
+ * the caller's particle order; the library reorders internally and always
+ * returns the caller's order.
+ *
+ * Every entry point returns ACG_OK (0) or a negative ACG_ERR_* code; the
+ * message of the last failure on the calling thread is acg_last_error().
+ * Calls on one handle must come from one host thread at a time.
+ */
+#ifndef ACTIVECHI4_H
+#define ACTIVECHI4_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ACG_OK 0
+#define ACG_ERR_INVALID (-1)    /* bad argument or parameter */
+#define ACG_ERR_CUDA (-2)       /* a CUDA runtime call failed */
+#define ACG_ERR_NOMEM (-3)      /* device allocation failed / footprint too large */
+#define ACG_ERR_NONFINITE (-4)  /* a system's kinetic energy became NaN/inf */
+#define ACG_ERR_STATE (-5)      /* call not valid in the handle's current state */
+
+#define ACG_PREC_FP64 0 /* pair forces in FP64 (the reference's arithmetic) */
+#define ACG_PREC_FP32 1 /* pair forces in FP32; positions, velocities, thermostat,
+                           energies and virials stay FP64 */
+
+/* Parameters of one system.  Defaults (acg_params_default) are the
+ * reference's constants: MDcode/global.h:24-58, para_file (MDcode/main.c:410-426). */
+typedef struct acg_params {
+  int n;                  /* particles (N, MDcode/global.h:15) */
+  int nact;               /* active particles; -1 = (int)(0.1*n) (Nact, MDcode/global.h:55) */
+  double L;               /* box length; <= 0 means pow(n/density, 0.33333333) (MDcode/main.c:465) */
+  double density;         /* DENSITY (para_file line 4) */
+  double T;               /* thermostat temperature (para_file line 4) */
+  double f0;              /* active force magnitude (para_file line 6) */
+  int tau_p_steps;        /* direction persistence in steps (TAU_per, MDcode/global.h:58) */
+  double dt;              /* time_step (MDcode/global.h:32) */
+  double skin;            /* Verlet skin (MDcode/global.h:28) */
+  double rebuild_factor;  /* rebuild when factor*maxD^2 > skin^2 (MDcode/time_evolve.c:508 uses 3) */
+  int list_mode;          /* 0: list cut 2.5+skin for all pairs (Cell_cut, global.h:29);
+                             1: list cut 2.5*sigma_ab+skin per type pair */
+  int thermostat;         /* 1: Nose-Hoover chain NVT (AdvanceTimeNVTNoseHoover);
+                             0: NVE velocity Verlet (advance_time_NVEFrog) */
+  int shuffle;            /* 1: re-randomise active directions on the device every
+                             tau_p_steps steps (ShuffleActDirec cadence, MDcode/main.c:245);
+                             0: the caller sets them (acg_set_directions) */
+  int precision;          /* ACG_PREC_FP64 or ACG_PREC_FP32 */
+  int nb_capacity;        /* neighbour-list row capacity; 0 = automatic.  Particles
+                             with more neighbours are served from the cell list
+                             (the reference's MaxNeibs, MDcode/global.h:19, is
+                             unchecked) */
+  uint64_t seed;          /* device direction-shuffle stream */
+} acg_params;
+
+/* Scalars of one system at the last step boundary. */
+typedef struct acg_thermo {
+  double pe;       /* potential energy (peblk, MDcode/cell_list+forces.c:194) */
+  double ke;       /* kinetic energy 0.5*sum p^2 (ke, MDcode/time_evolve.c:520) */
+  double virial;   /* pair virial / 3 (virialblk, MDcode/cell_list+forces.c:220) */
+  double vir_act;  /* active virial (vir_actblk, MDcode/cell_list+forces.c:214) */
+  double inst_T;   /* 2 ke / DOF (MDcode/time_evolve.c:524) */
+  double maxD;     /* max squared displacement since the last rebuild (maxmaxD) */
+  double heff;     /* conserved NHC energy (Heff, MDcode/print.c:85-87) */
+  double eta[3], p_eta[3], q[3]; /* thermostat chain (MDcode/time_evolve.c:476-493) */
+  int64_t step;    /* steps taken (the run() loop index) */
+  int64_t rebuilds;/* cell/neighbour list rebuilds so far */
+  int overflow;    /* particles that overflowed the neighbour-list capacity at the
+                      last rebuild (served from the cell list instead) */
+  int status;      /* 0 or ACG_ERR_NONFINITE */
+} acg_thermo;
+
+typedef struct acg_engine acg_engine;
+
+/* Fill *p with the reference defaults for n particles. */
+int acg_params_default(acg_params *p, int n);
+
+/* Create an engine holding nsys systems (params[0..nsys-1]) on CUDA device
+ * `device`.  Allocates all device memory up front; no allocation happens on
+ * the stepping path.  Replaces the set-up half of main()
+ * (AllocateArrays, SetUpParallel, SetUpCellList: MDcode/Parallel.c:6-106,
+ * 778-809) — there is no domain decomposition, each system lives whole on
+ * the device. */
+int acg_create(const acg_params *params, int nsys, int device, acg_engine **out);
+int acg_destroy(acg_engine *e);
+
+/* Bytes of device memory acg_create would allocate for these systems
+ * (admission control for serving). */
+int acg_footprint(const acg_params *params, int nsys, size_t *bytes);
+
+/* Load one system's particles (caller order).  x: [n][3] wrapped reduced
+ * coordinates; xu: unfolded (NULL = x); p: momenta; type[n]: 0 = A, 1 = B;
+ * act_tag[n]: -1 or the particle's index into the direction arrays.
+ * Replaces BcastInitState / read_restart_state + initialise_restart_state
+ * (MDcode/Parallel.c:618-656, MDcode/main.c:290-334).  Forces, cells and
+ * neighbour lists are rebuilt before the next step. */
+int acg_set_state(acg_engine *e, int sys, const double *x, const double *xu, const double *p,
+                  const int *type, const int *act_tag);
+
+/* Read one system back in the caller's order; any pointer may be NULL.
+ * F are the forces of the last evaluation. */
+int acg_get_state(acg_engine *e, int sys, double *x, double *xu, double *p, double *F);
+
+/* Active directions k[3][nact] = kx, ky, kz in {-1,+1}
+ * (kx/ky/kz, MDcode/active.c:30-41; readActiveDirection :101-122). */
+int acg_set_directions(acg_engine *e, int sys, const int *k);
+int acg_get_directions(acg_engine *e, int sys, int *k);
+
+/* Re-randomise one system's directions now on the device (a uniformly random
+ * permutation per component, keeping the +1/-1 counts): ShuffleActDirec,
+ * MDcode/active.c:45-85. */
+int acg_shuffle_directions(acg_engine *e, int sys);
+
+/* Thermostat chain state (InitialiseNoseHoover, MDcode/time_evolve.c:476-493:
+ * eta = 0, p_eta drawn by the caller).  q follows from T and n. */
+int acg_set_nhc(acg_engine *e, int sys, const double *eta3, const double *p_eta3);
+/* Change a system's thermostat temperature (and with it q). */
+int acg_set_temperature(acg_engine *e, int sys, double T);
+
+/* update_cell_list (MDcode/cell_list+forces.c:58-148) for every system:
+ * counting-sort cell build + neighbour lists. */
+int acg_rebuild(acg_engine *e);
+
+/* calculate_forces (MDcode/cell_list+forces.c:153-227) for every system at
+ * the current positions (rebuilding cells/lists first when needed). */
+int acg_compute_forces(acg_engine *e);
+
+/* Advance every system nsteps steps: for each step the direction shuffle
+ * when due (MDcode/main.c:245-247) then AdvanceTimeNVTNoseHoover
+ * (MDcode/time_evolve.c:495-526) or advance_time_NVEFrog
+ * (MDcode/time_evolve.c:104-171).  Runs as CUDA-graph launches on the
+ * engine's stream; returns after queuing (acg_sync waits). */
+int acg_step(acg_engine *e, int nsteps);
+/* The same steps launched kernel by kernel without a CUDA graph (every
+ * rebuild kernel is launched and skips the systems that need no rebuild). */
+int acg_step_eager(acg_engine *e, int nsteps);
+int acg_sync(acg_engine *e);
+
+int acg_get_thermo(acg_engine *e, int sys, acg_thermo *out);
+
+/* Cell list of the last rebuild: dims[3] cells per side, counts[ncell],
+ * members[n] = particle indices (caller order) per cell, ascending within a
+ * cell (InCellCount / InCell, MDcode/cell_list+forces.c:71-80).  counts and
+ * members may be NULL; returns the number of cells via *ncell. */
+int acg_get_cells(acg_engine *e, int sys, int *dims, int *ncell, int *counts, int *members);
+
+/* Number of systems, particles of one system, and the engine's CUDA stream
+ * (a cudaStream_t) for callers that time or order work around it. */
+int acg_num_systems(acg_engine *e);
+int acg_system_size(acg_engine *e, int sys, int *n, int *nact);
+void *acg_stream(acg_engine *e);
+
+/* Kernel timing for profiling: average device time in ms of `reps`
+ * back-to-back launches of one stage over all systems, timed with CUDA events
+ * on the engine stream.  stage: 0 = kick+drift, 1 = pair forces + kick,
+ * 2 = full cell/neighbour rebuild. */
+int acg_time_stage(acg_engine *e, int stage, int reps, double *ms);
+
+/* Benchmark timing: advance every system nchunks * 32 steps as CUDA-graph
+ * launches of 32 steps, recording CUDA events on the engine stream around each
+ * launch, and write flush_bytes (> L2) with cudaMemsetAsync between launches
+ * (untimed) so that every timed launch starts from a cold L2.  *ms = summed
+ * device time of the launches; *launches = kernels launched inside the timed
+ * launches (counted from the rebuilds they took). */
+int acg_bench_steps(acg_engine *e, int nchunks, size_t flush_bytes, double *ms, int64_t *launches);
+
+/* Measured FP64 FMA throughput of `device` in TFLOP/s (2 flops per FMA):
+ * independent DFMA chains on every SM, timed with CUDA events. */
+int acg_measure_fp64_peak(int device, double *tflops);
+
+/* Launch-configuration knobs (the autotuner sets these). tpp: threads per
+ * particle in the force kernel (1,2,4,8,16,32); block: threads per block. */
+int acg_set_launch(acg_engine *e, int tpp, int block);
+int acg_get_launch(acg_engine *e, int *tpp, int *block);
+
+const char *acg_last_error(void);
+const char *acg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

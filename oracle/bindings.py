@@ -165,6 +165,7 @@ class Oracle(_Common):
         o.set_state(st)
         o.set_nhc(np.zeros(3) if eta is None else eta, np.zeros(3) if p_eta is None else p_eta)
         o.rebuild()
+        o.forces()
         return o
 
     def set_state(self, st):

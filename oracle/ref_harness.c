@@ -10,7 +10,8 @@
  *
  *   ref_setup          state -> sphere[], SetUpParallel/SetUpCellList
  *                      (MDcode/Parallel.c:6-106), CommunicateCoordinates(0),
- *                      update_cell_list (MDcode/cell_list+forces.c:58-148)
+ *                      update_cell_list (MDcode/cell_list+forces.c:58-148),
+ *                      calculate_forces
  *   ref_forces         calculate_forces (MDcode/cell_list+forces.c:153-227)
  *   ref_run            run() loop body (MDcode/main.c:244-248): ShuffleActDirec
  *                      every TAU_per steps + AdvanceTimeNVTNoseHoover
@@ -96,6 +97,7 @@ void ref_setup(double Lbox, double Tset, double f0set, const double *x, const do
   SetUpCellList();
   CommunicateCoordinates(0);
   update_cell_list();
+  calculate_forces(); /* as initialise_restart_state (MDcode/main.c:331-332) */
 }
 
 void ref_set_k(const int *k) {
