@@ -76,21 +76,20 @@ struct View {
   int *id_s, *act_s;
   int *cell_tmp, *perm_u, *perm;
   int *ccount_b, *cfill, *cstart, *ccount;
-  const int2 *tiles_a, *tiles_b, *tiles_l, *tiles_c;
+  const int2 *tiles_a, *tiles_b, *tiles_l, *tiles_c, *tiles_x;
   double4 *part_b;
   unsigned int *counter_a;
   double *stage_d;  // [9n] x, xu, p interleaved per system (original order)
   int *stage_i;     // [2n] type, act
   double *stage_f;  // [3n] forces
-  int ntiles_a, ntiles_b, ntiles_l, ntiles_c, nsys, maxnb;
+  int ntiles_a, ntiles_b, ntiles_l, ntiles_c, ntiles_x, nsys, maxnb;
 };
 
-// minimum image in reduced units, as MDcode/cell_list+forces.c:177-182
-__device__ __forceinline__ double min_image(double d) {
-  if (d < -0.5) d += 1.0;
-  if (d > 0.5) d -= 1.0;
-  return d;
-}
+// minimum image in reduced units.  For |d| < 1.5 (all differences of wrapped
+// coordinates) d - rint(d) performs exactly the reference's operations
+// (MDcode/cell_list+forces.c:177-182): d-1 for d > 0.5, d+1 for d < -0.5, d
+// unchanged otherwise, including d = +-0.5 (round-half-even gives 0).
+__device__ __forceinline__ double min_image(double d) { return d - rint(d); }
 
 // applypbc1 (MDcode/time_evolve.c:15-26) for a displacement far below one box:
 // the while loops run at most once.  A coordinate still outside [0,1) (only

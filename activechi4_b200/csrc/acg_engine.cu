@@ -134,6 +134,7 @@ int plan(const acg_params *params, int nsys, Layout &lay) {
   add(8 * (S / 4 + nsys + 1));            // tiles_b (>= 4 particles per block)
   add(8 * (S / PART_L + nsys + 1));       // tiles_l
   add(8 * (Cn / CELLS_PER_TILE + nsys + 1));
+  add(8 * (Cn + 1));                      // tiles_x (one per cell)
   add(32 * (S / 4 + nsys + 1));           // part_b
   add(64);                                // counters
   add(72 * S);                            // stage_d
@@ -153,7 +154,7 @@ struct acg_engine {
   View v{};
   SysDesc *d_desc = nullptr;
   int tpp = 4, block = 128;
-  int ntiles_a = 0, ntiles_b = 0, ntiles_l = 0, ntiles_c = 0;
+  int ntiles_a = 0, ntiles_b = 0, ntiles_l = 0, ntiles_c = 0, ntiles_x = 0;
   int2 *d_tiles_b = nullptr;
   std::vector<int> dirty;  // systems whose forces/lists must be recomputed
   bool any_dirty = false;
@@ -220,7 +221,8 @@ int launch_rebuild(acg_engine *e) {
   k_cells_scatter<<<e->ntiles_a, BLOCK_R, 0, s>>>(v);
   k_cells_order<<<e->ntiles_c, 32 * CELLS_PER_TILE, 0, s>>>(v);
   k_permute<<<e->ntiles_a, BLOCK_R, 0, s>>>(v);
-  k_build_list<<<e->ntiles_l, BLOCK_L, 0, s>>>(v);
+  if (e->ntiles_x) k_build_list_cells<<<e->ntiles_x, LB_THREADS, 0, s>>>(v);
+  if (e->ntiles_l) k_build_list<<<e->ntiles_l, BLOCK_L, 0, s>>>(v);
   CK(cudaGetLastError());
   return ACG_OK;
 }
@@ -303,9 +305,11 @@ int build_graph(acg_engine *e, int K, cudaGraph_t *gout, cudaGraphExec_t *xout) 
               {(void *)k_cells_scatter, e->ntiles_a, BLOCK_R},
               {(void *)k_cells_order, e->ntiles_c, 32 * CELLS_PER_TILE},
               {(void *)k_permute, e->ntiles_a, BLOCK_R},
+              {(void *)k_build_list_cells, e->ntiles_x, LB_THREADS},
               {(void *)k_build_list, e->ntiles_l, BLOCK_L}};
     cudaGraphNode_t bp = nullptr;
     for (auto &k : rb) {
+      if (k.grid == 0) continue;
       cudaGraphNode_t nn;
       rc = add_kernel(body, bp ? &bp : nullptr, bp ? 1 : 0, &nn, k.fn, k.grid, k.block, va);
       if (rc) return rc;
@@ -426,6 +430,7 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   e->d_tiles_b = (int2 *)take(8 * (S / 4 + nsys + 1));
   int2 *tl = (int2 *)take(8 * (S / PART_L + nsys + 1));
   int2 *tc = (int2 *)take(8 * (Cn / CELLS_PER_TILE + nsys + 1));
+  int2 *tx = (int2 *)take(8 * (Cn + 1));
   v.part_b = (double4 *)take(32 * (S / 4 + nsys + 1));
   v.counter_a = (unsigned int *)take(64);
   v.stage_d = (double *)take(72 * S);
@@ -435,22 +440,28 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   v.tiles_b = e->d_tiles_b;
   v.tiles_l = tl;
   v.tiles_c = tc;
+  v.tiles_x = tx;
   v.nsys = nsys;
   v.maxnb = L.maxnb;
 
-  std::vector<int2> h_a, h_l, h_c;
+  std::vector<int2> h_a, h_l, h_c, h_x;
   for (int r = 0; r < nsys; r++) {
     const SysDesc &d = L.desc[r];
     for (int s = 0; s < d.n; s += BLOCK_A) h_a.push_back(make_int2(r, s));
-    for (int s = 0; s < d.n; s += PART_L) h_l.push_back(make_int2(r, s));
     for (int s = 0; s < d.ncell; s += CELLS_PER_TILE) h_c.push_back(make_int2(r, s));
+    if (d.nc >= 3)
+      for (int c = 0; c < d.ncell; c++) h_x.push_back(make_int2(r, c));
+    else
+      for (int s = 0; s < d.n; s += PART_L) h_l.push_back(make_int2(r, s));
   }
   e->ntiles_a = (int)h_a.size();
   e->ntiles_l = (int)h_l.size();
   e->ntiles_c = (int)h_c.size();
+  e->ntiles_x = (int)h_x.size();
   v.ntiles_a = e->ntiles_a;
   v.ntiles_l = e->ntiles_l;
   v.ntiles_c = e->ntiles_c;
+  v.ntiles_x = e->ntiles_x;
   auto cleanup_fail = [&](int code) {
     acg_destroy(e);
     return code;
@@ -458,10 +469,14 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   if (cudaMemsetAsync(e->arena, 0, L.bytes, e->stream) != cudaSuccess ||
       cudaMemcpyAsync(ta, h_a.data(), h_a.size() * sizeof(int2), cudaMemcpyHostToDevice, e->stream) !=
           cudaSuccess ||
-      cudaMemcpyAsync(tl, h_l.data(), h_l.size() * sizeof(int2), cudaMemcpyHostToDevice, e->stream) !=
-          cudaSuccess ||
       cudaMemcpyAsync(tc, h_c.data(), h_c.size() * sizeof(int2), cudaMemcpyHostToDevice, e->stream) !=
-          cudaSuccess)
+          cudaSuccess ||
+      (!h_x.empty() &&
+       cudaMemcpyAsync(tx, h_x.data(), h_x.size() * sizeof(int2), cudaMemcpyHostToDevice, e->stream) !=
+           cudaSuccess) ||
+      (!h_l.empty() &&
+       cudaMemcpyAsync(tl, h_l.data(), h_l.size() * sizeof(int2), cudaMemcpyHostToDevice, e->stream) !=
+           cudaSuccess))
     return cleanup_fail(fail(ACG_ERR_CUDA, "initial upload failed"));
   std::vector<SysState> st(nsys);
   memset(st.data(), 0, sizeof(SysState) * nsys);

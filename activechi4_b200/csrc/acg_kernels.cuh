@@ -14,8 +14,10 @@
 //     k_cells_order    per cell: order members by original index (stable
 //                      counting sort, so InCell order is reproduced exactly)
 //     k_permute        gather all per-particle arrays into cell order (scratch)
-//     k_build_list     full neighbour list per particle (warp per particle,
-//                      ballot compaction) and copy-back of the scratch arrays
+//     k_build_list_cells  full neighbour lists, one block per cell with the
+//                      27 neighbour cells staged in shared memory (FP32 test,
+//                      ballot compaction) and copy-back of the scratch arrays;
+//                      k_build_list does the same per particle for 2-cell boxes
 //   k_force_kick   pair forces from the list (TPP threads per particle, shuffle
 //                  reduction), active force, second kick v += F dt/2, block
 //                  sums of pe/virial/KE; the last block of each system finishes
@@ -269,7 +271,8 @@ __global__ void __launch_bounds__(BLOCK_R) k_cells_scatter(View v) {
   v.perm_u[d.poff + v.cstart[d.coff + c] + k] = i;
 }
 
-// one warp per cell: order the members by original particle index
+// one warp per cell: order the members by original particle index.  Each
+// lane holds one member; ranks are counted over register shuffles.
 __global__ void __launch_bounds__(32 * CELLS_PER_TILE) k_cells_order(View v) {
   int2 t = v.tiles_c[blockIdx.x];
   const int r = t.x;
@@ -279,13 +282,24 @@ __global__ void __launch_bounds__(32 * CELLS_PER_TILE) k_cells_order(View v) {
   if (c >= d.ncell) return;
   const int m = v.ccount[d.coff + c];
   const int base = d.poff + v.cstart[d.coff + c];
-  for (int a = lane; a < m; a += 32) {
-    int sa = v.perm_u[base + a];
-    int ida = v.id[sa];
+  for (int a0 = 0; a0 < m; a0 += 32) {
+    const int a = a0 + lane;
+    int sa = -1, ida = 0x7fffffff;
+    if (a < m) {
+      sa = v.perm_u[base + a];
+      ida = v.id[sa];
+    }
     int rank = 0;
-    for (int b = 0; b < m; b++) rank += v.id[v.perm_u[base + b]] < ida;
-    v.perm[base + rank] = sa;
-    v.cellof[base + rank] = c;
+    for (int b0 = 0; b0 < m; b0 += 32) {
+      const int b = b0 + lane;
+      const int idb = b < m ? v.id[v.perm_u[base + b]] : 0x7fffffff;
+#pragma unroll 8
+      for (int q = 0; q < 32; q++) rank += __shfl_sync(0xffffffffu, idb, q) < ida;
+    }
+    if (a < m) {
+      v.perm[base + rank] = sa;
+      v.cellof[base + rank] = c;
+    }
   }
 }
 
@@ -316,9 +330,144 @@ __device__ __forceinline__ double lcut2_of(const SysDesc &d, int tsum) {
   return tsum == 0 ? d.lcut2[0] : (tsum == 1 ? d.lcut2[1] : d.lcut2[2]);
 }
 
-// one warp per particle (sorted slot): scan the neighbour cells of its cell
-// and append every slot closer than the list cut (MDcode/cell_list+forces.c:
-// 82-140, here as a full list: each pair appears in both particles' rows)
+__device__ __forceinline__ void copy_back(const View &v, int i) {
+  v.pos[i] = v.pos_s[i];
+  v.ux[i] = v.ux_s[i];
+  v.uy[i] = v.uy_s[i];
+  v.uz[i] = v.uz_s[i];
+  v.ox[i] = v.ux_s[i];
+  v.oy[i] = v.uy_s[i];
+  v.oz[i] = v.uz_s[i];
+  v.vx[i] = v.vx_s[i];
+  v.vy[i] = v.vy_s[i];
+  v.vz[i] = v.vz_s[i];
+  v.fx[i] = v.fx_s[i];
+  v.fy[i] = v.fy_s[i];
+  v.fz[i] = v.fz_s[i];
+  v.id[i] = v.id_s[i];
+  v.act[i] = v.act_s[i];
+}
+
+// Neighbour lists for boxes with >= 3 cells per side: one block per cell.
+// The 27 neighbour cells are staged in shared memory as FP32 coordinates in
+// the frame of the centre cell, each neighbour cell shifted by its periodic
+// image; with >= 3 cells per side and cells no smaller than the list cut that
+// frame gives every pair within the cut its minimum image.  The FP32 test
+// uses a cut enlarged by 1e-5 (relative, on r^2) — far above the FP32 error of
+// coordinates below 9 length units — so the list holds every pair the
+// reference's FP64 test keeps (MDcode/cell_list+forces.c:82-140) plus possibly
+// a few just outside; the force kernel's exact FP64 cut test leaves those out.
+// Rows list each pair for both particles (full list).
+constexpr int LB_THREADS = 128;
+constexpr int STAGE_MAX = 1536;
+constexpr int ICHUNK = 128;
+
+__global__ void __launch_bounds__(LB_THREADS) k_build_list_cells(View v) {
+  __shared__ float4 stg[STAGE_MAX];
+  __shared__ int cnt[ICHUNK];
+  __shared__ int s_start[27], s_pre[28];
+  __shared__ float s_sh[27][3];
+  const int2 t = v.tiles_x[blockIdx.x];
+  const int r = t.x, c = t.y;
+  if (!v.st[r].rebuild) return;
+  const SysDesc &d = v.desc[r];
+  const int nc = d.nc;
+  const int cx = c % nc, cy = (c / nc) % nc, cz = c / (nc * nc);
+  const double L = d.L;
+  const double ox = (cx + 0.5) / nc, oy = (cy + 0.5) / nc, oz = (cz + 0.5) / nc;
+  const int m0 = v.ccount[d.coff + c], s0 = d.poff + v.cstart[d.coff + c];
+  if (threadIdx.x == 0) {
+    int q = 0, pre = 0;
+    for (int dz = -1; dz <= 1; dz++)
+      for (int dy = -1; dy <= 1; dy++)
+        for (int dx = -1; dx <= 1; dx++, q++) {
+          int ix = cx + dx, iy = cy + dy, iz = cz + dz;
+          float shx = ix < 0 ? -1.f : (ix >= nc ? 1.f : 0.f);
+          float shy = iy < 0 ? -1.f : (iy >= nc ? 1.f : 0.f);
+          float shz = iz < 0 ? -1.f : (iz >= nc ? 1.f : 0.f);
+          int c2 = wrap_cell(ix, nc) + wrap_cell(iy, nc) * nc + wrap_cell(iz, nc) * nc * nc;
+          s_start[q] = d.poff + v.cstart[d.coff + c2];
+          s_pre[q] = pre;
+          pre += v.ccount[d.coff + c2];
+          s_sh[q][0] = shx;
+          s_sh[q][1] = shy;
+          s_sh[q][2] = shz;
+        }
+    s_pre[27] = pre;
+  }
+  __syncthreads();
+  const int total = s_pre[27];
+  float lc[3];
+  for (int k = 0; k < 3; k++) lc[k] = (float)(lcut2_of(d, k) * (1.0 + 1e-5));
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int maxnb = v.maxnb;
+  for (int ib = 0; ib < m0; ib += ICHUNK) {
+    const int icount = min(ICHUNK, m0 - ib);
+    for (int k = threadIdx.x; k < icount; k += blockDim.x) cnt[k] = 0;
+    for (int q0 = 0; q0 < total; q0 += STAGE_MAX) {
+      const int qn = min(STAGE_MAX, total - q0);
+      __syncthreads();
+      for (int k = threadIdx.x; k < qn; k += blockDim.x) {
+        const int g = q0 + k;
+        int cc = 0;
+        while (s_pre[cc + 1] <= g) cc++;
+        const int j = s_start[cc] + (g - s_pre[cc]);
+        const double4 pj = v.pos_s[j];
+        float4 f;
+        f.x = (float)(((pj.x + (double)s_sh[cc][0]) - ox) * L);
+        f.y = (float)(((pj.y + (double)s_sh[cc][1]) - oy) * L);
+        f.z = (float)(((pj.z + (double)s_sh[cc][2]) - oz) * L);
+        f.w = __int_as_float(2 * j + (int)pj.w);
+        stg[k] = f;
+      }
+      __syncthreads();
+      for (int ii = warp; ii < icount; ii += nwarps) {
+        const int i = s0 + ib + ii;
+        const double4 pi = v.pos_s[i];
+        const float xi = (float)((pi.x - ox) * L), yi = (float)((pi.y - oy) * L),
+                    zi = (float)((pi.z - oz) * L);
+        const int ti = (int)pi.w;
+        int n = cnt[ii];
+        int *row = v.nbl + (size_t)i * maxnb;
+        for (int k0 = 0; k0 < qn; k0 += 32) {
+          const int k = k0 + lane;
+          bool ok = false;
+          int j = 0;
+          if (k < qn) {
+            const float4 f = stg[k];
+            const int code = __float_as_int(f.w);
+            j = code >> 1;
+            const float dx = xi - f.x, dy = yi - f.y, dz = zi - f.z;
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            const int tt = ti + (code & 1);
+            ok = (j != i) && r2 < (tt == 0 ? lc[0] : (tt == 1 ? lc[1] : lc[2]));
+          }
+          const unsigned int mask = __ballot_sync(0xffffffffu, ok);
+          if (ok) {
+            const int pos = n + __popc(mask & ((1u << lane) - 1u));
+            if (pos < maxnb) row[pos] = j;
+          }
+          n += __popc(mask);
+        }
+        if (lane == 0) cnt[ii] = n;
+      }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < icount; k += blockDim.x) {
+      const int i = s0 + ib + k, n = cnt[k];
+      if (n > maxnb) {
+        v.nbn[i] = -1;  // served from the cell list by the force kernel
+        atomicAdd(&v.st[r].overflow, 1);
+      } else {
+        v.nbn[i] = n;
+      }
+    }
+  }
+  for (int k = threadIdx.x; k < m0; k += blockDim.x) copy_back(v, s0 + k);
+}
+
+// Neighbour lists for boxes with 2 cells per side (one warp per particle, FP64
+// minimum image per pair: the stencil's shifted frame is ambiguous there).
 __global__ void __launch_bounds__(BLOCK_L) k_build_list(View v) {
   int2 t = v.tiles_l[blockIdx.x];
   const int r = t.x;
@@ -366,21 +515,7 @@ __global__ void __launch_bounds__(BLOCK_L) k_build_list(View v) {
     } else {
       v.nbn[i] = cnt;
     }
-    v.pos[i] = pi;
-    v.ux[i] = v.ux_s[i];
-    v.uy[i] = v.uy_s[i];
-    v.uz[i] = v.uz_s[i];
-    v.ox[i] = v.ux_s[i];
-    v.oy[i] = v.uy_s[i];
-    v.oz[i] = v.uz_s[i];
-    v.vx[i] = v.vx_s[i];
-    v.vy[i] = v.vy_s[i];
-    v.vz[i] = v.vz_s[i];
-    v.fx[i] = v.fx_s[i];
-    v.fy[i] = v.fy_s[i];
-    v.fz[i] = v.fz_s[i];
-    v.id[i] = v.id_s[i];
-    v.act[i] = v.act_s[i];
+    copy_back(v, i);
   }
 }
 
@@ -534,13 +669,29 @@ __global__ void __launch_bounds__(512) k_force_kick(View v, int mode) {
     const int ti = (int)pi.w;
     const int nn = v.nbn[i];
     if (nn >= 0) {
-      const int *row = v.nbl + (size_t)i * v.maxnb;
-      for (int k = lane; k < nn; k += TPP) {
-        const double4 pj = v.pos[__ldg(row + k)];
-        if (PREC == 0)
-          pair_fp64(a, pi, ti, pj, L, L2);
-        else
-          pair_fp32(a, pi, ti, pj, L, L2);
+      // four list entries per lane per iteration (one 16-byte load; rows are
+      // 16-byte aligned and padded to maxnb, entries past nn are not used)
+      const int4 *row4 = reinterpret_cast<const int4 *>(v.nbl + (size_t)i * v.maxnb);
+      const int nb4 = (nn + 3) >> 2;
+      for (int b = lane; b < nb4; b += TPP) {
+        const int4 jj = __ldg(row4 + b);
+        const int k0 = 4 * b;
+        const bool v1 = k0 + 1 < nn, v2 = k0 + 2 < nn, v3 = k0 + 3 < nn;
+        const double4 p0 = v.pos[jj.x];
+        const double4 p1 = v1 ? v.pos[jj.y] : pi;
+        const double4 p2 = v2 ? v.pos[jj.z] : pi;
+        const double4 p3 = v3 ? v.pos[jj.w] : pi;
+        if (PREC == 0) {
+          pair_fp64(a, pi, ti, p0, L, L2);
+          if (v1) pair_fp64(a, pi, ti, p1, L, L2);
+          if (v2) pair_fp64(a, pi, ti, p2, L, L2);
+          if (v3) pair_fp64(a, pi, ti, p3, L, L2);
+        } else {
+          pair_fp32(a, pi, ti, p0, L, L2);
+          if (v1) pair_fp32(a, pi, ti, p1, L, L2);
+          if (v2) pair_fp32(a, pi, ti, p2, L, L2);
+          if (v3) pair_fp32(a, pi, ti, p3, L, L2);
+        }
       }
     } else {
       // neighbour-list overflow: scan the cells around the cell of the last

@@ -86,6 +86,7 @@ def test_shuffled_directions_50_steps(cuda_lib, g1000):
     """The reference shuffles at step 0 with its own RNG; the same directions
     handed to the device reproduce its trajectory."""
     e = engine_for(g1000)
+    e.compute_forces()  # initial forces with the pre-shuffle directions, as the reference
     e.set_directions(0, g1000["shf_k"])
     e.step(50)
     _check_traj(e, g1000, "shf_")
