@@ -76,6 +76,8 @@ _SIGS = {
     "acg_get_launch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "acg_bench_steps": (C.c_int, [C.c_void_p, C.c_int, C.c_size_t, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "acg_measure_fp64_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
+    "acg_forces_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                     C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]),
     "acg_last_error": (C.c_char_p, []),
     "acg_version": (C.c_char_p, []),
 }

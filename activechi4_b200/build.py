@@ -14,7 +14,7 @@ CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libactivechi4_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-SOURCES = ["acg_engine.cu"]
+SOURCES = ["acg_engine.cu", "acg_noalloc.cu"]
 HEADERS = ["acg_device.cuh", "acg_kernels.cuh"]
 
 

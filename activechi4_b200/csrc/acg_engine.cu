@@ -146,6 +146,11 @@ int plan(const acg_params *params, int nsys, Layout &lay) {
 
 }  // namespace
 
+namespace acg {
+// lets other translation units of the library report through acg_last_error
+int set_last_error(int code, const std::string &msg) { return fail(code, msg); }
+}  // namespace acg
+
 struct acg_engine {
   int device = 0;
   cudaStream_t stream = nullptr;

@@ -192,6 +192,38 @@ int acg_get_launch(acg_engine *e, int *tpp, int *block);
 const char *acg_last_error(void);
 const char *acg_version(void);
 
+/* ---- allocation-free force evaluation -----------------------------------
+ * No counterpart in the reference: this entry point exists for callers that
+ * cannot allocate device memory — code running inside a framework that owns
+ * all device memory through its own pool, hosts that forbid allocation once a
+ * latency-bounded loop has started, and plug-ins that are only handed device
+ * pointers by their host.  It computes calculate_forces' result (pair forces,
+ * active forces, pe, virial, vir_act) for one system from arrays the caller
+ * already has on the device, and allocates nothing: its intermediates live in
+ * one file-scope device array of ACG_NOALLOC_SCRATCH_BYTES that every GPU
+ * which loads the library holds until the process exits.
+ *
+ * All pointers are device pointers on the current device: x [n][3] wrapped
+ * reduced coordinates, xu [n][3] unfolded (NULL = x, used for vir_act only),
+ * type[n], act_tag[n] (-1 or index into k), k [3][nact]; outputs F [n][3]
+ * and scalars[3] = {pe, virial, vir_act}.  stream is a cudaStream_t (NULL =
+ * the default stream); the call only queues work on it.
+ * Limits: 2 <= n <= ACG_NOALLOC_MAX_N and at most ACG_NOALLOC_MAX_CELLS cells
+ * of side >= 2.85 (cells per side = (int)((int)L / 2.85) >= 2); larger sizes
+ * return ACG_ERR_INVALID with a message.
+ * The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture.  Calls share the array and it keeps the last
+ * call's contents (each call clears what must start at zero); calls that
+ * overlap on the GPU (two streams, or two host threads) race on it and must
+ * be serialised by the caller. */
+#define ACG_NOALLOC_MAX_N 262144
+#define ACG_NOALLOC_MAX_CELLS 32768
+#define ACG_NOALLOC_SCRATCH_BYTES (3u << 20)
+int acg_forces_noalloc(const double *x, const double *xu, const int *type, const int *act_tag,
+                       const int *k, int n, int nact, double L, double f0, double *F,
+                       double *scalars, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
