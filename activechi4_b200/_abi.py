@@ -74,6 +74,7 @@ _SIGS = {
     "acg_time_stage": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)]),
     "acg_set_launch": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "acg_get_launch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "acg_set_group_tpp": (C.c_int, [C.c_void_p, C.c_int]),
     "acg_bench_steps": (C.c_int, [C.c_void_p, C.c_int, C.c_size_t, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "acg_measure_fp64_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
     "acg_forces_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,

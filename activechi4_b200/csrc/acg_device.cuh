@@ -11,7 +11,9 @@
 //     id   : original particle index inside its system
 //     act  : -1 or index into the system's direction array
 //     cellof: cell of the slot at the last rebuild
-//     nbn / nbl : full neighbour list, row-major, `maxnb` entries per slot
+//     nbn / nbl : full neighbour lists, `maxnb` entries per particle: 16-bit
+//            staged indices per cell group (transposed) for boxes with >= 3
+//            cells per side, int32 slot rows for 2-cell boxes
 //   cells           [coff_r, coff_r + ncell_r): cstart (slot offset inside the
 //                   system), ccount
 //   directions      [aoff_r, aoff_r + nact_r): char4 {kx, ky, kz, 0}
@@ -28,6 +30,27 @@ constexpr int PART_L = BLOCK_L / 32;
 constexpr int BLOCK_R = 256;    // per-slot rebuild kernels (tiles of BLOCK_A)
 constexpr int CELLS_PER_TILE = 8;
 constexpr int BLOCK_SCAN = 512;
+constexpr int BLOCK_G = 256;      // threads of the group kernels
+constexpr int MAX_UNION = 64;     // 4 x 4 x 4 union cells of a 2 x 2 x 2 group
+
+// A cell group: up to 2 x 2 x 2 cells (clipped at the box edge) and the union
+// of their neighbour cells, up to 4 x 4 x 4, in which union cell (ux,uy,uz)
+// is box cell lo+u wrapped, with the periodic image shift of that wrap.
+struct GroupGeom {
+  int lo[3], nu[3];
+  double org[3];  // group centre, reduced units
+};
+
+__device__ __forceinline__ void group_geom(int g, int nc, int ng, GroupGeom &G) {
+  const int gc[3] = {g % ng, (g / ng) % ng, g / (ng * ng)};
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const int c0 = 2 * gc[k], c1 = min(c0 + 2, nc);
+    G.lo[k] = c0 - 1;
+    G.nu[k] = (c1 - c0) + 2;
+    G.org[k] = 0.5 * (double)(c0 + c1) / (double)nc;
+  }
+}
 
 // KA pair constants (MDcode/cell_list+forces.c:19-20, MDcode/global.h:26,39-40)
 constexpr double KA_C0 = 0.0162665594880;
@@ -36,9 +59,9 @@ constexpr double KA_RC2 = 6.25;  // (r/sigma)^2 cut
 
 struct SysDesc {
   int n, nact, poff, aoff;
-  int coff, ncell, nc, pad0;
+  int coff, ncell, nc, ng;     // ng: cell groups per side (0: no group path, nc < 3)
   int tile0_b, ntile_b, tau_p, thermostat;
-  int shuffle, list_mode, precision, pad1;
+  int shuffle, list_mode, precision, goff;  // goff: offset of the system's groups
   double L, invL, inv_cell;  // inv_cell: cells per unit reduced length (InvCellSize)
   double T, f0, dt, half_dt, skin2, rebuild_factor, dof;
   double q[NHC_M];
@@ -76,13 +99,15 @@ struct View {
   int *id_s, *act_s;
   int *cell_tmp, *perm_u, *perm;
   int *ccount_b, *cfill, *cstart, *ccount;
-  const int2 *tiles_a, *tiles_b, *tiles_l, *tiles_c, *tiles_x;
+  const int2 *tiles_a, *tiles_b, *tiles_l, *tiles_c, *tiles_g;
+  int *gstart;      // per group: first centre particle (prefix over the system's groups)
   double4 *part_b;
   unsigned int *counter_a;
   double *stage_d;  // [9n] x, xu, p interleaved per system (original order)
   int *stage_i;     // [2n] type, act
   double *stage_f;  // [3n] forces
-  int ntiles_a, ntiles_b, ntiles_l, ntiles_c, ntiles_x, nsys, maxnb;
+  int ntiles_a, ntiles_b, ntiles_l, ntiles_c, ntiles_g, nsys, maxnb;
+  int gcap;         // staged-particle capacity of a cell group (shared memory)
 };
 
 // minimum image in reduced units.  For |d| < 1.5 (all differences of wrapped

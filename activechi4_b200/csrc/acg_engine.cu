@@ -35,7 +35,7 @@ constexpr double TAU_T = 0.20;  // MDcode/time_evolve.c:477
 constexpr int GRAPH_STEPS = 32;
 
 struct Layout {
-  int nsys = 0, nslots = 0, ncells = 0, nact = 0, maxnb = 0;
+  int nsys = 0, nslots = 0, ncells = 0, nact = 0, maxnb = 0, ngroups = 0;
   std::vector<SysDesc> desc;
   size_t bytes = 0;
 };
@@ -104,6 +104,9 @@ int plan(const acg_params *params, int nsys, Layout &lay) {
     d.poff = lay.nslots;
     d.coff = lay.ncells;
     d.aoff = lay.nact;
+    d.ng = d.nc >= 3 ? (d.nc + 1) / 2 : 0;
+    d.goff = lay.ngroups;
+    lay.ngroups += d.ng * d.ng * d.ng;
     lay.nslots += (int)align_up((size_t)d.n, 32);
     lay.ncells += d.ncell;
     lay.nact += d.nact;
@@ -134,8 +137,10 @@ int plan(const acg_params *params, int nsys, Layout &lay) {
   add(8 * (S / 4 + nsys + 1));            // tiles_b (>= 4 particles per block)
   add(8 * (S / PART_L + nsys + 1));       // tiles_l
   add(8 * (Cn / CELLS_PER_TILE + nsys + 1));
-  add(8 * (Cn + 1));                      // tiles_x (one per cell)
-  add(32 * (S / 4 + nsys + 1));           // part_b
+  const size_t Gn = (size_t)lay.ngroups;
+  add(8 * (Gn + 1));                      // tiles_g
+  add(4 * (Gn + 1));                      // gstart
+  add(32 * (Gn + S / 4 + nsys + 1));      // part_b
   add(64);                                // counters
   add(72 * S);                            // stage_d
   add(8 * S);                             // stage_i
@@ -158,8 +163,8 @@ struct acg_engine {
   void *arena = nullptr;
   View v{};
   SysDesc *d_desc = nullptr;
-  int tpp = 4, block = 128;
-  int ntiles_a = 0, ntiles_b = 0, ntiles_l = 0, ntiles_c = 0, ntiles_x = 0;
+  int tpp = 4, block = 128, gtpp = 2;
+  int ntiles_a = 0, ntiles_b = 0, ntiles_l = 0, ntiles_c = 0, ntiles_g = 0;
   int2 *d_tiles_b = nullptr;
   std::vector<int> dirty;  // systems whose forces/lists must be recomputed
   bool any_dirty = false;
@@ -174,7 +179,19 @@ struct acg_engine {
 
 namespace {
 
-using ForceFn = void (*)(View, int);
+using ForceFn = void (*)(View, int, int);
+using GroupFn = void (*)(View, int);
+
+GroupFn group_fn(int gtpp, int prec) {
+  switch (gtpp) {
+    case 1: return prec ? (GroupFn)k_force_groups<1, 1> : (GroupFn)k_force_groups<1, 0>;
+    case 2: return prec ? (GroupFn)k_force_groups<2, 1> : (GroupFn)k_force_groups<2, 0>;
+    case 4: return prec ? (GroupFn)k_force_groups<4, 1> : (GroupFn)k_force_groups<4, 0>;
+  }
+  return nullptr;
+}
+size_t group_smem(int gcap) { return 3 * (size_t)gcap * sizeof(double); }
+size_t list_smem(int gcap) { return (size_t)gcap * sizeof(float4); }
 
 ForceFn force_fn(int tpp, int prec) {
 #define F(T)                                                                     \
@@ -187,20 +204,34 @@ ForceFn force_fn(int tpp, int prec) {
   return nullptr;
 }
 
+// force tiles: one block per cell group for systems with >= 3 cells per
+// side (partials [0, ntiles_g)), block/tpp particles per block for the others
+// (partials [ntiles_g, ntiles_g + ntiles_b))
 int build_tiles_b(acg_engine *e) {
   const int pb = e->block / e->tpp;
   std::vector<int2> tb;
+  int ng_total = 0;
   for (int r = 0; r < e->lay.nsys; r++) {
     SysDesc &d = e->lay.desc[r];
-    d.tile0_b = (int)tb.size();
+    if (d.ng > 0) {
+      d.tile0_b = d.goff;
+      d.ntile_b = d.ng * d.ng * d.ng;
+      ng_total += d.ntile_b;
+    }
+  }
+  for (int r = 0; r < e->lay.nsys; r++) {
+    SysDesc &d = e->lay.desc[r];
+    if (d.ng > 0) continue;
+    d.tile0_b = ng_total + (int)tb.size();
     for (int s = 0; s < d.n; s += pb) tb.push_back(make_int2(r, s));
-    d.ntile_b = (int)tb.size() - d.tile0_b;
+    d.ntile_b = ng_total + (int)tb.size() - d.tile0_b;
   }
   e->ntiles_b = (int)tb.size();
   const size_t cap = e->lay.nslots / 4 + e->lay.nsys + 1;
   if (tb.size() > cap) return fail(ACG_ERR_INVALID, "launch shape needs >= 4 particles per block");
-  CK(cudaMemcpyAsync(e->d_tiles_b, tb.data(), tb.size() * sizeof(int2), cudaMemcpyHostToDevice,
-                     e->stream));
+  if (!tb.empty())
+    CK(cudaMemcpyAsync(e->d_tiles_b, tb.data(), tb.size() * sizeof(int2), cudaMemcpyHostToDevice,
+                       e->stream));
   CK(cudaMemcpyAsync(e->d_desc, e->lay.desc.data(), sizeof(SysDesc) * e->lay.nsys,
                      cudaMemcpyHostToDevice, e->stream));
   e->v.ntiles_b = e->ntiles_b;
@@ -226,15 +257,16 @@ int launch_rebuild(acg_engine *e) {
   k_cells_scatter<<<e->ntiles_a, BLOCK_R, 0, s>>>(v);
   k_cells_order<<<e->ntiles_c, 32 * CELLS_PER_TILE, 0, s>>>(v);
   k_permute<<<e->ntiles_a, BLOCK_R, 0, s>>>(v);
-  if (e->ntiles_x) k_build_list_cells<<<e->ntiles_x, LB_THREADS, 0, s>>>(v);
+  if (e->ntiles_g) k_build_list_groups<<<e->ntiles_g, BLOCK_G, list_smem(v.gcap), s>>>(v);
   if (e->ntiles_l) k_build_list<<<e->ntiles_l, BLOCK_L, 0, s>>>(v);
   CK(cudaGetLastError());
   return ACG_OK;
 }
 
 int launch_force(acg_engine *e, int mode) {
-  ForceFn f = force_fn(e->tpp, e->lay.desc[0].precision);
-  f<<<e->ntiles_b, e->block, 0, e->stream>>>(e->v, mode);
+  const int prec = e->lay.desc[0].precision;
+  if (e->ntiles_g) group_fn(e->gtpp, prec)<<<e->ntiles_g, BLOCK_G, group_smem(e->v.gcap), e->stream>>>(e->v, mode);
+  if (e->ntiles_b) force_fn(e->tpp, prec)<<<e->ntiles_b, e->block, 0, e->stream>>>(e->v, mode, e->ntiles_g);
   CK(cudaGetLastError());
   return ACG_OK;
 }
@@ -268,12 +300,12 @@ int prime(acg_engine *e) {
 
 // ---- graphs ----------------------------------------------------------------
 int add_kernel(cudaGraph_t g, const cudaGraphNode_t *dep, size_t ndep, cudaGraphNode_t *out,
-               void *fn, int grid, int block, void **args) {
+               void *fn, int grid, int block, void **args, size_t smem = 0) {
   cudaKernelNodeParams p = {};
   p.func = fn;
   p.gridDim = dim3(grid);
   p.blockDim = dim3(block);
-  p.sharedMemBytes = 0;
+  p.sharedMemBytes = (unsigned)smem;
   p.kernelParams = args;
   CK(cudaGraphAddKernelNode(out, g, dep, ndep, &p));
   return ACG_OK;
@@ -283,9 +315,11 @@ int build_graph(acg_engine *e, int K, cudaGraph_t *gout, cudaGraphExec_t *xout) 
   cudaGraph_t g;
   CK(cudaGraphCreate(&g, 0));
   View v = e->v;
-  ForceFn ff = force_fn(e->tpp, e->lay.desc[0].precision);
+  const int prec = e->lay.desc[0].precision;
+  ForceFn ff = force_fn(e->tpp, prec);
+  GroupFn gf = group_fn(e->gtpp, prec);
   cudaGraphNode_t prev = nullptr;
-  int mode0 = 0, use_cond = 1;
+  int mode0 = 0, use_cond = 1, tbase = e->ntiles_g;
   for (int s = 0; s < K; s++) {
     cudaGraphConditionalHandle h;
     CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
@@ -305,25 +339,36 @@ int build_graph(acg_engine *e, int K, cudaGraph_t *gout, cudaGraphExec_t *xout) 
     struct {
       void *fn;
       int grid, block;
-    } rb[] = {{(void *)k_cells_count, e->ntiles_a, BLOCK_R},
-              {(void *)k_cells_scan, e->lay.nsys, BLOCK_SCAN},
-              {(void *)k_cells_scatter, e->ntiles_a, BLOCK_R},
-              {(void *)k_cells_order, e->ntiles_c, 32 * CELLS_PER_TILE},
-              {(void *)k_permute, e->ntiles_a, BLOCK_R},
-              {(void *)k_build_list_cells, e->ntiles_x, LB_THREADS},
-              {(void *)k_build_list, e->ntiles_l, BLOCK_L}};
+      size_t smem;
+    } rb[] = {{(void *)k_cells_count, e->ntiles_a, BLOCK_R, 0},
+              {(void *)k_cells_scan, e->lay.nsys, BLOCK_SCAN, 0},
+              {(void *)k_cells_scatter, e->ntiles_a, BLOCK_R, 0},
+              {(void *)k_cells_order, e->ntiles_c, 32 * CELLS_PER_TILE, 0},
+              {(void *)k_permute, e->ntiles_a, BLOCK_R, 0},
+              {(void *)k_build_list_groups, e->ntiles_g, BLOCK_G, list_smem(v.gcap)},
+              {(void *)k_build_list, e->ntiles_l, BLOCK_L, 0}};
     cudaGraphNode_t bp = nullptr;
     for (auto &k : rb) {
       if (k.grid == 0) continue;
       cudaGraphNode_t nn;
-      rc = add_kernel(body, bp ? &bp : nullptr, bp ? 1 : 0, &nn, k.fn, k.grid, k.block, va);
+      rc = add_kernel(body, bp ? &bp : nullptr, bp ? 1 : 0, &nn, k.fn, k.grid, k.block, va, k.smem);
       if (rc) return rc;
       bp = nn;
     }
-    void *ba[] = {&v, &mode0};
-    rc = add_kernel(g, &nc, 1, &nb, (void *)ff, e->ntiles_b, e->block, ba);
-    if (rc) return rc;
-    prev = nb;
+    cudaGraphNode_t last = nc;
+    if (e->ntiles_g) {
+      void *ga[] = {&v, &mode0};
+      rc = add_kernel(g, &last, 1, &nb, (void *)gf, e->ntiles_g, BLOCK_G, ga, group_smem(v.gcap));
+      if (rc) return rc;
+      last = nb;
+    }
+    if (e->ntiles_b) {
+      void *ba[] = {&v, &mode0, &tbase};
+      rc = add_kernel(g, &last, 1, &nb, (void *)ff, e->ntiles_b, e->block, ba);
+      if (rc) return rc;
+      last = nb;
+    }
+    prev = last;
   }
   cudaGraphExec_t x;
   CK(cudaGraphInstantiate(&x, g, 0));
@@ -435,8 +480,10 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   e->d_tiles_b = (int2 *)take(8 * (S / 4 + nsys + 1));
   int2 *tl = (int2 *)take(8 * (S / PART_L + nsys + 1));
   int2 *tc = (int2 *)take(8 * (Cn / CELLS_PER_TILE + nsys + 1));
-  int2 *tx = (int2 *)take(8 * (Cn + 1));
-  v.part_b = (double4 *)take(32 * (S / 4 + nsys + 1));
+  const size_t Gn = (size_t)L.ngroups;
+  int2 *tg = (int2 *)take(8 * (Gn + 1));
+  v.gstart = (int *)take(4 * (Gn + 1));
+  v.part_b = (double4 *)take(32 * (Gn + S / 4 + nsys + 1));
   v.counter_a = (unsigned int *)take(64);
   v.stage_d = (double *)take(72 * S);
   v.stage_i = (int *)take(8 * S);
@@ -445,28 +492,50 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   v.tiles_b = e->d_tiles_b;
   v.tiles_l = tl;
   v.tiles_c = tc;
-  v.tiles_x = tx;
+  v.tiles_g = tg;
   v.nsys = nsys;
   v.maxnb = L.maxnb;
 
-  std::vector<int2> h_a, h_l, h_c, h_x;
+  std::vector<int2> h_a, h_l, h_c, h_g;
   for (int r = 0; r < nsys; r++) {
     const SysDesc &d = L.desc[r];
     for (int s = 0; s < d.n; s += BLOCK_A) h_a.push_back(make_int2(r, s));
     for (int s = 0; s < d.ncell; s += CELLS_PER_TILE) h_c.push_back(make_int2(r, s));
-    if (d.nc >= 3)
-      for (int c = 0; c < d.ncell; c++) h_x.push_back(make_int2(r, c));
+    if (d.ng > 0)
+      for (int g = 0; g < d.ng * d.ng * d.ng; g++) h_g.push_back(make_int2(r, g));
     else
       for (int s = 0; s < d.n; s += PART_L) h_l.push_back(make_int2(r, s));
   }
   e->ntiles_a = (int)h_a.size();
   e->ntiles_l = (int)h_l.size();
   e->ntiles_c = (int)h_c.size();
-  e->ntiles_x = (int)h_x.size();
+  e->ntiles_g = (int)h_g.size();
   v.ntiles_a = e->ntiles_a;
   v.ntiles_l = e->ntiles_l;
   v.ntiles_c = e->ntiles_c;
-  v.ntiles_x = e->ntiles_x;
+  v.ntiles_g = e->ntiles_g;
+  // staged-particle capacity of a cell group: 1.4x the mean union (4^3 cells)
+  // of the densest system plus margin; a group above it uses the cell scan
+  {
+    double mean_u = 0;
+    for (int r = 0; r < nsys; r++)
+      if (L.desc[r].ng > 0) mean_u = std::max(mean_u, 64.0 * L.desc[r].n / (double)L.desc[r].ncell);
+    v.gcap = (int)align_up((size_t)(1.2 * mean_u + 64.0), 64);
+    v.gcap = std::min(v.gcap, 8192);
+  }
+  bool attr_ok = true;
+  for (int gt : {1, 2, 4})
+    for (int pr : {0, 1})
+      attr_ok = attr_ok && cudaFuncSetAttribute((const void *)group_fn(gt, pr),
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)group_smem(v.gcap)) == cudaSuccess;
+  attr_ok = attr_ok && cudaFuncSetAttribute((const void *)k_build_list_groups,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)list_smem(v.gcap)) == cudaSuccess;
+  if (!attr_ok) {
+    acg_destroy(e);
+    return fail(ACG_ERR_CUDA, "cudaFuncSetAttribute (group kernels' shared memory) failed");
+  }
   auto cleanup_fail = [&](int code) {
     acg_destroy(e);
     return code;
@@ -476,8 +545,8 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
           cudaSuccess ||
       cudaMemcpyAsync(tc, h_c.data(), h_c.size() * sizeof(int2), cudaMemcpyHostToDevice, e->stream) !=
           cudaSuccess ||
-      (!h_x.empty() &&
-       cudaMemcpyAsync(tx, h_x.data(), h_x.size() * sizeof(int2), cudaMemcpyHostToDevice, e->stream) !=
+      (!h_g.empty() &&
+       cudaMemcpyAsync(tg, h_g.data(), h_g.size() * sizeof(int2), cudaMemcpyHostToDevice, e->stream) !=
            cudaSuccess) ||
       (!h_l.empty() &&
        cudaMemcpyAsync(tl, h_l.data(), h_l.size() * sizeof(int2), cudaMemcpyHostToDevice, e->stream) !=
@@ -799,6 +868,16 @@ int acg_set_launch(acg_engine *e, int tpp, int block) {
   int rc = build_tiles_b(e);
   if (rc) return rc;
   CK(cudaStreamSynchronize(e->stream));
+  return ACG_OK;
+}
+
+int acg_set_group_tpp(acg_engine *e, int gtpp) {
+  if (!e) return fail(ACG_ERR_INVALID, "null engine");
+  if (!group_fn(gtpp, 0)) return fail(ACG_ERR_INVALID, "group threads per particle must be 1, 2 or 4");
+  CK(cudaSetDevice(e->device));
+  CK(cudaStreamSynchronize(e->stream));
+  e->gtpp = gtpp;
+  drop_graphs(e);
   return ACG_OK;
 }
 

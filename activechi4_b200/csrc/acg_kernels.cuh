@@ -14,12 +14,15 @@
 //     k_cells_order    per cell: order members by original index (stable
 //                      counting sort, so InCell order is reproduced exactly)
 //     k_permute        gather all per-particle arrays into cell order (scratch)
-//     k_build_list_cells  full neighbour lists, one block per cell with the
-//                      27 neighbour cells staged in shared memory (FP32 test,
-//                      ballot compaction) and copy-back of the scratch arrays;
-//                      k_build_list does the same per particle for 2-cell boxes
-//   k_force_kick   pair forces from the list (TPP threads per particle, shuffle
-//                  reduction), active force, second kick v += F dt/2, block
+//     k_build_list_groups full neighbour lists, one block per group of 2x2x2
+//                      cells with the union of their neighbour cells staged in
+//                      shared memory (FP32 test, ballot compaction; 16-bit
+//                      staged indices) and copy-back of the scratch arrays;
+//                      k_build_list: int32 lists per particle for 2-cell boxes
+//   k_force_groups pair forces from the 16-bit lists against the staged union
+//                  (one thread per particle; k_force_kick: TPP threads per
+//                  particle from int32 lists for 2-cell boxes), active force,
+//                  second kick v += F dt/2, block
 //                  sums of pe/virial/KE; the last block of each system finishes
 //                  the sums in a fixed order and runs the thermostat chain
 //                  (U4 U3 U4) for the end of this step and the first half of
@@ -256,6 +259,39 @@ __global__ void __launch_bounds__(BLOCK_SCAN) k_cells_scan(View v) {
     st.rebuilds += 1;
     st.overflow = 0;
   }
+  if (d.ng > 0) {
+    // first centre particle of every cell group (groups in index order):
+    // per-thread chunks of groups, then the same block scan
+    __syncthreads();
+    const int ng = d.ng, nc_ = d.nc, ngr = ng * ng * ng;
+    const int gch = (ngr + B - 1) / B;
+    const int g0 = min(threadIdx.x * gch, ngr), g1 = min(g0 + gch, ngr);
+    int gsum = 0;
+    for (int g = g0; g < g1; g++) {
+      const int gx = g % ng, gy = (g / ng) % ng, gz = g / (ng * ng);
+      for (int cz = 2 * gz; cz < min(2 * gz + 2, nc_); cz++)
+        for (int cy = 2 * gy; cy < min(2 * gy + 2, nc_); cy++)
+          for (int cx = 2 * gx; cx < min(2 * gx + 2, nc_); cx++)
+            gsum += v.ccount[d.coff + cx + cy * nc_ + cz * nc_ * nc_];
+    }
+    sh[threadIdx.x] = gsum;
+    __syncthreads();
+    for (int o = 1; o < B; o <<= 1) {
+      int x = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
+      __syncthreads();
+      sh[threadIdx.x] += x;
+      __syncthreads();
+    }
+    int grun = sh[threadIdx.x] - gsum;
+    for (int g = g0; g < g1; g++) {
+      v.gstart[d.goff + g] = grun;
+      const int gx = g % ng, gy = (g / ng) % ng, gz = g / (ng * ng);
+      for (int cz = 2 * gz; cz < min(2 * gz + 2, nc_); cz++)
+        for (int cy = 2 * gy; cy < min(2 * gy + 2, nc_); cy++)
+          for (int cx = 2 * gx; cx < min(2 * gx + 2, nc_); cx++)
+            grun += v.ccount[d.coff + cx + cy * nc_ + cz * nc_ * nc_];
+    }
+  }
 }
 
 __global__ void __launch_bounds__(BLOCK_R) k_cells_scatter(View v) {
@@ -346,124 +382,6 @@ __device__ __forceinline__ void copy_back(const View &v, int i) {
   v.fz[i] = v.fz_s[i];
   v.id[i] = v.id_s[i];
   v.act[i] = v.act_s[i];
-}
-
-// Neighbour lists for boxes with >= 3 cells per side: one block per cell.
-// The 27 neighbour cells are staged in shared memory as FP32 coordinates in
-// the frame of the centre cell, each neighbour cell shifted by its periodic
-// image; with >= 3 cells per side and cells no smaller than the list cut that
-// frame gives every pair within the cut its minimum image.  The FP32 test
-// uses a cut enlarged by 1e-5 (relative, on r^2) — far above the FP32 error of
-// coordinates below 9 length units — so the list holds every pair the
-// reference's FP64 test keeps (MDcode/cell_list+forces.c:82-140) plus possibly
-// a few just outside; the force kernel's exact FP64 cut test leaves those out.
-// Rows list each pair for both particles (full list).
-constexpr int LB_THREADS = 128;
-constexpr int STAGE_MAX = 1536;
-constexpr int ICHUNK = 128;
-
-__global__ void __launch_bounds__(LB_THREADS) k_build_list_cells(View v) {
-  __shared__ float4 stg[STAGE_MAX];
-  __shared__ int cnt[ICHUNK];
-  __shared__ int s_start[27], s_pre[28];
-  __shared__ float s_sh[27][3];
-  const int2 t = v.tiles_x[blockIdx.x];
-  const int r = t.x, c = t.y;
-  if (!v.st[r].rebuild) return;
-  const SysDesc &d = v.desc[r];
-  const int nc = d.nc;
-  const int cx = c % nc, cy = (c / nc) % nc, cz = c / (nc * nc);
-  const double L = d.L;
-  const double ox = (cx + 0.5) / nc, oy = (cy + 0.5) / nc, oz = (cz + 0.5) / nc;
-  const int m0 = v.ccount[d.coff + c], s0 = d.poff + v.cstart[d.coff + c];
-  if (threadIdx.x == 0) {
-    int q = 0, pre = 0;
-    for (int dz = -1; dz <= 1; dz++)
-      for (int dy = -1; dy <= 1; dy++)
-        for (int dx = -1; dx <= 1; dx++, q++) {
-          int ix = cx + dx, iy = cy + dy, iz = cz + dz;
-          float shx = ix < 0 ? -1.f : (ix >= nc ? 1.f : 0.f);
-          float shy = iy < 0 ? -1.f : (iy >= nc ? 1.f : 0.f);
-          float shz = iz < 0 ? -1.f : (iz >= nc ? 1.f : 0.f);
-          int c2 = wrap_cell(ix, nc) + wrap_cell(iy, nc) * nc + wrap_cell(iz, nc) * nc * nc;
-          s_start[q] = d.poff + v.cstart[d.coff + c2];
-          s_pre[q] = pre;
-          pre += v.ccount[d.coff + c2];
-          s_sh[q][0] = shx;
-          s_sh[q][1] = shy;
-          s_sh[q][2] = shz;
-        }
-    s_pre[27] = pre;
-  }
-  __syncthreads();
-  const int total = s_pre[27];
-  float lc[3];
-  for (int k = 0; k < 3; k++) lc[k] = (float)(lcut2_of(d, k) * (1.0 + 1e-5));
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const int maxnb = v.maxnb;
-  for (int ib = 0; ib < m0; ib += ICHUNK) {
-    const int icount = min(ICHUNK, m0 - ib);
-    for (int k = threadIdx.x; k < icount; k += blockDim.x) cnt[k] = 0;
-    for (int q0 = 0; q0 < total; q0 += STAGE_MAX) {
-      const int qn = min(STAGE_MAX, total - q0);
-      __syncthreads();
-      for (int k = threadIdx.x; k < qn; k += blockDim.x) {
-        const int g = q0 + k;
-        int cc = 0;
-        while (s_pre[cc + 1] <= g) cc++;
-        const int j = s_start[cc] + (g - s_pre[cc]);
-        const double4 pj = v.pos_s[j];
-        float4 f;
-        f.x = (float)(((pj.x + (double)s_sh[cc][0]) - ox) * L);
-        f.y = (float)(((pj.y + (double)s_sh[cc][1]) - oy) * L);
-        f.z = (float)(((pj.z + (double)s_sh[cc][2]) - oz) * L);
-        f.w = __int_as_float(2 * j + (int)pj.w);
-        stg[k] = f;
-      }
-      __syncthreads();
-      for (int ii = warp; ii < icount; ii += nwarps) {
-        const int i = s0 + ib + ii;
-        const double4 pi = v.pos_s[i];
-        const float xi = (float)((pi.x - ox) * L), yi = (float)((pi.y - oy) * L),
-                    zi = (float)((pi.z - oz) * L);
-        const int ti = (int)pi.w;
-        int n = cnt[ii];
-        int *row = v.nbl + (size_t)i * maxnb;
-        for (int k0 = 0; k0 < qn; k0 += 32) {
-          const int k = k0 + lane;
-          bool ok = false;
-          int j = 0;
-          if (k < qn) {
-            const float4 f = stg[k];
-            const int code = __float_as_int(f.w);
-            j = code >> 1;
-            const float dx = xi - f.x, dy = yi - f.y, dz = zi - f.z;
-            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            const int tt = ti + (code & 1);
-            ok = (j != i) && r2 < (tt == 0 ? lc[0] : (tt == 1 ? lc[1] : lc[2]));
-          }
-          const unsigned int mask = __ballot_sync(0xffffffffu, ok);
-          if (ok) {
-            const int pos = n + __popc(mask & ((1u << lane) - 1u));
-            if (pos < maxnb) row[pos] = j;
-          }
-          n += __popc(mask);
-        }
-        if (lane == 0) cnt[ii] = n;
-      }
-    }
-    __syncthreads();
-    for (int k = threadIdx.x; k < icount; k += blockDim.x) {
-      const int i = s0 + ib + k, n = cnt[k];
-      if (n > maxnb) {
-        v.nbn[i] = -1;  // served from the cell list by the force kernel
-        atomicAdd(&v.st[r].overflow, 1);
-      } else {
-        v.nbn[i] = n;
-      }
-    }
-  }
-  for (int k = threadIdx.x; k < m0; k += blockDim.x) copy_back(v, s0 + k);
 }
 
 // Neighbour lists for boxes with 2 cells per side (one warp per particle, FP64
@@ -650,7 +568,7 @@ __device__ void finalize_system(const View &v, int r, int mode) {
 // applied, thermostat first half recomputed); 2 = forces only, velocities and
 // thermostat untouched (calculate_forces)
 template <int TPP, int PREC>
-__global__ void __launch_bounds__(512) k_force_kick(View v, int mode) {
+__global__ void __launch_bounds__(512) k_force_kick(View v, int mode, int tile_base) {
   __shared__ double sh[32];
   __shared__ int s_last;
   const int2 t = v.tiles_b[blockIdx.x];
@@ -761,6 +679,433 @@ __global__ void __launch_bounds__(512) k_force_kick(View v, int mode) {
     ke = px * px + py * py + pz * pz;
     pe = a.pe;
     vir = a.vir;
+  }
+  pe = block_sum_dyn(pe, sh);
+  vir = block_sum_dyn(vir, sh);
+  ke = block_sum_dyn(ke, sh);
+  va = block_sum_dyn(va, sh);
+  if (threadIdx.x == 0) {
+    v.part_b[tile_base + blockIdx.x] = make_double4(pe, vir, ke, va);
+    __threadfence();
+    s_last = atomicAdd(&st.counter_b, 1u) == (unsigned)(d.ntile_b - 1);
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  finalize_system(v, r, mode);
+}
+
+// ---------------------------------------------------------------------------
+// Cell-group kernels (boxes with >= 3 cells per side).  One block per group
+// of up to 2 x 2 x 2 cells.  The union of the group cells' neighbour cells
+// (up to 4 x 4 x 4) is staged in shared memory in the group's frame: each
+// union cell is shifted by its periodic image, so every pair within the cut
+// has its minimum image without a per-pair test (cells are at least as wide
+// as the list cut and there are >= 3 per side).  Neighbour lists hold 16-bit
+// staged indices (bit 15: the neighbour's type), stored per group transposed
+// (entry k of centre particle t at k*M + t) so a warp's loads are contiguous.
+struct GroupStage {
+  int nU, nC, Q, M;
+  int ustart[MAX_UNION];     // first slot of each union cell
+  int upre[MAX_UNION + 1];   // staged offset of each union cell
+  int ushift[MAX_UNION];     // periodic image shifts, 2 bits per dimension
+  double ucen[3][MAX_UNION]; // centre of each union cell's box cell, reduced units
+  int cu[8];                 // union index of each centre cell
+  int cpre[9];               // centre offset of each centre cell
+};
+
+__device__ void group_prologue(const View &v, const SysDesc &d, const GroupGeom &G, GroupStage &S) {
+  const int nc = d.nc;
+  const int nux = G.nu[0], nuy = G.nu[1], nuz = G.nu[2];
+  const int nU = nux * nuy * nuz;
+  __shared__ int cnt_u[MAX_UNION];
+  if (threadIdx.x < nU) {
+    const int t = threadIdx.x;
+    const int u[3] = {t % nux, (t / nux) % nuy, t / (nux * nuy)};
+    int c = 0, mul = 1, sh = 0;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const int ci = G.lo[k] + u[k];
+      const int s = ci < 0 ? -1 : (ci >= nc ? 1 : 0);
+      const int cw = wrap_cell(ci, nc);
+      c += cw * mul;
+      mul *= nc;
+      sh |= (s + 1) << (2 * k);
+      S.ucen[k][t] = ((double)cw + 0.5) / (double)nc;
+    }
+    S.ustart[t] = d.poff + v.cstart[d.coff + c];
+    cnt_u[t] = v.ccount[d.coff + c];
+    S.ushift[t] = sh;
+  }
+  __syncthreads();
+  // inclusive scan of the (<= 64) union-cell counts over the first two warps
+  // (every thread of the block reaches every barrier below)
+  __shared__ int wtot;
+  int x = 0;
+  if (threadIdx.x < 64) {
+    const int l = threadIdx.x & 31;
+    x = threadIdx.x < nU ? cnt_u[threadIdx.x] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (l >= o) x += y;
+    }
+    if (threadIdx.x == 31) wtot = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < 64) {
+    const int incl = x + (threadIdx.x >= 32 ? wtot : 0);
+    if (threadIdx.x < nU) S.upre[threadIdx.x + 1] = incl;
+    if (threadIdx.x == 0) S.upre[0] = 0;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    S.Q = S.upre[nU];
+    S.nU = nU;
+    int k = 0, m = 0;
+    for (int uz = 1; uz <= nuz - 2; uz++)
+      for (int uy = 1; uy <= nuy - 2; uy++)
+        for (int ux = 1; ux <= nux - 2; ux++) {
+          const int t = ux + uy * nux + uz * nux * nuy;
+          S.cu[k] = t;
+          S.cpre[k] = m;
+          m += cnt_u[t];
+          k++;
+        }
+    S.cpre[k] = m;
+    S.nC = k;
+    S.M = m;
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ double shift_of(int code, int k) { return (double)(((code >> (2 * k)) & 3) - 1); }
+
+// staged coordinate of a particle of union cell u along dimension k: the
+// image of its wrapped coordinate nearest to its cell's centre (a particle that
+// crossed the box edge since the rebuild keeps a continuous coordinate; it has
+// moved far less than half a box), plus the union cell's image shift, relative
+// to the group centre, in absolute units
+__device__ __forceinline__ double staged_coord(const GroupStage &S, const GroupGeom &G, int u, int k,
+                                               double x, double L) {
+  const double img = x + rint(S.ucen[k][u] - x);
+  return ((img + shift_of(S.ushift[u], k)) - G.org[k]) * L;
+}
+
+// centre particle t -> (centre cell k, slot, staged index)
+__device__ __forceinline__ void group_centre(const GroupStage &S, int t, int &k, int &slot, int &qself) {
+  k = 0;
+  while (S.cpre[k + 1] <= t) k++;
+  const int w = t - S.cpre[k];
+  slot = S.ustart[S.cu[k]] + w;
+  qself = S.upre[S.cu[k]] + w;
+}
+
+__device__ __forceinline__ uint16_t *group_list(const View &v, const SysDesc &d, int g) {
+  return reinterpret_cast<uint16_t *>(v.nbl) + 2 * (size_t)d.poff * v.maxnb +
+         (size_t)v.gstart[d.goff + g] * v.maxnb;
+}
+
+// list entry k of centre particle t, chunks of four entries per particle
+// (entry k at ((k/4)*M + t)*4 + k%4): the force kernel reads four entries with
+// one 8-byte load and a warp's loads are contiguous
+__device__ __forceinline__ size_t group_entry(int k, int t, int M) {
+  return ((size_t)(k >> 2) * M + t) * 4 + (k & 3);
+}
+
+// one warp per centre cell, one lane per particle of that cell: every lane
+// tests the same staged candidate (a shared-memory broadcast)
+__global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
+  extern __shared__ float4 stg[];
+  __shared__ GroupStage S;
+  const int2 tile = v.tiles_g[blockIdx.x];
+  const int r = tile.x, g = tile.y;
+  if (!v.st[r].rebuild) return;
+  const SysDesc &d = v.desc[r];
+  GroupGeom G;
+  group_geom(g, d.nc, d.ng, G);
+  group_prologue(v, d, G, S);
+  const int Q = S.Q, M = S.M, nux = G.nu[0], nuy = G.nu[1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int maxnb = v.maxnb;
+  if (Q <= v.gcap) {
+    const double L = d.L;
+    for (int u = warp; u < S.nU; u += nwarps) {
+      const int q0 = S.upre[u], m = S.upre[u + 1] - q0, j0 = S.ustart[u];
+      for (int k = lane; k < m; k += 32) {
+        const double4 p = v.pos_s[j0 + k];
+        float4 f;
+        f.x = (float)staged_coord(S, G, u, 0, p.x, L);
+        f.y = (float)staged_coord(S, G, u, 1, p.y, L);
+        f.z = (float)staged_coord(S, G, u, 2, p.z, L);
+        f.w = __int_as_float((int)p.w);
+        stg[q0 + k] = f;
+      }
+    }
+    __syncthreads();
+    float lc[3];
+    for (int k = 0; k < 3; k++) lc[k] = (float)(lcut2_of(d, k) * (1.0 + 1e-5));
+    uint16_t *lst = group_list(v, d, g);
+    for (int kc = warp; kc < S.nC; kc += nwarps) {
+      const int cu = S.cu[kc];
+      const int m = S.cpre[kc + 1] - S.cpre[kc];
+      const int ux = cu % nux, uy = (cu / nux) % nuy, uz = cu / (nux * nuy);
+      for (int w0 = 0; w0 < m; w0 += 32) {
+        const int w = w0 + lane;
+        const bool valid = w < m;
+        const int t = S.cpre[kc] + w, qs = S.upre[cu] + w;
+        const float4 fi = valid ? stg[qs] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const int ti = __float_as_int(fi.w);
+        int n = 0;
+        for (int dz = -1; dz <= 1; dz++)
+          for (int dy = -1; dy <= 1; dy++)
+            for (int dx = -1; dx <= 1; dx++) {
+              const int u2 = (ux + dx) + (uy + dy) * nux + (uz + dz) * nux * nuy;
+              const int q1 = S.upre[u2 + 1];
+              // four candidates per iteration: independent tests, then appends
+              for (int q = S.upre[u2]; q < q1; q += 4) {
+                int code[4];
+                bool ok[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                  const int qq = q + u;
+                  const float4 fj = stg[qq < q1 ? qq : q];
+                  const int tj = __float_as_int(fj.w);
+                  const float ex = fi.x - fj.x, ey = fi.y - fj.y, ez = fi.z - fj.z;
+                  const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+                  const int tt = ti + tj;
+                  ok[u] = valid && qq < q1 && qq != qs && r2 < (tt == 0 ? lc[0] : (tt == 1 ? lc[1] : lc[2]));
+                  code[u] = qq | (tj << 15);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+                  if (ok[u]) {
+                    if (n < maxnb) lst[group_entry(n, t, M)] = (uint16_t)code[u];
+                    n++;
+                  }
+              }
+            }
+        if (valid) {
+          const int i = S.ustart[cu] + w;
+          if (n > maxnb) {
+            v.nbn[i] = -1;
+            atomicAdd(&v.st[r].overflow, 1);
+          } else {
+            v.nbn[i] = n;
+          }
+        }
+      }
+    }
+  } else {
+    // the union does not fit in shared memory: the force kernel scans cells
+    for (int t = threadIdx.x; t < M; t += blockDim.x) {
+      int kc, i, qs;
+      group_centre(S, t, kc, i, qs);
+      v.nbn[i] = -1;
+      atomicAdd(&v.st[r].overflow, 1);
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < M; t += blockDim.x) {
+    int kc, i, qs;
+    group_centre(S, t, kc, i, qs);
+    copy_back(v, i);
+  }
+}
+
+// pair term on a separation already in the minimum image, absolute units
+template <int PREC>
+__device__ __forceinline__ void pair_rel(PairAcc &a, double dx, double dy, double dz, int tp) {
+  const double is2 = tp == 0 ? 1.0 : (tp == 1 ? 1.5625 : 1.0 / (0.88 * 0.88));
+  const double e4 = tp == 0 ? 4.0 : (tp == 1 ? 6.0 : 2.0);
+  if (PREC == 0) {
+    const double dr2 = dx * dx + dy * dy + dz * dz;
+    const double rs2 = dr2 * is2;
+    if (rs2 < KA_RC2) {
+      const double s2 = 1.0 / rs2;
+      const double s6 = s2 * s2 * s2;
+      a.pe += e4 * ((s6 * (s6 - 1.0)) + KA_C0 + KA_C2 * rs2);
+      const double g = (2.0 * e4 * is2) * (6.0 * s6 * (s6 - 0.5) * s2 - KA_C2);
+      a.fx += g * dx;
+      a.fy += g * dy;
+      a.fz += g * dz;
+      a.vir += g * dr2;
+    }
+  } else {
+    const float fx = (float)dx, fy = (float)dy, fz = (float)dz;
+    const float dr2 = fx * fx + fy * fy + fz * fz;
+    const float fis2 = (float)is2;
+    const float rs2 = dr2 * fis2;
+    if (rs2 < (float)KA_RC2) {
+      const float fe4 = (float)e4;
+      const float s2 = __frcp_rn(rs2);
+      const float s6 = s2 * s2 * s2;
+      a.pe += (double)(fe4 * ((s6 * (s6 - 1.0f)) + (float)KA_C0 + (float)KA_C2 * rs2));
+      const float g = (2.0f * fe4 * fis2) * (6.0f * s6 * (s6 - 0.5f) * s2 - (float)KA_C2);
+      a.fx += (double)(g * fx);
+      a.fy += (double)(g * fy);
+      a.fz += (double)(g * fz);
+      a.vir += (double)(g * dr2);
+    }
+  }
+}
+
+template <int TPP, int PREC>
+__global__ void __launch_bounds__(BLOCK_G) k_force_groups(View v, int mode) {
+  extern __shared__ double gsm[];
+  double *sx = gsm, *sy = gsm + v.gcap, *sz = gsm + 2 * v.gcap;
+  __shared__ GroupStage S;
+  __shared__ double sh[32];
+  __shared__ int s_last;
+  const int2 tile = v.tiles_g[blockIdx.x];
+  const int r = tile.x, g = tile.y;
+  SysState &st = v.st[r];
+  if (mode == 1 && !st.prime) return;
+  const SysDesc &d = v.desc[r];
+  GroupGeom G;
+  group_geom(g, d.nc, d.ng, G);
+  group_prologue(v, d, G, S);
+  const int Q = S.Q, M = S.M;
+  const bool staged = Q <= v.gcap;
+  const double L = d.L;
+  if (staged) {
+    // one warp per union cell: coalesced loads, no search
+    const int wl = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int u = threadIdx.x >> 5; u < S.nU; u += nw) {
+      const int q0 = S.upre[u], m = S.upre[u + 1] - q0, j0 = S.ustart[u];
+      for (int k = wl; k < m; k += 32) {
+        const double4 p = v.pos[j0 + k];
+        sx[q0 + k] = staged_coord(S, G, u, 0, p.x, L);
+        sy[q0 + k] = staged_coord(S, G, u, 1, p.y, L);
+        sz[q0 + k] = staged_coord(S, G, u, 2, p.z, L);
+      }
+    }
+  }
+  __syncthreads();
+  const uint16_t *lst = staged ? group_list(v, d, g) : nullptr;
+  double pe = 0.0, vir = 0.0, ke = 0.0, va = 0.0;
+  const int lane = threadIdx.x % TPP, nper = blockDim.x / TPP;
+  // rounds over the centre particles: TPP threads per particle, all threads of
+  // a round take part in the shuffle reduction
+  for (int t0 = 0; t0 < M; t0 += nper) {
+    const int t = t0 + threadIdx.x / TPP;
+    const bool valid = t < M;
+    int kc = 0, i = 0, qs = 0;
+    if (valid) group_centre(S, t, kc, i, qs);
+    const double4 pi = valid ? v.pos[i] : make_double4(0, 0, 0, 0);
+    const int ti = (int)pi.w;
+    const int nn = valid ? v.nbn[i] : 0;
+    // per-particle inputs of the epilogue, loaded before the pair loop
+    const int ai = valid && lane == 0 ? v.act[i] : -1;
+    double vx0 = 0.0, vy0 = 0.0, vz0 = 0.0, uxi = 0.0, uyi = 0.0, uzi = 0.0;
+    if (valid && lane == 0) {
+      if (mode != 2) {
+        vx0 = v.vx[i];
+        vy0 = v.vy[i];
+        vz0 = v.vz[i];
+      }
+      if (ai >= 0) {
+        uxi = v.ux[i];
+        uyi = v.uy[i];
+        uzi = v.uz[i];
+      }
+    }
+    PairAcc a = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (valid && staged && nn >= 0) {
+      const double xi = sx[qs], yi = sy[qs], zi = sz[qs];
+      const int nch = (nn + 3) >> 2;
+      const uint2 *lp = reinterpret_cast<const uint2 *>(lst) + t;
+      // list chunks are loaded one iteration ahead; two accumulators break
+      // the dependency chains of consecutive pairs
+      PairAcc b = {0.0, 0.0, 0.0, 0.0, 0.0};
+      uint2 w = lane < nch ? __ldg(lp + (size_t)lane * M) : make_uint2(0u, 0u);
+      for (int c = lane; c < nch; c += TPP) {
+        const uint2 wn = c + TPP < nch ? __ldg(lp + (size_t)(c + TPP) * M) : make_uint2(0u, 0u);
+        const int e0 = w.x & 0xffff, e1 = w.x >> 16, e2 = w.y & 0xffff, e3 = w.y >> 16;
+        const int k0 = 4 * c;
+        {
+          const int q = e0 & 0x7fff;
+          pair_rel<PREC>(a, xi - sx[q], yi - sy[q], zi - sz[q], ti + (e0 >> 15));
+        }
+        if (k0 + 1 < nn) {
+          const int q = e1 & 0x7fff;
+          pair_rel<PREC>(b, xi - sx[q], yi - sy[q], zi - sz[q], ti + (e1 >> 15));
+        }
+        if (k0 + 2 < nn) {
+          const int q = e2 & 0x7fff;
+          pair_rel<PREC>(a, xi - sx[q], yi - sy[q], zi - sz[q], ti + (e2 >> 15));
+        }
+        if (k0 + 3 < nn) {
+          const int q = e3 & 0x7fff;
+          pair_rel<PREC>(b, xi - sx[q], yi - sy[q], zi - sz[q], ti + (e3 >> 15));
+        }
+        w = wn;
+      }
+      a.fx += b.fx;
+      a.fy += b.fy;
+      a.fz += b.fz;
+      a.pe += b.pe;
+      a.vir += b.vir;
+    } else if (valid) {
+      // list overflow or oversized union: scan the neighbour cells directly
+      const int nc = d.nc, c = v.cellof[i];
+      const int cx = c % nc, cy = (c / nc) % nc, cz = c / (nc * nc);
+      const double L2 = L * L;
+      for (int oz = -1; oz <= 1; oz++)
+        for (int oy = -1; oy <= 1; oy++)
+          for (int ox = -1; ox <= 1; ox++) {
+            const int c2 = wrap_cell(cx + ox, nc) + wrap_cell(cy + oy, nc) * nc + wrap_cell(cz + oz, nc) * nc * nc;
+            const int s0 = d.poff + v.cstart[d.coff + c2], m = v.ccount[d.coff + c2];
+            for (int k = lane; k < m; k += TPP) {
+              const int j = s0 + k;
+              if (j == i) continue;
+              const double4 pj = v.pos[j];
+              if (PREC == 0)
+                pair_fp64(a, pi, ti, pj, L, L2);
+              else
+                pair_fp32(a, pi, ti, pj, L, L2);
+            }
+          }
+    }
+#pragma unroll
+    for (int o = TPP / 2; o > 0; o >>= 1) {
+      a.fx += __shfl_xor_sync(0xffffffffu, a.fx, o);
+      a.fy += __shfl_xor_sync(0xffffffffu, a.fy, o);
+      a.fz += __shfl_xor_sync(0xffffffffu, a.fz, o);
+      a.pe += __shfl_xor_sync(0xffffffffu, a.pe, o);
+      a.vir += __shfl_xor_sync(0xffffffffu, a.vir, o);
+    }
+    if (!valid || lane != 0) continue;
+    double fx = a.fx, fy = a.fy, fz = a.fz;
+    if (ai >= 0) {  // active force (MDcode/cell_list+forces.c:207-218)
+      const char4 kk = v.kdir[d.aoff + ai];
+      const double kx = (double)kk.x, ky = (double)kk.y, kz = (double)kk.z;
+      fx += d.f0 * kx;
+      fy += d.f0 * ky;
+      fz += d.f0 * kz;
+      va += d.f0 * (kx * uxi + ky * uyi + kz * uzi);
+    }
+    v.fx[i] = fx;
+    v.fy[i] = fy;
+    v.fz[i] = fz;
+    if (mode != 2) {
+      double px, py, pz;
+      if (mode == 0) {  // U2 (MDcode/time_evolve.c:558-567)
+        px = __dadd_rn(vx0, __dmul_rn(fx, d.half_dt));
+        py = __dadd_rn(vy0, __dmul_rn(fy, d.half_dt));
+        pz = __dadd_rn(vz0, __dmul_rn(fz, d.half_dt));
+      } else {
+        const double s2 = st.s2;
+        px = __dmul_rn(vx0, s2);
+        py = __dmul_rn(vy0, s2);
+        pz = __dmul_rn(vz0, s2);
+      }
+      v.vx[i] = px;
+      v.vy[i] = py;
+      v.vz[i] = pz;
+      ke += px * px + py * py + pz * pz;
+    }
+    pe += a.pe;
+    vir += a.vir;
   }
   pe = block_sum_dyn(pe, sh);
   vir = block_sum_dyn(vir, sh);

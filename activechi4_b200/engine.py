@@ -174,6 +174,9 @@ class Engine:
     def set_launch(self, tpp: int, block: int):
         check(self._lib.acg_set_launch(self.h, int(tpp), int(block)))
 
+    def set_group_tpp(self, gtpp: int):
+        check(self._lib.acg_set_group_tpp(self.h, int(gtpp)))
+
     def get_launch(self):
         t, b = C.c_int(), C.c_int()
         check(self._lib.acg_get_launch(self.h, C.byref(t), C.byref(b)))

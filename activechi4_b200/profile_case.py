@@ -28,10 +28,13 @@ def main():
     ap.add_argument("--tpp", type=int, default=0)
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--list-mode", type=int, default=0)
+    ap.add_argument("--group-tpp", type=int, default=0)
     a = ap.parse_args()
     e = Engine(default_params(a.n, T=2.0, precision=a.precision, list_mode=a.list_mode))
     if a.tpp:
         e.set_launch(a.tpp, a.block or 128)
+    if a.group_tpp:
+        e.set_group_tpp(a.group_tpp)
     e.set_state(0, lattice_state(a.n, 2.0, seed=3))
     e.set_nhc(0, np.zeros(3), np.array([0.1, 0.0, -0.1]))
     e.step(a.melt)

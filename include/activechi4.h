@@ -188,6 +188,9 @@ int acg_measure_fp64_peak(int device, double *tflops);
  * particle in the force kernel (1,2,4,8,16,32); block: threads per block. */
 int acg_set_launch(acg_engine *e, int tpp, int block);
 int acg_get_launch(acg_engine *e, int *tpp, int *block);
+/* Threads per particle (1, 2 or 4) of the cell-group force kernel used for
+ * boxes with >= 3 cells per side. */
+int acg_set_group_tpp(acg_engine *e, int gtpp);
 
 const char *acg_last_error(void);
 const char *acg_version(void);
