@@ -5,7 +5,7 @@ active.c and time_evolve.c entry points.
 The compute path is the in-tree CUDA library ``libactivechi4_b200.so`` (built
 by ``activechi4_b200.build``) behind the C ABI in ``include/activechi4.h``.
 """
-from .engine import Engine, default_params, footprint  # noqa: F401
+from .engine import Engine, default_params, footprint, observables_from_sums, qvectors  # noqa: F401
 from .init import State, box_length, lattice_state, n_active, select_active  # noqa: F401
 
 __all__ = ["Engine", "default_params", "footprint", "State", "box_length", "lattice_state",

@@ -40,6 +40,14 @@ class acg_thermo(C.Structure):
     ]
 
 
+class acg_obs_config(C.Structure):
+    _fields_ = [
+        ("run_length", C.c_int64), ("num_origins", C.c_int), ("factor", C.c_double),
+        ("max_interval", C.c_int64), ("a", C.c_double), ("nq", C.c_int), ("qvec", C.c_void_p),
+        ("max_live_origins", C.c_int),
+    ]
+
+
 class AcgError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"activechi4 error {code}: {msg}")
@@ -75,6 +83,8 @@ _SIGS = {
     "acg_set_launch": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "acg_get_launch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "acg_set_group_tpp": (C.c_int, [C.c_void_p, C.c_int]),
+    "acg_obs_configure": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(acg_obs_config)]),
+    "acg_obs_sums": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "acg_bench_steps": (C.c_int, [C.c_void_p, C.c_int, C.c_size_t, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "acg_measure_fp64_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
     "acg_forces_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,

@@ -62,6 +62,7 @@ struct SysDesc {
   int coff, ncell, nc, ng;     // ng: cell groups per side (0: no group path, nc < 3)
   int tile0_b, ntile_b, tau_p, thermostat;
   int shuffle, list_mode, precision, goff;  // goff: offset of the system's groups
+  int tile0_a, ntile_a, pad2, pad3;           // the system's kick/drift tiles
   double L, invL, inv_cell;  // inv_cell: cells per unit reduced length (InvCellSize)
   double T, f0, dt, half_dt, skin2, rebuild_factor, dof;
   double q[NHC_M];
@@ -85,6 +86,23 @@ struct SysState {
   int status;                // 1 = non-finite kinetic energy seen
   unsigned int counter_b;    // last-block counter of the force kernel
   int overflow;
+  int obs_lo, obs_hi, obs_cur;  // observable events due this step, next event
+  unsigned int counter_o;       // last-block counter of the observable kernel
+};
+
+// In-place observables of one system (set by acg_obs_configure): events of the
+// log-time schedule sorted by step; kind 0 = measure against an origin slot
+// into a time bin, 1 = store the origin snapshot into a slot.
+constexpr int OBS_EMAX = 16;  // events handled in one step
+constexpr int OBS_NV = 5;     // per-event sums: overlap, r^2, sum d^4, r^4, Fs
+struct ObsDesc {
+  const long long *ev_step;
+  const int *ev_info;   // kind | slot << 1 | bin << 13
+  double *snap;         // [slot][particle id][3] unfolded reduced positions
+  double *acc;          // [bin][8]: sum Q, sum Q^2, msd, msd_d4, msd_r4, Fs, count, -
+  const int *qvec;      // [nq][3] integer wave vectors (q = 2 pi n / L)
+  int n_events, nbins, nq, nslots;
+  double a2;            // overlap cut squared (absolute units)
 };
 
 struct View {
@@ -103,6 +121,8 @@ struct View {
   int *gstart;      // per group: first centre particle (prefix over the system's groups)
   double4 *part_b;
   unsigned int *counter_a;
+  ObsDesc *obs;      // [nsys]
+  double *part_o;    // [tiles_a][OBS_EMAX][OBS_NV]
   double *stage_d;  // [9n] x, xu, p interleaved per system (original order)
   int *stage_i;     // [2n] type, act
   double *stage_f;  // [3n] forces

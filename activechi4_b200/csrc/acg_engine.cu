@@ -142,6 +142,8 @@ int plan(const acg_params *params, int nsys, Layout &lay) {
   add(4 * (Gn + 1));                      // gstart
   add(32 * (Gn + S / 4 + nsys + 1));      // part_b
   add(64);                                // counters
+  add(sizeof(ObsDesc) * nsys);            // observables
+  add(8 * (S / BLOCK_A + nsys + 1) * OBS_EMAX * OBS_NV);  // part_o
   add(72 * S);                            // stage_d
   add(8 * S);                             // stage_i
   add(24 * S);                            // stage_f
@@ -175,6 +177,8 @@ struct acg_engine {
   cudaGraph_t graph1 = nullptr;
   void *flush = nullptr;  // bench-only L2 flush buffer
   size_t flush_bytes = 0;
+  std::vector<std::vector<void *>> obs_bufs;  // per system: device buffers of the observables
+  std::vector<std::vector<long long>> obs_offsets;  // per system: offset (steps) of each time bin
 };
 
 namespace {
@@ -272,11 +276,15 @@ int launch_force(acg_engine *e, int mode) {
 }
 
 int launch_step_eager(acg_engine *e) {
-  k_kick_drift<<<e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, 0, e->stream>>>(e->v, 0, 0);
+  k_kick_drift<<<e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, 0, e->stream>>>(e->v, 0, 0, 0);
   CK(cudaGetLastError());
   int rc = launch_rebuild(e);
   if (rc) return rc;
-  return launch_force(e, 0);
+  rc = launch_force(e, 0);
+  if (rc) return rc;
+  k_observe<<<e->ntiles_a, BLOCK_A, 0, e->stream>>>(e->v);
+  CK(cudaGetLastError());
+  return ACG_OK;
 }
 
 // forces (and lists) for every system flagged dirty
@@ -321,10 +329,11 @@ int build_graph(acg_engine *e, int K, cudaGraph_t *gout, cudaGraphExec_t *xout) 
   cudaGraphNode_t prev = nullptr;
   int mode0 = 0, use_cond = 1, tbase = e->ntiles_g;
   for (int s = 0; s < K; s++) {
-    cudaGraphConditionalHandle h;
+    cudaGraphConditionalHandle h, ho;
     CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+    CK(cudaGraphConditionalHandleCreate(&ho, g, 0, cudaGraphCondAssignDefault));
     cudaGraphNode_t na, nc, nb;
-    void *aa[] = {&v, &use_cond, &h};
+    void *aa[] = {&v, &use_cond, &h, &ho};
     int rc = add_kernel(g, prev ? &prev : nullptr, prev ? 1 : 0, &na, (void *)k_kick_drift,
                         e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, aa);
     if (rc) return rc;
@@ -368,7 +377,17 @@ int build_graph(acg_engine *e, int K, cudaGraph_t *gout, cudaGraphExec_t *xout) 
       if (rc) return rc;
       last = nb;
     }
-    prev = last;
+    // observables at the scheduled steps (device-decided, like the rebuild)
+    cudaGraphNodeParams op = {};
+    op.type = cudaGraphNodeTypeConditional;
+    op.conditional.handle = ho;
+    op.conditional.type = cudaGraphCondTypeIf;
+    op.conditional.size = 1;
+    cudaGraphNode_t no, nk;
+    CK(cudaGraphAddNode(&no, g, &last, 1, &op));
+    rc = add_kernel(op.conditional.phGraph_out[0], nullptr, 0, &nk, (void *)k_observe, e->ntiles_a, BLOCK_A, va);
+    if (rc) return rc;
+    prev = no;
   }
   cudaGraphExec_t x;
   CK(cudaGraphInstantiate(&x, g, 0));
@@ -485,6 +504,8 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   v.gstart = (int *)take(4 * (Gn + 1));
   v.part_b = (double4 *)take(32 * (Gn + S / 4 + nsys + 1));
   v.counter_a = (unsigned int *)take(64);
+  v.obs = (ObsDesc *)take(sizeof(ObsDesc) * nsys);
+  v.part_o = (double *)take(8 * (S / BLOCK_A + nsys + 1) * OBS_EMAX * OBS_NV);
   v.stage_d = (double *)take(72 * S);
   v.stage_i = (int *)take(8 * S);
   v.stage_f = (double *)take(24 * S);
@@ -498,8 +519,10 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
 
   std::vector<int2> h_a, h_l, h_c, h_g;
   for (int r = 0; r < nsys; r++) {
-    const SysDesc &d = L.desc[r];
+    SysDesc &d = e->lay.desc[r];
+    d.tile0_a = (int)h_a.size();
     for (int s = 0; s < d.n; s += BLOCK_A) h_a.push_back(make_int2(r, s));
+    d.ntile_a = (int)h_a.size() - d.tile0_a;
     for (int s = 0; s < d.ncell; s += CELLS_PER_TILE) h_c.push_back(make_int2(r, s));
     if (d.ng > 0)
       for (int g = 0; g < d.ng * d.ng * d.ng; g++) h_g.push_back(make_int2(r, g));
@@ -563,6 +586,8 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   rc = build_tiles_b(e);
   if (rc) return cleanup_fail(rc);
   e->dirty.assign(nsys, 1);
+  e->obs_bufs.assign(nsys, {});
+  e->obs_offsets.assign(nsys, {});
   e->any_dirty = true;
   if (cudaStreamSynchronize(e->stream) != cudaSuccess)
     return cleanup_fail(fail(ACG_ERR_CUDA, "set-up synchronisation failed"));
@@ -575,6 +600,8 @@ int acg_destroy(acg_engine *e) {
   cudaSetDevice(e->device);
   if (e->stream) cudaStreamSynchronize(e->stream);
   drop_graphs(e);
+  for (auto &bs : e->obs_bufs)
+    for (void *b : bs) cudaFree(b);
   if (e->flush) cudaFree(e->flush);
   if (e->arena) cudaFree(e->arena);
   if (e->stream) cudaStreamDestroy(e->stream);
@@ -902,7 +929,7 @@ int acg_time_stage(acg_engine *e, int stage, int reps, double *ms) {
   CK(cudaEventRecord(a, e->stream));
   for (int i = 0; i < reps; i++) {
     if (stage == 0) {
-      k_kick_drift<<<e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, 0, e->stream>>>(e->v, 0, 0);
+      k_kick_drift<<<e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, 0, e->stream>>>(e->v, 0, 0, 0);
     } else if (stage == 1) {
       rc = launch_force(e, 2);
     } else {
@@ -918,6 +945,132 @@ int acg_time_stage(acg_engine *e, int stage, int reps, double *ms) {
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   *ms = (double)t / reps;
+  return ACG_OK;
+}
+
+// The log-time schedule of prepareSavingArray (MDcode/main.c:62-119) turned
+// into device events: origins every run/num_origins steps; from each origin
+// the offsets 1, then *factor truncated (+1 when that does not advance), below
+// max_interval (the analysis pairs offsets below half the run,
+// Analysis/overlap.c:28) and inside the run.  An origin snapshot occupies one of
+// max_live slots from its step to its last offset; an origin for which no slot
+// is free is left out.
+int acg_obs_configure(acg_engine *e, int sys, const acg_obs_config *c) {
+  int rc = check_sys(e, sys);
+  if (rc) return rc;
+  if (!c || c->run_length < 2 || c->num_origins < 1 || !(c->factor > 1.0) || !(c->a > 0) || c->nq < 0 ||
+      c->nq > 256 || (c->nq > 0 && !c->qvec) || c->max_live_origins < 1 || c->max_live_origins > 4095)
+    return fail(ACG_ERR_INVALID, "bad observable configuration");
+  CK(cudaSetDevice(e->device));
+  rc = prime(e);
+  if (rc) return rc;
+  SysState st;
+  CK(cudaMemcpyAsync(&st, e->v.st + sys, sizeof(st), cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  const long long base = st.step, run = c->run_length;
+  const long long lin = run / c->num_origins;
+  const long long maxint = c->max_interval > 0 ? c->max_interval : run / 2;
+  std::vector<long long> offs;
+  for (unsigned long long off = 1; (long long)off < maxint && (long long)off < run;) {
+    offs.push_back((long long)off);
+    if ((unsigned long long)(off * c->factor) == off)
+      off++;
+    else
+      off = (unsigned long long)((double)off * c->factor);
+  }
+  if (offs.empty() || offs.size() > 200000) return fail(ACG_ERR_INVALID, "schedule has no usable offsets");
+  struct Ev {
+    long long step;
+    int kind, slot, bin;
+  };
+  std::vector<Ev> ev;
+  std::vector<long long> busy(c->max_live_origins, -1);
+  for (long long k = 0; k < c->num_origins && lin > 0; k++) {
+    const long long t0 = k * lin;
+    long long last = t0;
+    for (long long o : offs)
+      if (t0 + o < run) last = t0 + o;
+    int slot = -1;
+    for (int q = 0; q < c->max_live_origins; q++)
+      if (busy[q] < t0) {
+        slot = q;
+        break;
+      }
+    if (slot < 0) continue;
+    busy[slot] = last;
+    ev.push_back({base + t0, 1, slot, 0});
+    for (size_t m = 0; m < offs.size(); m++)
+      if (t0 + offs[m] < run) ev.push_back({base + t0 + offs[m], 0, slot, (int)m});
+  }
+  std::sort(ev.begin(), ev.end(), [](const Ev &a, const Ev &b) {
+    return a.step != b.step ? a.step < b.step : a.kind < b.kind;  // measure before snapshot
+  });
+  for (size_t i = 0, j; i < ev.size(); i = j) {
+    for (j = i; j < ev.size() && ev[j].step == ev[i].step; j++) {
+    }
+    if (j - i > (size_t)OBS_EMAX) return fail(ACG_ERR_INVALID, "more than 16 observable events in one step");
+  }
+  const SysDesc &d = e->lay.desc[sys];
+  std::vector<long long> h_step(ev.size());
+  std::vector<int> h_info(ev.size());
+  for (size_t i = 0; i < ev.size(); i++) {
+    h_step[i] = ev[i].step;
+    h_info[i] = ev[i].kind | (ev[i].slot << 1) | (ev[i].bin << 13);
+  }
+  for (void *b : e->obs_bufs[sys]) cudaFree(b);
+  e->obs_bufs[sys].clear();
+  auto dalloc = [&](size_t bytes, void **p) {
+    cudaError_t ce = cudaMalloc(p, bytes > 0 ? bytes : 8);
+    if (ce == cudaSuccess) e->obs_bufs[sys].push_back(*p);
+    return ce;
+  };
+  void *p_step = nullptr, *p_info = nullptr, *p_snap = nullptr, *p_acc = nullptr, *p_q = nullptr;
+  if (dalloc(8 * ev.size(), &p_step) != cudaSuccess || dalloc(4 * ev.size(), &p_info) != cudaSuccess ||
+      dalloc((size_t)c->max_live_origins * d.n * 3 * sizeof(double), &p_snap) != cudaSuccess ||
+      dalloc(offs.size() * 8 * sizeof(double), &p_acc) != cudaSuccess || dalloc(12 * (size_t)c->nq, &p_q) != cudaSuccess)
+    return fail(ACG_ERR_NOMEM, "observable buffers: device allocation failed");
+  CK(cudaMemcpyAsync(p_step, h_step.data(), 8 * ev.size(), cudaMemcpyHostToDevice, e->stream));
+  CK(cudaMemcpyAsync(p_info, h_info.data(), 4 * ev.size(), cudaMemcpyHostToDevice, e->stream));
+  CK(cudaMemsetAsync(p_acc, 0, offs.size() * 8 * sizeof(double), e->stream));
+  if (c->nq) CK(cudaMemcpyAsync(p_q, c->qvec, 12 * (size_t)c->nq, cudaMemcpyHostToDevice, e->stream));
+  ObsDesc od = {};
+  od.ev_step = (const long long *)p_step;
+  od.ev_info = (const int *)p_info;
+  od.snap = (double *)p_snap;
+  od.acc = (double *)p_acc;
+  od.qvec = (const int *)p_q;
+  od.n_events = (int)ev.size();
+  od.nbins = (int)offs.size();
+  od.nq = c->nq;
+  od.nslots = c->max_live_origins;
+  od.a2 = c->a * c->a;
+  CK(cudaMemcpyAsync(e->v.obs + sys, &od, sizeof(od), cudaMemcpyHostToDevice, e->stream));
+  int zero = 0;
+  CK(cudaMemcpyAsync(&e->v.st[sys].obs_cur, &zero, sizeof(int), cudaMemcpyHostToDevice, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  e->obs_offsets[sys] = offs;
+  return ACG_OK;
+}
+
+int acg_obs_sums(acg_engine *e, int sys, int *nbins, int64_t *offset, double *sums) {
+  int rc = check_sys(e, sys);
+  if (rc) return rc;
+  const auto &offs = e->obs_offsets[sys];
+  if (nbins) *nbins = (int)offs.size();
+  if (offs.empty()) return ACG_OK;
+  if (offset)
+    for (size_t m = 0; m < offs.size(); m++) offset[m] = offs[m];
+  if (sums) {
+    CK(cudaSetDevice(e->device));
+    ObsDesc od;
+    CK(cudaMemcpyAsync(&od, e->v.obs + sys, sizeof(od), cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    std::vector<double> a(offs.size() * 8);
+    CK(cudaMemcpyAsync(a.data(), od.acc, a.size() * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    for (size_t m = 0; m < offs.size(); m++)
+      for (int k = 0; k < 7; k++) sums[7 * m + k] = a[8 * m + k];
+  }
   return ACG_OK;
 }
 

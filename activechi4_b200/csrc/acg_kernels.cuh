@@ -117,8 +117,8 @@ __device__ void shuffle_component(const View &v, int r, int comp, long long step
 
 // ---------------------------------------------------------------------------
 // stage 1: kick + drift (+ shuffle blocks) + rebuild decision
-__global__ void __launch_bounds__(BLOCK_A) k_kick_drift(View v, int use_cond,
-                                                        cudaGraphConditionalHandle h) {
+__global__ void __launch_bounds__(BLOCK_A) k_kick_drift(View v, int use_cond, cudaGraphConditionalHandle h,
+                                                        cudaGraphConditionalHandle h_obs) {
   __shared__ double sm[BLOCK_A / 32];
   __shared__ int s_last;
   const int b = blockIdx.x;
@@ -192,11 +192,135 @@ __global__ void __launch_bounds__(BLOCK_A) k_kick_drift(View v, int use_cond,
     st.force_rebuild = 0;
     any |= rb;
   }
+  // observable events due at the end of this step (frame = loop index step)
+  int any_obs = 0;
+  for (int s = threadIdx.x; s < v.nsys; s += blockDim.x) {
+    const ObsDesc &o = v.obs[s];
+    SysState &st = v.st[s];
+    if (o.n_events == 0) {
+      st.obs_lo = st.obs_hi = 0;
+      continue;
+    }
+    const long long step = st.step;
+    int c = st.obs_cur;
+    while (c < o.n_events && o.ev_step[c] < step) c++;
+    const int lo = c;
+    while (c < o.n_events && o.ev_step[c] == step && c - lo < OBS_EMAX) c++;
+    st.obs_lo = lo;
+    st.obs_hi = c;
+    st.obs_cur = c;
+    any_obs |= c > lo;
+  }
   any = __syncthreads_or(any);
+  any_obs = __syncthreads_or(any_obs);
   if (threadIdx.x == 0) {
     *v.counter_a = 0;
-    if (use_cond) cudaGraphSetConditional(h, any ? 1u : 0u);
+    if (use_cond) {
+      cudaGraphSetConditional(h, any ? 1u : 0u);
+      cudaGraphSetConditional(h_obs, any_obs ? 1u : 0u);
+    }
   }
+}
+
+// In-place observables at the scheduled steps (replaces writing data_coor.out
+// at the log times, MDcode/main.c:252-257, and the offline Analysis/overlap.c,
+// msd_pos.c, Fsqt.c sums over (origin, later frame) pairs).  Per particle and
+// due event: store the origin snapshot, or accumulate the overlap
+// Theta(a^2 - |dr_minimg|^2) (Analysis/overlap.c:61-83), |dr|^2, sum dx^4,
+// |dr|^4 (Analysis/msd_pos.c:64-76) and sum_q cos(q.dr) over the wave vectors.
+__global__ void __launch_bounds__(BLOCK_A) k_observe(View v) {
+  __shared__ double red[OBS_EMAX * OBS_NV][BLOCK_A / 32];
+  __shared__ int s_last;
+  const int2 t = v.tiles_a[blockIdx.x];
+  const int r = t.x;
+  SysState &st = v.st[r];
+  const int lo = st.obs_lo, hi = st.obs_hi;
+  if (hi <= lo) return;
+  const SysDesc &d = v.desc[r];
+  const ObsDesc &o = v.obs[r];
+  const int loc = t.y + threadIdx.x;
+  const bool valid = loc < d.n;
+  const int i = d.poff + (valid ? loc : 0);
+  const int id = valid ? v.id[i] : 0;
+  const double ux = valid ? v.ux[i] : 0.0, uy = valid ? v.uy[i] : 0.0, uz = valid ? v.uz[i] : 0.0;
+  const double L = d.L;
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  for (int e = lo; e < hi; e++) {
+    const int info = o.ev_info[e];
+    const int kind = info & 1, slot = (info >> 1) & 4095;
+    double *sn = o.snap + ((size_t)slot * d.n + id) * 3;
+    double val[OBS_NV] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (kind == 1) {
+      if (valid) {
+        sn[0] = ux;
+        sn[1] = uy;
+        sn[2] = uz;
+      }
+    } else if (valid) {
+      const double dx = ux - sn[0], dy = uy - sn[1], dz = uz - sn[2];
+      double mx = dx, my = dy, mz = dz;  // Analysis/overlap.c:67-78
+      if (mz >= 0.5) mz -= 1.0; else if (mz < -0.5) mz += 1.0;
+      if (my >= 0.5) my -= 1.0; else if (my < -0.5) my += 1.0;
+      if (mx >= 0.5) mx -= 1.0; else if (mx < -0.5) mx += 1.0;
+      const double r2q = L * L * (mx * mx + my * my + mz * mz);
+      val[0] = r2q < o.a2 ? 1.0 : 0.0;
+      const double r2 = L * L * (dx * dx + dy * dy + dz * dz);
+      val[1] = r2;
+      val[2] = L * L * L * L * (dx * dx * dx * dx + dy * dy * dy * dy + dz * dz * dz * dz);
+      val[3] = r2 * r2;
+      double fs = 0.0;
+      for (int q = 0; q < o.nq; q++)
+        fs += cos(6.283185307179586 * ((double)o.qvec[3 * q] * dx + (double)o.qvec[3 * q + 1] * dy +
+                                       (double)o.qvec[3 * q + 2] * dz));
+      val[4] = fs;
+    }
+    if (kind == 0) {
+#pragma unroll
+      for (int k = 0; k < OBS_NV; k++) {
+        double x = val[k];
+        for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
+        if (l == 0) red[(e - lo) * OBS_NV + k][w] = x;
+      }
+    }
+  }
+  __syncthreads();
+  double *part = v.part_o + (size_t)blockIdx.x * OBS_EMAX * OBS_NV;
+  for (int k = threadIdx.x; k < (hi - lo) * OBS_NV; k += blockDim.x) {
+    if (o.ev_info[lo + k / OBS_NV] & 1) continue;
+    double x = 0.0;
+    for (int ww = 0; ww < BLOCK_A / 32; ww++) x += red[k][ww];
+    part[k] = x;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(&st.counter_o, 1u) == (unsigned)(d.ntile_a - 1);
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (threadIdx.x < hi - lo) {
+    const int e = lo + threadIdx.x;
+    const int info = o.ev_info[e];
+    if ((info & 1) == 0) {
+      const int bin = info >> 13;
+      double sum[OBS_NV] = {0.0, 0.0, 0.0, 0.0, 0.0};
+      for (int b = 0; b < d.ntile_a; b++) {
+        const double *pb = v.part_o + ((size_t)(d.tile0_a + b) * OBS_EMAX + threadIdx.x) * OBS_NV;
+        for (int k = 0; k < OBS_NV; k++) sum[k] += __ldcg(pb + k);
+      }
+      const double tot = (double)d.n;  // TotPart (Analysis/overlap.c:25)
+      const double Q = sum[0] / tot;
+      double *acc = o.acc + (size_t)bin * 8;
+      acc[0] += Q;  // c[time_index] (Analysis/overlap.c:90-93)
+      acc[1] += Q * Q;
+      acc[2] += sum[1] / tot;  // msd[0..2] (Analysis/msd_pos.c:88-91)
+      acc[3] += sum[2] / tot;
+      acc[4] += sum[3] / tot;
+      acc[5] += o.nq > 0 ? sum[4] / (tot * o.nq) : 0.0;
+      acc[6] += 1.0;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) st.counter_o = 0;
 }
 
 // host request: rebuild the systems flagged `prime` (all < 0: rebuild all)

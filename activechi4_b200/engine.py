@@ -47,6 +47,34 @@ def measure_fp64_peak(device: int = 0) -> float:
     return t.value
 
 
+def observables_from_sums(offset, sums, dt=0.005) -> dict:
+    """Per-bin averages from summed (Q, Q^2, msd, msd_d4, msd_r4, Fs, count);
+    sums of several replicas with equal parameters may be added first (chi4
+    across replicas).  chi4 = <Q^2> - <Q>^2, not multiplied by N
+    (Analysis/overlap.c:118)."""
+    s = np.asarray(sums, dtype=np.float64)
+    cnt = s[:, 6]
+    m = cnt > 0
+    c = cnt[m]
+    Q = s[m, 0] / c
+    return {"t": np.asarray(offset)[m] * dt, "offset": np.asarray(offset)[m], "count": c.astype(np.int64),
+            "Q": Q, "chi4": s[m, 1] / c - Q * Q, "msd": s[m, 2] / c, "msd_d4": s[m, 3] / c,
+            "msd_r4": s[m, 4] / c, "Fs": s[m, 5] / c}
+
+
+def qvectors(L: float, q: float, count: int = 48, tol: float = 0.1):
+    """Integer vectors n with |2 pi n / L| within tol of q (up to `count`,
+    nearest first, sign-symmetric pairs kept together)."""
+    nmax = int(np.ceil((q + tol) * L / (2 * np.pi))) + 1
+    g = np.arange(-nmax, nmax + 1)
+    n = np.stack(np.meshgrid(g, g, g, indexing="ij"), axis=-1).reshape(-1, 3)
+    qq = 2 * np.pi * np.sqrt((n * n).sum(axis=1)) / L
+    sel = np.abs(qq - q) <= tol
+    n, qq = n[sel], qq[sel]
+    order = np.lexsort((n[:, 2], n[:, 1], n[:, 0], np.abs(qq - q)))
+    return n[order][:count].astype(np.int32)
+
+
 def footprint(params: Sequence[acg_params]) -> int:
     arr = (acg_params * len(params))(*params)
     out = C.c_size_t(0)
@@ -169,6 +197,28 @@ class Engine:
         members = np.zeros(self.n(sys), dtype=np.int32)
         check(self._lib.acg_get_cells(self.h, sys, _ptr(dims), C.byref(nc), _ptr(counts), _ptr(members)))
         return dims, counts, members
+
+    # -- in-place observables -------------------------------------------
+    def obs_configure(self, sys: int, run_length: int, num_origins: int = 200, factor: float = 1.4,
+                      max_interval: int = 0, a: float = 0.3, qvec=None, max_live_origins: int = 64):
+        q = np.ascontiguousarray(np.zeros((0, 3)) if qvec is None else qvec, dtype=np.int32).reshape(-1, 3)
+        cfg = _abi.acg_obs_config(int(run_length), int(num_origins), float(factor), int(max_interval),
+                                  float(a), int(q.shape[0]), q.ctypes.data_as(C.c_void_p) if q.size else None,
+                                  int(max_live_origins))
+        check(self._lib.acg_obs_configure(self.h, sys, C.byref(cfg)))
+
+    def obs_sums(self, sys: int = 0):
+        nb = C.c_int()
+        check(self._lib.acg_obs_sums(self.h, sys, C.byref(nb), None, None))
+        off = np.zeros(nb.value, dtype=np.int64)
+        sums = np.zeros((nb.value, 7))
+        check(self._lib.acg_obs_sums(self.h, sys, C.byref(nb), _ptr(off), _ptr(sums)))
+        return off, sums
+
+    def observables(self, sys: int = 0, dt: float = 0.005) -> dict:
+        """Q(t), chi4(t), MSD and moments, Fs(q,t) per time bin with data."""
+        off, s = self.obs_sums(sys)
+        return observables_from_sums(off, s, dt)
 
     # -- tuning / timing -------------------------------------------------
     def set_launch(self, tpp: int, block: int):

@@ -160,6 +160,32 @@ int acg_get_thermo(acg_engine *e, int sys, acg_thermo *out);
  * members may be NULL; returns the number of cells via *ncell. */
 int acg_get_cells(acg_engine *e, int sys, int *dims, int *ncell, int *counts, int *members);
 
+/* ---- in-place observables on the log-time schedule -----------------------
+ * The reference writes unfolded coordinates at the steps of prepareSavingArray
+ * (MDcode/main.c:62-119, 252-257) and computes the overlap Q(t), chi4(t), the
+ * MSD and its moments and Fs(q,t) offline (Analysis/overlap.c, msd_pos.c,
+ * Fsqt.c).  Here the same sums are accumulated on the device while stepping:
+ * origin snapshots stay in device memory and every (origin, later step) pair of
+ * the schedule adds to its time bin.  The schedule starts at the system's
+ * current step. */
+typedef struct acg_obs_config {
+  int64_t run_length;     /* steps of the run (runLength) */
+  int num_origins;        /* origins, every run_length/num_origins steps (200) */
+  double factor;          /* offset growth factor (1.4) */
+  int64_t max_interval;   /* offsets analysed are < max_interval; <= 0: run_length/2 */
+  double a;               /* overlap cut (0.3, Analysis/main.c:6) */
+  int nq;                 /* wave vectors for Fs (0..256) */
+  const int *qvec;        /* [nq][3] integers n, q = 2 pi n / L */
+  int max_live_origins;   /* origin snapshots kept (device memory n*24 bytes each) */
+} acg_obs_config;
+int acg_obs_configure(acg_engine *e, int sys, const acg_obs_config *c);
+/* Raw per-bin sums over the pairs accumulated so far: *nbins bins with
+ * offset[m] steps and sums[m][7] = {sum Q, sum Q^2, sum msd, sum msd_d4,
+ * sum msd_r4, sum Fs, count}; Q(t) = sum Q / count, chi4 = sum Q^2/count -
+ * Q(t)^2 (not x N, as Analysis/overlap.c:118), msd = <|dr|^2>, msd_d4 =
+ * <dx^4+dy^4+dz^4>, msd_r4 = <|dr|^4> (Analysis/msd_pos.c:88-91). */
+int acg_obs_sums(acg_engine *e, int sys, int *nbins, int64_t *offset, double *sums);
+
 /* Number of systems, particles of one system, and the engine's CUDA stream
  * (a cudaStream_t) for callers that time or order work around it. */
 int acg_num_systems(acg_engine *e);
