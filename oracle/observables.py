@@ -59,13 +59,18 @@ def pair_sums(x0, x1, L, a, qvec=None):
     return ov, float(r2.sum()), float(r4.sum()), float((r2 * r2).sum()), fs
 
 
-def analyse(frames, L, run_length, num_origins, factor, max_interval, a, qvec=None, max_live=64):
+def analyse(frames, L, run_length, num_origins, factor, max_interval, a, qvec=None, max_live=64,
+            skip_missing=False):
     """Per-bin sums (Q, Q^2, msd, msd_d4, msd_r4, Fs, count) from frames =
-    {step: [N,3] unfolded reduced coordinates}, as the device accumulates them."""
+    {step: [N,3] unfolded reduced coordinates}, as the device accumulates them.
+    skip_missing: leave out pairs whose frame is absent, as the reference's
+    frame lookup does (Analysis/overlap.c:55-57)."""
     offs, pairs = log_pairs(run_length, num_origins, factor, max_interval, max_live)
     out = np.zeros((len(offs), 7))
     nq = 0 if qvec is None else len(qvec)
     for t0, t1, m in pairs:
+        if skip_missing and (t0 not in frames or t1 not in frames):
+            continue
         x0, x1 = frames[t0], frames[t1]
         n = x0.shape[0]
         ov, r2, r4, r2sq, fs = pair_sums(x0, x1, L, a, qvec)

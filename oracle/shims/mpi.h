@@ -57,6 +57,9 @@ int MPI_Gather(const void *send, int scount, MPI_Datatype stype, void *recv,
 int MPI_Gatherv(const void *send, int scount, MPI_Datatype stype, void *recv,
                 const int *rcounts, const int *displs, MPI_Datatype rtype,
                 int root, MPI_Comm comm);
+int MPI_Send(const void *buf, int count, MPI_Datatype type, int dest, int tag, MPI_Comm comm);
+int MPI_Recv(void *buf, int count, MPI_Datatype type, int source, int tag, MPI_Comm comm,
+             MPI_Status *status);
 int MPI_Type_create_struct(int count, const int *blocklens, const MPI_Aint *offsets,
                            const MPI_Datatype *types, MPI_Datatype *newtype);
 int MPI_Type_commit(MPI_Datatype *type);
