@@ -23,12 +23,12 @@ def oracle_lib_path() -> str:
     return os.path.join(HERE, "_build", "libacg_oracle.so")
 
 
-def ref_lib_path(n: int) -> str:
-    return os.path.join(HERE, "_ref", f"libref_md_n{n}.so")
+def ref_lib_path(n: int, kind: str = "ref") -> str:
+    return os.path.join(HERE, "_ref", f"lib{kind}_md_n{n}.so")
 
 
-def reference_available(n: int) -> bool:
-    return os.path.exists(ref_lib_path(n))
+def reference_available(n: int, kind: str = "ref") -> bool:
+    return os.path.exists(ref_lib_path(n, kind))
 
 
 def build_oracle() -> str:
@@ -213,19 +213,24 @@ class Oracle(_Common):
         return out[:m].copy()
 
 
-_rlibs: dict[int, C.CDLL] = {}
+_rlibs: dict[tuple, C.CDLL] = {}
 
 
 class Reference(_Common):
     """The reference engine compiled from its own sources (N fixed per library).
 
+    kind "ref": the reference's own timestep files; kind "dropin": the same
+    program with cell_list+forces.c and time_evolve.c replaced by the drop-in
+    files of activechi4_b200/legacy (the timestep runs on the GPU).
     The reference keeps its state in process globals, so there is exactly one
-    system per particle count per process."""
+    system per particle count and kind per process."""
 
-    def __init__(self, n):
+    def __init__(self, n, kind="ref"):
         self.n = int(n)
-        if self.n not in _rlibs:
-            path = ref_lib_path(self.n)
+        self.kind = kind
+        key = (self.n, kind)
+        if key not in _rlibs:
+            path = ref_lib_path(self.n, kind)
             if not os.path.exists(path):
                 raise FileNotFoundError(f"reference oracle for N={n} not built: {path}")
             lib = C.CDLL(path)
@@ -250,8 +255,8 @@ class Reference(_Common):
             lib.ref_log_schedule.argtypes = [C.c_ulonglong, C.c_int, C.c_double, C.c_char_p, _up, C.c_int]
             lib.ref_write_restart.argtypes = [C.c_char_p, C.c_int, C.c_int]
             lib.ref_set_time.argtypes = [C.c_long]
-            _rlibs[self.n] = lib
-        self.lib = _rlibs[self.n]
+            _rlibs[key] = lib
+        self.lib = _rlibs[key]
         self.nact = self.lib.ref_nact()
         self.tau_per = self.lib.ref_tau_per()
 

@@ -70,3 +70,14 @@ def test_create_without_gpu_fails_cleanly(lib):
     with pytest.raises(AcgError) as ei:
         Engine(default_params(1000))
     assert ei.value.code == -2
+
+
+def test_dropin_files_define_the_reference_entry_points():
+    """The drop-in C files define the timestep entry points of
+    MDcode/subroutine.h that other reference files call."""
+    import glob
+    src = "".join(open(f).read() for f in glob.glob(os.path.join(ROOT, "activechi4_b200", "legacy", "*.c")))
+    for name in ("update_cell_list", "calculate_forces", "getcell_I", "maps", "len_check",
+                 "AdvanceTimeNVTNoseHoover", "advance_time_NVEFrog", "InitialiseNoseHoover",
+                 "applypbc1", "applypbc"):
+        assert re.search(r"\b" + name + r"\s*\([^;{]*\)\s*\{", src), name
