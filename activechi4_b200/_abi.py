@@ -74,6 +74,7 @@ _SIGS = {
     "acg_step": (C.c_int, [C.c_void_p, C.c_int]),
     "acg_step_eager": (C.c_int, [C.c_void_p, C.c_int]),
     "acg_sync": (C.c_int, [C.c_void_p]),
+    "acg_poll": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "acg_get_thermo": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(acg_thermo)]),
     "acg_get_cells": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "acg_num_systems": (C.c_int, [C.c_void_p]),

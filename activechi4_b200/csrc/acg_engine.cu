@@ -546,15 +546,18 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
     v.gcap = (int)align_up((size_t)(1.2 * mean_u + 64.0), 64);
     v.gcap = std::min(v.gcap, 8192);
   }
+  // the shared-memory limit is a property of the kernel function, shared by
+  // every engine of the process: only ever raise it
+  auto raise_smem = [](const void *fn, size_t need) {
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, fn) != cudaSuccess) return false;
+    if ((size_t)fa.maxDynamicSharedSizeBytes >= need) return true;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need) == cudaSuccess;
+  };
   bool attr_ok = true;
   for (int gt : {1, 2, 4})
-    for (int pr : {0, 1})
-      attr_ok = attr_ok && cudaFuncSetAttribute((const void *)group_fn(gt, pr),
-                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                (int)group_smem(v.gcap)) == cudaSuccess;
-  attr_ok = attr_ok && cudaFuncSetAttribute((const void *)k_build_list_groups,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)list_smem(v.gcap)) == cudaSuccess;
+    for (int pr : {0, 1}) attr_ok = attr_ok && raise_smem((const void *)group_fn(gt, pr), group_smem(v.gcap));
+  attr_ok = attr_ok && raise_smem((const void *)k_build_list_groups, list_smem(v.gcap));
   if (!attr_ok) {
     acg_destroy(e);
     return fail(ACG_ERR_CUDA, "cudaFuncSetAttribute (group kernels' shared memory) failed");
@@ -824,6 +827,21 @@ int acg_sync(acg_engine *e) {
   CK(cudaSetDevice(e->device));
   CK(cudaStreamSynchronize(e->stream));
   return ACG_OK;
+}
+
+int acg_poll(acg_engine *e, int *done) {
+  if (!e || !done) return fail(ACG_ERR_INVALID, "bad arguments");
+  CK(cudaSetDevice(e->device));
+  cudaError_t q = cudaStreamQuery(e->stream);
+  if (q == cudaSuccess) {
+    *done = 1;
+    return ACG_OK;
+  }
+  if (q == cudaErrorNotReady) {
+    *done = 0;
+    return ACG_OK;
+  }
+  return fail(ACG_ERR_CUDA, std::string("cudaStreamQuery: ") + cudaGetErrorString(q));
 }
 
 int acg_get_thermo(acg_engine *e, int sys, acg_thermo *out) {

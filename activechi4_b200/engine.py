@@ -180,6 +180,12 @@ class Engine:
     def sync(self):
         check(self._lib.acg_sync(self.h))
 
+    def poll(self) -> bool:
+        """True when all queued work has finished (does not block)."""
+        d = C.c_int()
+        check(self._lib.acg_poll(self.h, C.byref(d)))
+        return bool(d.value)
+
     def thermo(self, sys: int = 0) -> dict:
         t = acg_thermo()
         rc = self._lib.acg_get_thermo(self.h, sys, C.byref(t))

@@ -1,0 +1,185 @@
+"""Continuous-batching run server.
+
+A request asks for `steps` steps of one active KA system (N particles, T, f0,
+tau_p) from a seeded lattice, with the overlap Q(t), chi4(t), MSD and Fs
+accumulated in place on the log-time schedule of the run (no trajectory is
+written).  Requests arrive over time; the server admits a queued request as
+soon as its device footprint fits the memory budget and an active slot is
+free, keeps its whole state on the device in its own engine and CUDA stream,
+and advances every active run in chunks of CUDA-graph launches, so the work of
+runs admitted at different times overlaps on the GPU.  When a run ends its
+observables and energies are read back, its memory is released and the next
+queued request is admitted.  Latency is arrival -> results.
+
+Runs are independent and deterministic, so each result is bit-identical
+whether the run was served alone or in a mix (tested).
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import time
+
+import numpy as np
+
+from .engine import Engine, default_params, footprint, qvectors
+from .init import lattice_state
+
+
+@dataclasses.dataclass
+class RunRequest:
+    rid: int
+    n: int
+    steps: int
+    T: float = 0.45
+    f0: float = 1.0
+    tau_p_steps: int = 200
+    seed: int = 0
+    arrival: float = 0.0     # seconds after the start of serving
+    precision: int = 1       # ACG_PREC_FP32 pair forces
+    num_origins: int = 20
+    max_live_origins: int = 16
+    q: float = 7.25          # |q| of the Fs(q,t) shell
+
+
+@dataclasses.dataclass
+class RunResult:
+    rid: int
+    n: int
+    steps: int
+    arrival: float
+    admitted: float
+    finished: float
+    observables: tuple       # (offsets, per-bin sums) of acg_obs_sums
+    pe: float
+    ke: float
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+def request_params(req: RunRequest):
+    return default_params(req.n, T=req.T, f0=req.f0, tau_p_steps=req.tau_p_steps, precision=req.precision,
+                          seed=1000003 * req.seed + 17, list_mode=1, rebuild_factor=4.0)
+
+
+def request_footprint(req: RunRequest) -> int:
+    return footprint([request_params(req)]) + req.max_live_origins * req.n * 24 + (4 << 20)
+
+
+def start_run(req: RunRequest, device: int = 0) -> Engine:
+    e = Engine(request_params(req), device=device)
+    st = lattice_state(req.n, req.T, seed=req.seed)
+    e.set_state(0, st)
+    rng = np.random.default_rng(req.seed)
+    q = e.thermo(0)["q"]
+    e.set_nhc(0, np.zeros(3), np.sqrt(req.T * q) * rng.standard_normal(3))
+    e.obs_configure(0, req.steps, min(req.num_origins, max(1, req.steps // 2)), 1.4, 0, 0.3,
+                    qvectors(st.L, req.q, 24), req.max_live_origins)
+    return e
+
+
+def finish_run(e: Engine, req: RunRequest, arrival, admitted, finished) -> RunResult:
+    th = e.thermo(0)
+    return RunResult(req.rid, req.n, req.steps, arrival, admitted, finished, e.obs_sums(0), th["pe"], th["ke"])
+
+
+class Server:
+    """Admit-as-memory-frees scheduler over per-run engines and streams."""
+
+    def __init__(self, device=0, hbm_budget=None, max_active=32, chunk_work=2.0e7):
+        self.device = device
+        if hbm_budget is None:
+            import torch
+            free, _ = torch.cuda.mem_get_info(device)
+            hbm_budget = int(0.8 * free)
+        self.budget = int(hbm_budget)
+        self.max_active = max_active
+        self.chunk_work = chunk_work
+
+    def _chunk(self, n, left):
+        k = int(max(32, min(8192, round(self.chunk_work / max(n, 1) / 32) * 32)))
+        return min(k, left)
+
+    def run(self, requests, clock=time.perf_counter):
+        pending = sorted(requests, key=lambda r: r.arrival)
+        queue, active, results = [], {}, []
+        used = 0
+        t0 = clock()
+        while pending or queue or active:
+            now = clock() - t0
+            while pending and pending[0].arrival <= now:
+                queue.append(pending.pop(0))
+            # admission in arrival order while memory and slots allow
+            while queue and len(active) < self.max_active:
+                fp = request_footprint(queue[0])
+                if used + fp > self.budget and active:
+                    break
+                req = queue.pop(0)
+                e = start_run(req, self.device)
+                used += fp
+                left = req.steps
+                k = self._chunk(req.n, left)
+                e.step(k)
+                active[req.rid] = [e, req, left - k, clock() - t0, fp]
+            progressed = False
+            for rid in list(active):
+                e, req, left, adm, fp = active[rid]
+                if not e.poll():
+                    continue
+                progressed = True
+                if left == 0:
+                    results.append(finish_run(e, req, req.arrival, adm, clock() - t0))
+                    e.close()
+                    used -= fp
+                    del active[rid]
+                else:
+                    k = self._chunk(req.n, left)
+                    e.step(k)
+                    active[rid][2] = left - k
+            if not progressed:
+                nxt = pending[0].arrival - (clock() - t0) if (pending and not queue and not active) else 2e-4
+                time.sleep(max(5e-5, min(nxt, 2e-3)))
+        return sorted(results, key=lambda r: r.rid)
+
+
+def run_serial(requests, device=0, precision=0, clock=time.perf_counter):
+    """The same requests one after another, each alone on the GPU (the
+    serial baseline); returns (results, wall seconds)."""
+    out = []
+    t0 = clock()
+    for req in requests:
+        r = dataclasses.replace(req, precision=precision)
+        e = start_run(r, device)
+        a = clock() - t0
+        e.step(r.steps)
+        e.sync()
+        out.append(finish_run(e, r, a, a, clock() - t0))
+        e.close()
+    return out, clock() - t0
+
+
+def poisson_requests(count, rate=20.0, n_range=(1000, 256000), step_range=(10000, 1000000), scale=1.0,
+                     seed=0, precision=1):
+    """Poisson arrivals at `rate` per second; N and steps log-uniform; T, f0,
+    tau_p drawn from the batched workload's sets.  `scale` multiplies the step
+    counts (a bounded sample of the workload)."""
+    from .batch import F0_SET, T_SET, TAU_SET
+    rng = np.random.default_rng(seed)
+    t, reqs = 0.0, []
+    for i in range(count):
+        t += rng.exponential(1.0 / rate)
+        n = int(math.exp(rng.uniform(math.log(n_range[0]), math.log(n_range[1]))))
+        steps = int(math.exp(rng.uniform(math.log(step_range[0]), math.log(step_range[1]))) * scale)
+        reqs.append(RunRequest(i, n, max(64, steps), float(rng.choice(T_SET)), float(rng.choice(F0_SET)),
+                               int(rng.choice(TAU_SET)), seed=10000 * seed + i, arrival=t, precision=precision))
+    return reqs
+
+
+def latency_stats(results):
+    lat = np.array([r.latency for r in results])
+    work = sum(r.n * r.steps for r in results)
+    span = max(r.finished for r in results) - min(r.arrival for r in results)
+    return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "particle_steps_per_s": work / span, "requests": len(results), "span_s": span}

@@ -151,6 +151,8 @@ int acg_step(acg_engine *e, int nsteps);
  * rebuild kernel is launched and skips the systems that need no rebuild). */
 int acg_step_eager(acg_engine *e, int nsteps);
 int acg_sync(acg_engine *e);
+/* Non-blocking: *done = 1 when all work queued on the engine has finished. */
+int acg_poll(acg_engine *e, int *done);
 
 int acg_get_thermo(acg_engine *e, int sys, acg_thermo *out);
 
