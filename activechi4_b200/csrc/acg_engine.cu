@@ -1131,12 +1131,16 @@ int acg_bench_steps(acg_engine *e, int nchunks, size_t flush_bytes, double *ms, 
   std::vector<long long> rb1(e->lay.nsys);
   for (int r = 0; r < e->lay.nsys; r++)
     CK(cudaMemcpy(&rb1[r], &e->v.st[r].rebuilds, sizeof(long long), cudaMemcpyDeviceToHost));
-  // every step launches the kick/drift and force kernels; a step whose
-  // conditional fires also launches the six rebuild kernels
+  // every step launches the kick/drift kernel and one launch of each force
+  // kernel in use; a step whose rebuild conditional fires also launches the
+  // rebuild kernels with a non-empty grid (the node list of build_graph)
   long long steps_with_rebuild = 0;
   for (int r = 0; r < e->lay.nsys; r++) steps_with_rebuild = std::max(steps_with_rebuild, rb1[r] - rb0[r]);
+  const long long per_step = 1 + (e->ntiles_g > 0) + (e->ntiles_b > 0);
+  const long long per_rebuild = 3 * (e->ntiles_a > 0) + (e->lay.nsys > 0) + (e->ntiles_c > 0) +
+                                (e->ntiles_g > 0) + (e->ntiles_l > 0);
   *ms = tot;
-  if (launches) *launches = 2LL * GRAPH_STEPS * nchunks + 6LL * steps_with_rebuild;
+  if (launches) *launches = per_step * GRAPH_STEPS * nchunks + per_rebuild * steps_with_rebuild;
   return ACG_OK;
 }
 

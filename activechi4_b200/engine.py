@@ -94,6 +94,7 @@ class Engine:
         h = C.c_void_p()
         check(self._lib.acg_create(arr, len(self.params), int(device), C.byref(h)))
         self.h = h
+        self._meta = {}
         self.sizes = []
         for r in range(len(self.params)):
             n, na = C.c_int(), C.c_int()
@@ -133,6 +134,7 @@ class Engine:
         t = _i32(state.type, (n,))
         a = _i32(state.act_tag, (n,))
         check(self._lib.acg_set_state(self.h, sys, _ptr(x), _ptr(xu), _ptr(p), _ptr(t), _ptr(a)))
+        self._meta[sys] = (float(state.L), t.copy(), a.copy())
         if set_directions and self.nact(sys):
             self.set_directions(sys, state.k)
 
@@ -141,6 +143,14 @@ class Engine:
         x, xu, p, F = (np.empty((n, 3)) for _ in range(4))
         check(self._lib.acg_get_state(self.h, sys, _ptr(x), _ptr(xu), _ptr(p), _ptr(F)))
         return x, xu, p, F
+
+    def state_meta(self, sys: int = 0) -> dict:
+        """Box length, types and active tags of the last set_state (constant
+        during a run: the device keeps particles in id order at the ABI)."""
+        if sys not in self._meta:
+            raise KeyError(f"system {sys} has no state loaded")
+        L, t, a = self._meta[sys]
+        return {"L": L, "type": t, "act_tag": a}
 
     def set_directions(self, sys: int, k):
         na = self.nact(sys)

@@ -46,6 +46,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--equil", type=int, default=2048, help="melt steps at T=2.0 and again at T=0.45")
+    ap.add_argument("--workload", default="all", choices=["all", "plain", "batch", "serve"],
+                    help="plain: the headline line only; all: plus the batched and served objects")
+    ap.add_argument("--replicas", type=int, default=256)
+    ap.add_argument("--requests", type=int, default=48)
     return ap.parse_args()
 
 
@@ -230,6 +234,55 @@ def e2e_run(e, st, nchunks):
     return n * steps / wall, state_bytes / steps, (state_bytes + 24 * n + thermo_bytes * nchunks) / steps
 
 
+def batched_run(args, device):
+    """256 replicas, N uniform in [500, 4000], T/f0/tau_p from the batched
+    sets, FP32 pair forces, one launch per kernel per step (CUDA graphs),
+    launch shapes from the autotuner; melted at T=2.0 before timing."""
+    from activechi4_b200.batch import make_engine, replica_set
+    from activechi4_b200.tune import autotune
+    reps = replica_set(count=args.replicas, seed=11, precision=1)
+    e = make_engine(reps, device=device)
+    for r, (p, _) in enumerate(reps):
+        e.set_temperature(r, 2.0)
+    e.step(1024)
+    for r, (p, _) in enumerate(reps):
+        e.set_temperature(r, p.T)
+    e.step(512)
+    e.sync()
+    cfg = autotune(e, reps=5)
+    e.step(64)
+    e.sync()
+    nchunks = max(8, args.steps // 32 // 8)
+    ms, launches = e.bench_steps(nchunks, 256 << 20)
+    ntot = sum(e.n(r) for r in range(e.nsys))
+    steps = 32 * nchunks
+    e.close()
+    return {"value": ntot * steps / (ms * 1e-3), "unit": "particle-steps/s", "replicas": len(reps),
+            "particles": ntot, "steps": steps, "ms_per_step": ms / steps, "dtype": "f32-pair/f64-state",
+            "autotune": cfg, "gpu_launches": int(launches),
+            "workload": "256 replicas, N uniform [500,4000], T {0.45,0.5,0.6}, f0 {0,0.5,1,2}, "
+                        "tau_p {20,200,2000} steps, rho 1.2, NHC NVT, FP32 pair forces"}
+
+
+def served_run(args, device, plain_value):
+    """Poisson arrivals (20/s) of runs with N log-uniform in [1e3, 2.56e5] and
+    steps log-uniform in [1e4, 1e6] scaled by 1/100 (a bounded sample), FP32
+    pair forces, in-place Q/chi4/MSD/Fs; against the same requests run one by
+    one on the plain FP64 path."""
+    from activechi4_b200.serve import Server, latency_stats, poisson_requests, run_serial
+    reqs = poisson_requests(args.requests, rate=20.0, scale=0.01, seed=5, precision=1)
+    res = Server(device=device, max_active=32).run(reqs)
+    st = latency_stats(res)
+    ser, wall = run_serial(reqs, device=device, precision=0)
+    work = sum(r.n * r.steps for r in reqs)
+    st.update({"serial_fp64_particle_steps_per_s": work / wall, "serial_fp64_wall_s": wall,
+               "vs_serial_fp64": st["particle_steps_per_s"] / (work / wall),
+               "vs_plain_fp64": st["particle_steps_per_s"] / plain_value,
+               "workload": f"{len(reqs)} requests, Poisson 20/s, N log-uniform [1e3,2.56e5], steps log-uniform "
+                           "[1e4,1e6]/100, T/f0/tau_p from the batched sets, FP32 pair forces, lattice starts"})
+    return st
+
+
 def run_ours(args):
     import torch
     rank = int(os.environ.get("RANK", "0"))
@@ -282,6 +335,13 @@ def run_ours(args):
     th = e.thermo(0)
 
     e2e_val, h2d, d2h = e2e_run(e, st, nchunks)
+    e.close()
+    extra = {}
+    if world == 1 and args.workload in ("all", "batch"):
+        extra["batched"] = batched_run(args, local)
+        extra["batched"]["vs_plain_fp64"] = extra["batched"]["value"] / value
+    if world == 1 and args.workload in ("all", "serve"):
+        extra["served"] = served_run(args, local, value)
     if dist is not None:
         te = torch.tensor([e2e_val], dtype=torch.float64, device=f"cuda:{local}")
         dist.all_reduce(te, op=dist.ReduceOp.MIN)
@@ -316,7 +376,7 @@ def run_ours(args):
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak_gbs, "unit": "GB/s",
                          "frac": achieved / peak_gbs, "traffic": traffic.get("bytes_per_launch") if traffic else None,
-                         "kernel": "k_force_kick", "peak_source": peak_src,
+                         "kernel": "k_force_groups", "peak_source": peak_src,
                          "alg_bytes_per_particle": B_ALG, "kernel_ms": t_force,
                          "fp64": {"achieved_tflops": fp64_ach, "peak_tflops_measured": fp64_peak,
                                   "frac": fp64_ach / fp64_peak,
@@ -327,8 +387,8 @@ def run_ours(args):
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        line.update(extra)
         print(json.dumps(line), flush=True)
-    e.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
