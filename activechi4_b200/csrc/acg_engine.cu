@@ -195,7 +195,7 @@ GroupFn group_fn(int gtpp, int prec) {
   return nullptr;
 }
 size_t group_smem(int gcap) { return 3 * (size_t)gcap * sizeof(double); }
-size_t list_smem(int gcap) { return (size_t)gcap * sizeof(float4); }
+size_t list_smem(int gcap) { return ((size_t)gcap + 3 * MAX_UNION) * sizeof(float4); }
 
 ForceFn force_fn(int tpp, int prec) {
 #define F(T)                                                                     \

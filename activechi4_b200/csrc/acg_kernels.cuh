@@ -937,10 +937,15 @@ __device__ __forceinline__ size_t group_entry(int k, int t, int M) {
 }
 
 // one warp per centre cell, one lane per particle of that cell: every lane
-// tests the same staged candidate (a shared-memory broadcast)
+// tests the same staged candidate (a shared-memory broadcast).  Each union
+// cell's staged run is padded to a multiple of four with far-away dummies so
+// the candidate loop reads four entries without bounds tests; the staged .w
+// holds the list code (unpadded staged index | type << 15).  Each lane packs
+// its entries into a 64-bit register and stores whole 4-entry chunks.
 __global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
   extern __shared__ float4 stg[];
   __shared__ GroupStage S;
+  __shared__ int pre4[MAX_UNION + 1];
   const int2 tile = v.tiles_g[blockIdx.x];
   const int r = tile.x, g = tile.y;
   if (!v.st[r].rebuild) return;
@@ -952,23 +957,38 @@ __global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int maxnb = v.maxnb;
   if (Q <= v.gcap) {
+    if (threadIdx.x == 0) {
+      int m = 0;
+      for (int u = 0; u < S.nU; u++) {
+        pre4[u] = m;
+        m += (S.upre[u + 1] - S.upre[u] + 3) & ~3;
+      }
+      pre4[S.nU] = m;
+    }
+    __syncthreads();
     const double L = d.L;
     for (int u = warp; u < S.nU; u += nwarps) {
-      const int q0 = S.upre[u], m = S.upre[u + 1] - q0, j0 = S.ustart[u];
-      for (int k = lane; k < m; k += 32) {
-        const double4 p = v.pos_s[j0 + k];
+      const int q0 = S.upre[u], m = S.upre[u + 1] - q0, j0 = S.ustart[u], p0 = pre4[u];
+      const int m4 = pre4[u + 1] - p0;
+      for (int k = lane; k < m4; k += 32) {
         float4 f;
-        f.x = (float)staged_coord(S, G, u, 0, p.x, L);
-        f.y = (float)staged_coord(S, G, u, 1, p.y, L);
-        f.z = (float)staged_coord(S, G, u, 2, p.z, L);
-        f.w = __int_as_float((int)p.w);
-        stg[q0 + k] = f;
+        if (k < m) {
+          const double4 p = v.pos_s[j0 + k];
+          f.x = (float)staged_coord(S, G, u, 0, p.x, L);
+          f.y = (float)staged_coord(S, G, u, 1, p.y, L);
+          f.z = (float)staged_coord(S, G, u, 2, p.z, L);
+          f.w = __int_as_float((q0 + k) | ((int)p.w << 15));
+        } else {
+          f = make_float4(1e18f, 1e18f, 1e18f, __int_as_float(0));
+        }
+        stg[p0 + k] = f;
       }
     }
     __syncthreads();
     float lc[3];
     for (int k = 0; k < 3; k++) lc[k] = (float)(lcut2_of(d, k) * (1.0 + 1e-5));
-    uint16_t *lst = group_list(v, d, g);
+    const bool one_cut = lc[0] == lc[1] && lc[1] == lc[2];
+    uint2 *lst = reinterpret_cast<uint2 *>(group_list(v, d, g));
     for (int kc = warp; kc < S.nC; kc += nwarps) {
       const int cu = S.cu[kc];
       const int m = S.cpre[kc + 1] - S.cpre[kc];
@@ -976,39 +996,44 @@ __global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
       for (int w0 = 0; w0 < m; w0 += 32) {
         const int w = w0 + lane;
         const bool valid = w < m;
-        const int t = S.cpre[kc] + w, qs = S.upre[cu] + w;
-        const float4 fi = valid ? stg[qs] : make_float4(0.f, 0.f, 0.f, 0.f);
-        const int ti = __float_as_int(fi.w);
+        const int t = S.cpre[kc] + w, ps = pre4[cu] + w;
+        const float4 fi = valid ? stg[ps] : make_float4(-1e18f, -1e18f, -1e18f, __int_as_float(0));
+        const int ti = __float_as_int(fi.w) >> 15;
+        // cut for a partner of type 0 / 1 (the sum of the two types indexes lc)
+        const float c0 = ti == 0 ? lc[0] : lc[1], c1 = ti == 0 ? lc[1] : lc[2];
+        unsigned long long pend = 0ull;
         int n = 0;
         for (int dz = -1; dz <= 1; dz++)
           for (int dy = -1; dy <= 1; dy++)
             for (int dx = -1; dx <= 1; dx++) {
               const int u2 = (ux + dx) + (uy + dy) * nux + (uz + dz) * nux * nuy;
-              const int q1 = S.upre[u2 + 1];
-              // four candidates per iteration: independent tests, then appends
-              for (int q = S.upre[u2]; q < q1; q += 4) {
+              const int q1 = pre4[u2 + 1];
+              for (int q = pre4[u2]; q < q1; q += 4) {
                 int code[4];
                 bool ok[4];
 #pragma unroll
-                for (int u = 0; u < 4; u++) {
-                  const int qq = q + u;
-                  const float4 fj = stg[qq < q1 ? qq : q];
-                  const int tj = __float_as_int(fj.w);
+                for (int e = 0; e < 4; e++) {
+                  const float4 fj = stg[q + e];
                   const float ex = fi.x - fj.x, ey = fi.y - fj.y, ez = fi.z - fj.z;
                   const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
-                  const int tt = ti + tj;
-                  ok[u] = valid && qq < q1 && qq != qs && r2 < (tt == 0 ? lc[0] : (tt == 1 ? lc[1] : lc[2]));
-                  code[u] = qq | (tj << 15);
+                  code[e] = __float_as_int(fj.w);
+                  const float cut = one_cut ? c0 : ((code[e] >> 15) ? c1 : c0);
+                  ok[e] = r2 < cut && q + e != ps;
                 }
 #pragma unroll
-                for (int u = 0; u < 4; u++)
-                  if (ok[u]) {
-                    if (n < maxnb) lst[group_entry(n, t, M)] = (uint16_t)code[u];
+                for (int e = 0; e < 4; e++)
+                  if (ok[e]) {
+                    pend |= (unsigned long long)(code[e] & 0xffff) << (16 * (n & 3));
                     n++;
+                    if ((n & 3) == 0) {
+                      if (n <= maxnb) lst[(size_t)((n >> 2) - 1) * M + t] = make_uint2((unsigned)pend, (unsigned)(pend >> 32));
+                      pend = 0ull;
+                    }
                   }
               }
             }
         if (valid) {
+          if ((n & 3) && n <= maxnb) lst[(size_t)(n >> 2) * M + t] = make_uint2((unsigned)pend, (unsigned)(pend >> 32));
           const int i = S.ustart[cu] + w;
           if (n > maxnb) {
             v.nbn[i] = -1;
@@ -1036,6 +1061,46 @@ __global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
   }
 }
 
+// 1/x for x in the pair range (0.3 < x < 7): the hardware estimate
+// (rcp.approx.ftz.f64) refined by two Newton-Raphson steps y += y (1 - x y),
+// each squaring the relative error, to within an ulp of the rounded quotient
+__device__ __forceinline__ double rcp_nr(double x) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  return fma(y, e, y);
+}
+
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+struct PairAccF {
+  float fx, fy, fz, pe, vir;
+};
+
+// FP32 pair term (separation in FP32 from the hi/lo staged coordinates)
+__device__ __forceinline__ void pair_f32(PairAccF &a, float dx, float dy, float dz, int tp) {
+  const float is2 = tp == 0 ? 1.0f : (tp == 1 ? 1.5625f : (float)(1.0 / (0.88 * 0.88)));
+  const float e4 = tp == 0 ? 4.0f : (tp == 1 ? 6.0f : 2.0f);
+  const float dr2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  const float rs2 = dr2 * is2;
+  if (rs2 < (float)KA_RC2) {
+    const float s2 = rcp_approx(rs2);
+    const float s6 = s2 * s2 * s2;
+    a.pe = fmaf(e4, fmaf(s6, s6 - 1.0f, fmaf((float)KA_C2, rs2, (float)KA_C0)), a.pe);
+    const float g = (2.0f * e4 * is2) * fmaf(6.0f * s6 * (s6 - 0.5f), s2, -(float)KA_C2);
+    a.fx = fmaf(g, dx, a.fx);
+    a.fy = fmaf(g, dy, a.fy);
+    a.fz = fmaf(g, dz, a.fz);
+    a.vir = fmaf(g, dr2, a.vir);
+  }
+}
+
 // pair term on a separation already in the minimum image, absolute units
 template <int PREC>
 __device__ __forceinline__ void pair_rel(PairAcc &a, double dx, double dy, double dz, int tp) {
@@ -1045,7 +1110,7 @@ __device__ __forceinline__ void pair_rel(PairAcc &a, double dx, double dy, doubl
     const double dr2 = dx * dx + dy * dy + dz * dz;
     const double rs2 = dr2 * is2;
     if (rs2 < KA_RC2) {
-      const double s2 = 1.0 / rs2;
+      const double s2 = rcp_nr(rs2);
       const double s6 = s2 * s2 * s2;
       a.pe += e4 * ((s6 * (s6 - 1.0)) + KA_C0 + KA_C2 * rs2);
       const double g = (2.0 * e4 * is2) * (6.0 * s6 * (s6 - 0.5) * s2 - KA_C2);
@@ -1075,8 +1140,14 @@ __device__ __forceinline__ void pair_rel(PairAcc &a, double dx, double dy, doubl
 
 template <int TPP, int PREC>
 __global__ void __launch_bounds__(BLOCK_G) k_force_groups(View v, int mode) {
-  extern __shared__ double gsm[];
+  // FP64: three double arrays; FP32: float4 {hi x, y, z, lo x} + float2
+  // {lo y, lo z} (hi = the coordinate rounded to float, lo = the remainder),
+  // 24 bytes per staged particle either way
+  extern __shared__ __align__(16) unsigned char gsm_raw[];
+  double *gsm = reinterpret_cast<double *>(gsm_raw);
   double *sx = gsm, *sy = gsm + v.gcap, *sz = gsm + 2 * v.gcap;
+  float4 *shi = reinterpret_cast<float4 *>(gsm_raw);
+  float2 *slo = reinterpret_cast<float2 *>(gsm_raw + 16 * (size_t)v.gcap);
   __shared__ GroupStage S;
   __shared__ double sh[32];
   __shared__ int s_last;
@@ -1098,9 +1169,18 @@ __global__ void __launch_bounds__(BLOCK_G) k_force_groups(View v, int mode) {
       const int q0 = S.upre[u], m = S.upre[u + 1] - q0, j0 = S.ustart[u];
       for (int k = wl; k < m; k += 32) {
         const double4 p = v.pos[j0 + k];
-        sx[q0 + k] = staged_coord(S, G, u, 0, p.x, L);
-        sy[q0 + k] = staged_coord(S, G, u, 1, p.y, L);
-        sz[q0 + k] = staged_coord(S, G, u, 2, p.z, L);
+        const double cx = staged_coord(S, G, u, 0, p.x, L);
+        const double cy = staged_coord(S, G, u, 1, p.y, L);
+        const double cz = staged_coord(S, G, u, 2, p.z, L);
+        if (PREC == 0) {
+          sx[q0 + k] = cx;
+          sy[q0 + k] = cy;
+          sz[q0 + k] = cz;
+        } else {
+          const float hx = (float)cx, hy = (float)cy, hz = (float)cz;
+          shi[q0 + k] = make_float4(hx, hy, hz, (float)(cx - (double)hx));
+          slo[q0 + k] = make_float2((float)(cy - (double)hy), (float)(cz - (double)hz));
+        }
       }
     }
   }
@@ -1134,7 +1214,37 @@ __global__ void __launch_bounds__(BLOCK_G) k_force_groups(View v, int mode) {
       }
     }
     PairAcc a = {0.0, 0.0, 0.0, 0.0, 0.0};
-    if (valid && staged && nn >= 0) {
+    if (PREC == 1 && valid && staged && nn >= 0) {
+      const float4 hi = shi[qs];
+      const float2 li = slo[qs];
+      const int nch = (nn + 3) >> 2;
+      const uint2 *lp = reinterpret_cast<const uint2 *>(lst) + t;
+      PairAccF fa = {0.f, 0.f, 0.f, 0.f, 0.f}, fb = {0.f, 0.f, 0.f, 0.f, 0.f};
+      uint2 w = lane < nch ? __ldg(lp + (size_t)lane * M) : make_uint2(0u, 0u);
+      for (int c = lane; c < nch; c += TPP) {
+        const uint2 wn = c + TPP < nch ? __ldg(lp + (size_t)(c + TPP) * M) : make_uint2(0u, 0u);
+        const int k0 = 4 * c;
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          const int code = ((e < 2 ? w.x : w.y) >> (16 * (e & 1))) & 0xffff;
+          if (e == 0 || k0 + e < nn) {
+            const int q = code & 0x7fff;
+            const float4 hj = shi[q];
+            const float2 lj = slo[q];
+            const float dx = (hi.x - hj.x) + (hi.w - hj.w);
+            const float dy = (hi.y - hj.y) + (li.x - lj.x);
+            const float dz = (hi.z - hj.z) + (li.y - lj.y);
+            pair_f32(e & 1 ? fb : fa, dx, dy, dz, ti + (code >> 15));
+          }
+        }
+        w = wn;
+      }
+      a.fx = (double)fa.fx + (double)fb.fx;
+      a.fy = (double)fa.fy + (double)fb.fy;
+      a.fz = (double)fa.fz + (double)fb.fz;
+      a.pe = (double)fa.pe + (double)fb.pe;
+      a.vir = (double)fa.vir + (double)fb.vir;
+    } else if (PREC == 0 && valid && staged && nn >= 0) {
       const double xi = sx[qs], yi = sy[qs], zi = sz[qs];
       const int nch = (nn + 3) >> 2;
       const uint2 *lp = reinterpret_cast<const uint2 *>(lst) + t;
