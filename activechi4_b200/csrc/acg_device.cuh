@@ -32,6 +32,11 @@ constexpr int CELLS_PER_TILE = 8;
 constexpr int BLOCK_SCAN = 512;
 constexpr int BLOCK_G = 256;      // threads of the group kernels
 constexpr int MAX_UNION = 64;     // 4 x 4 x 4 union cells of a 2 x 2 x 2 group
+constexpr int BLOCK_X = 256;      // threads of the whole-box kernels
+constexpr int BOX_CELLS = 8;      // cells per whole-box block (one warp per cell in the list build)
+constexpr int MAX_BOX_NC = 4;     // whole-box mode for 2..4 cells per side
+constexpr int MAX_BOX_CELLS = MAX_BOX_NC * MAX_BOX_NC * MAX_BOX_NC;
+constexpr int MAX_BOX_N = 8192;   // whole-box staging limit (FP64: 192 KB of shared memory)
 
 // A cell group: up to 2 x 2 x 2 cells (clipped at the box edge) and the union
 // of their neighbour cells, up to 4 x 4 x 4, in which union cell (ux,uy,uz)
@@ -59,10 +64,10 @@ constexpr double KA_RC2 = 6.25;  // (r/sigma)^2 cut
 
 struct SysDesc {
   int n, nact, poff, aoff;
-  int coff, ncell, nc, ng;     // ng: cell groups per side (0: no group path, nc < 3)
+  int coff, ncell, nc, ng;     // ng: cell groups per side (0: no group path)
   int tile0_b, ntile_b, tau_p, thermostat;
   int shuffle, list_mode, precision, goff;  // goff: offset of the system's groups
-  int tile0_a, ntile_a, pad2, pad3;           // the system's kick/drift tiles
+  int tile0_a, ntile_a, box, xoff;            // kick/drift tiles; box: whole-box kernels (2..4 cells per side), xoff: first box tile
   double L, invL, inv_cell;  // inv_cell: cells per unit reduced length (InvCellSize)
   double T, f0, dt, half_dt, skin2, rebuild_factor, dof;
   double q[NHC_M];
@@ -117,7 +122,7 @@ struct View {
   int *id_s, *act_s;
   int *cell_tmp, *perm_u, *perm;
   int *ccount_b, *cfill, *cstart, *ccount;
-  const int2 *tiles_a, *tiles_b, *tiles_l, *tiles_c, *tiles_g;
+  const int2 *tiles_a, *tiles_b, *tiles_l, *tiles_c, *tiles_g, *tiles_x;
   int *gstart;      // per group: first centre particle (prefix over the system's groups)
   double4 *part_b;
   unsigned int *counter_a;
@@ -126,7 +131,7 @@ struct View {
   double *stage_d;  // [9n] x, xu, p interleaved per system (original order)
   int *stage_i;     // [2n] type, act
   double *stage_f;  // [3n] forces
-  int ntiles_a, ntiles_b, ntiles_l, ntiles_c, ntiles_g, nsys, maxnb;
+  int ntiles_a, ntiles_b, ntiles_l, ntiles_c, ntiles_g, ntiles_x, nsys, maxnb;
   int gcap;         // staged-particle capacity of a cell group (shared memory)
 };
 

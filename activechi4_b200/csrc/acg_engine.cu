@@ -35,7 +35,7 @@ constexpr double TAU_T = 0.20;  // MDcode/time_evolve.c:477
 constexpr int GRAPH_STEPS = 32;
 
 struct Layout {
-  int nsys = 0, nslots = 0, ncells = 0, nact = 0, maxnb = 0, ngroups = 0;
+  int nsys = 0, nslots = 0, ncells = 0, nact = 0, maxnb = 0, ngroups = 0, nboxtiles = 0, box_nmax = 0;
   std::vector<SysDesc> desc;
   size_t bytes = 0;
 };
@@ -104,9 +104,15 @@ int plan(const acg_params *params, int nsys, Layout &lay) {
     d.poff = lay.nslots;
     d.coff = lay.ncells;
     d.aoff = lay.nact;
-    d.ng = d.nc >= 3 ? (d.nc + 1) / 2 : 0;
+    d.box = d.nc >= 2 && d.nc <= MAX_BOX_NC && d.n <= MAX_BOX_N;
+    d.ng = d.nc >= 3 && !d.box ? (d.nc + 1) / 2 : 0;
     d.goff = lay.ngroups;
     lay.ngroups += d.ng * d.ng * d.ng;
+    d.xoff = lay.nboxtiles;
+    if (d.box) {
+      lay.nboxtiles += (d.ncell + BOX_CELLS - 1) / BOX_CELLS;
+      lay.box_nmax = std::max(lay.box_nmax, d.n);
+    }
     lay.nslots += (int)align_up((size_t)d.n, 32);
     lay.ncells += d.ncell;
     lay.nact += d.nact;
@@ -140,7 +146,8 @@ int plan(const acg_params *params, int nsys, Layout &lay) {
   const size_t Gn = (size_t)lay.ngroups;
   add(8 * (Gn + 1));                      // tiles_g
   add(4 * (Gn + 1));                      // gstart
-  add(32 * (Gn + S / 4 + nsys + 1));      // part_b
+  add(8 * ((size_t)lay.nboxtiles + 1));   // tiles_x
+  add(32 * (Gn + lay.nboxtiles + S / 4 + nsys + 1));  // part_b
   add(64);                                // counters
   add(sizeof(ObsDesc) * nsys);            // observables
   add(8 * (S / BLOCK_A + nsys + 1) * OBS_EMAX * OBS_NV);  // part_o
@@ -166,7 +173,7 @@ struct acg_engine {
   View v{};
   SysDesc *d_desc = nullptr;
   int tpp = 4, block = 128, gtpp = 2;
-  int ntiles_a = 0, ntiles_b = 0, ntiles_l = 0, ntiles_c = 0, ntiles_g = 0;
+  int ntiles_a = 0, ntiles_b = 0, ntiles_l = 0, ntiles_c = 0, ntiles_g = 0, ntiles_x = 0;
   int2 *d_tiles_b = nullptr;
   std::vector<int> dirty;  // systems whose forces/lists must be recomputed
   bool any_dirty = false;
@@ -197,6 +204,18 @@ GroupFn group_fn(int gtpp, int prec) {
 size_t group_smem(int gcap) { return 3 * (size_t)gcap * sizeof(double); }
 size_t list_smem(int gcap) { return ((size_t)gcap + 3 * MAX_UNION) * sizeof(float4); }
 
+GroupFn box_fn(int gtpp, int prec) {
+  switch (gtpp) {
+    case 1: return prec ? (GroupFn)k_force_box<1, 1> : (GroupFn)k_force_box<1, 0>;
+    case 2: return prec ? (GroupFn)k_force_box<2, 1> : (GroupFn)k_force_box<2, 0>;
+    case 4: return prec ? (GroupFn)k_force_box<4, 1> : (GroupFn)k_force_box<4, 0>;
+  }
+  return nullptr;
+}
+// whole-box staging: int4 fixed point (FP32) or three doubles (FP64) per particle
+size_t box_smem(int nmax, int prec) { return (size_t)nmax * (prec ? sizeof(int4) : 3 * sizeof(double)); }
+size_t box_list_smem(int nmax) { return ((size_t)nmax + 3 * MAX_BOX_CELLS) * sizeof(float4); }
+
 ForceFn force_fn(int tpp, int prec) {
 #define F(T)                                                                     \
   case T:                                                                        \
@@ -220,12 +239,20 @@ int build_tiles_b(acg_engine *e) {
     if (d.ng > 0) {
       d.tile0_b = d.goff;
       d.ntile_b = d.ng * d.ng * d.ng;
-      ng_total += d.ntile_b;
     }
   }
+  ng_total = e->lay.ngroups;
   for (int r = 0; r < e->lay.nsys; r++) {
     SysDesc &d = e->lay.desc[r];
-    if (d.ng > 0) continue;
+    if (d.box) {
+      d.tile0_b = ng_total + d.xoff;
+      d.ntile_b = (d.ncell + BOX_CELLS - 1) / BOX_CELLS;
+    }
+  }
+  ng_total += e->lay.nboxtiles;
+  for (int r = 0; r < e->lay.nsys; r++) {
+    SysDesc &d = e->lay.desc[r];
+    if (d.ng > 0 || d.box) continue;
     d.tile0_b = ng_total + (int)tb.size();
     for (int s = 0; s < d.n; s += pb) tb.push_back(make_int2(r, s));
     d.ntile_b = ng_total + (int)tb.size() - d.tile0_b;
@@ -262,6 +289,7 @@ int launch_rebuild(acg_engine *e) {
   k_cells_order<<<e->ntiles_c, 32 * CELLS_PER_TILE, 0, s>>>(v);
   k_permute<<<e->ntiles_a, BLOCK_R, 0, s>>>(v);
   if (e->ntiles_g) k_build_list_groups<<<e->ntiles_g, BLOCK_G, list_smem(v.gcap), s>>>(v);
+  if (e->ntiles_x) k_build_list_box<<<e->ntiles_x, BLOCK_X, box_list_smem(e->lay.box_nmax), s>>>(v);
   if (e->ntiles_l) k_build_list<<<e->ntiles_l, BLOCK_L, 0, s>>>(v);
   CK(cudaGetLastError());
   return ACG_OK;
@@ -270,7 +298,10 @@ int launch_rebuild(acg_engine *e) {
 int launch_force(acg_engine *e, int mode) {
   const int prec = e->lay.desc[0].precision;
   if (e->ntiles_g) group_fn(e->gtpp, prec)<<<e->ntiles_g, BLOCK_G, group_smem(e->v.gcap), e->stream>>>(e->v, mode);
-  if (e->ntiles_b) force_fn(e->tpp, prec)<<<e->ntiles_b, e->block, 0, e->stream>>>(e->v, mode, e->ntiles_g);
+  if (e->ntiles_x)
+    box_fn(e->gtpp, prec)<<<e->ntiles_x, BLOCK_X, box_smem(e->lay.box_nmax, prec), e->stream>>>(e->v, mode);
+  if (e->ntiles_b)
+    force_fn(e->tpp, prec)<<<e->ntiles_b, e->block, 0, e->stream>>>(e->v, mode, e->ntiles_g + e->ntiles_x);
   CK(cudaGetLastError());
   return ACG_OK;
 }
@@ -327,7 +358,8 @@ int build_graph(acg_engine *e, int K, cudaGraph_t *gout, cudaGraphExec_t *xout) 
   ForceFn ff = force_fn(e->tpp, prec);
   GroupFn gf = group_fn(e->gtpp, prec);
   cudaGraphNode_t prev = nullptr;
-  int mode0 = 0, use_cond = 1, tbase = e->ntiles_g;
+  GroupFn xf = box_fn(e->gtpp, prec);
+  int mode0 = 0, use_cond = 1, tbase = e->ntiles_g + e->ntiles_x;
   for (int s = 0; s < K; s++) {
     cudaGraphConditionalHandle h, ho;
     CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
@@ -355,6 +387,7 @@ int build_graph(acg_engine *e, int K, cudaGraph_t *gout, cudaGraphExec_t *xout) 
               {(void *)k_cells_order, e->ntiles_c, 32 * CELLS_PER_TILE, 0},
               {(void *)k_permute, e->ntiles_a, BLOCK_R, 0},
               {(void *)k_build_list_groups, e->ntiles_g, BLOCK_G, list_smem(v.gcap)},
+              {(void *)k_build_list_box, e->ntiles_x, BLOCK_X, box_list_smem(e->lay.box_nmax)},
               {(void *)k_build_list, e->ntiles_l, BLOCK_L, 0}};
     cudaGraphNode_t bp = nullptr;
     for (auto &k : rb) {
@@ -368,6 +401,12 @@ int build_graph(acg_engine *e, int K, cudaGraph_t *gout, cudaGraphExec_t *xout) 
     if (e->ntiles_g) {
       void *ga[] = {&v, &mode0};
       rc = add_kernel(g, &last, 1, &nb, (void *)gf, e->ntiles_g, BLOCK_G, ga, group_smem(v.gcap));
+      if (rc) return rc;
+      last = nb;
+    }
+    if (e->ntiles_x) {
+      void *xa[] = {&v, &mode0};
+      rc = add_kernel(g, &last, 1, &nb, (void *)xf, e->ntiles_x, BLOCK_X, xa, box_smem(e->lay.box_nmax, prec));
       if (rc) return rc;
       last = nb;
     }
@@ -502,7 +541,9 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   const size_t Gn = (size_t)L.ngroups;
   int2 *tg = (int2 *)take(8 * (Gn + 1));
   v.gstart = (int *)take(4 * (Gn + 1));
-  v.part_b = (double4 *)take(32 * (Gn + S / 4 + nsys + 1));
+  const size_t Xn = (size_t)L.nboxtiles;
+  int2 *tx = (int2 *)take(8 * (Xn + 1));
+  v.part_b = (double4 *)take(32 * (Gn + Xn + S / 4 + nsys + 1));
   v.counter_a = (unsigned int *)take(64);
   v.obs = (ObsDesc *)take(sizeof(ObsDesc) * nsys);
   v.part_o = (double *)take(8 * (S / BLOCK_A + nsys + 1) * OBS_EMAX * OBS_NV);
@@ -514,10 +555,11 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   v.tiles_l = tl;
   v.tiles_c = tc;
   v.tiles_g = tg;
+  v.tiles_x = tx;
   v.nsys = nsys;
   v.maxnb = L.maxnb;
 
-  std::vector<int2> h_a, h_l, h_c, h_g;
+  std::vector<int2> h_a, h_l, h_c, h_g, h_x;
   for (int r = 0; r < nsys; r++) {
     SysDesc &d = e->lay.desc[r];
     d.tile0_a = (int)h_a.size();
@@ -526,9 +568,27 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
     for (int s = 0; s < d.ncell; s += CELLS_PER_TILE) h_c.push_back(make_int2(r, s));
     if (d.ng > 0)
       for (int g = 0; g < d.ng * d.ng * d.ng; g++) h_g.push_back(make_int2(r, g));
+    else if (d.box)
+      for (int b = 0; b < (d.ncell + BOX_CELLS - 1) / BOX_CELLS; b++) h_x.push_back(make_int2(r, b));
     else
       for (int s = 0; s < d.n; s += PART_L) h_l.push_back(make_int2(r, s));
   }
+  // cell groups with the most cells first (2x2x2, then the thinner groups at
+  // odd box edges), so the blocks of a second wave are the short ones; every
+  // block writes its partial sums at its group's index, so the order of the
+  // sums does not depend on the launch order
+  auto group_cells = [&](int2 t) {
+    const SysDesc &d = e->lay.desc[t.x];
+    int c = 1;
+    for (int k = 0, q = t.y; k < 3; k++, q /= d.ng) c *= std::min(2 * (q % d.ng) + 2, d.nc) - 2 * (q % d.ng);
+    return c;
+  };
+  std::stable_sort(h_g.begin(), h_g.end(), [&](int2 a, int2 b) { return group_cells(a) > group_cells(b); });
+  // whole-box blocks of the largest systems first
+  std::stable_sort(h_x.begin(), h_x.end(),
+                   [&](int2 a, int2 b) { return e->lay.desc[a.x].n > e->lay.desc[b.x].n; });
+  e->ntiles_x = (int)h_x.size();
+  v.ntiles_x = e->ntiles_x;
   e->ntiles_a = (int)h_a.size();
   e->ntiles_l = (int)h_l.size();
   e->ntiles_c = (int)h_c.size();
@@ -537,13 +597,13 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   v.ntiles_l = e->ntiles_l;
   v.ntiles_c = e->ntiles_c;
   v.ntiles_g = e->ntiles_g;
-  // staged-particle capacity of a cell group: 1.4x the mean union (4^3 cells)
+  // staged-particle capacity of a cell group: 1.08x the mean union (4^3 cells)
   // of the densest system plus margin; a group above it uses the cell scan
   {
     double mean_u = 0;
     for (int r = 0; r < nsys; r++)
       if (L.desc[r].ng > 0) mean_u = std::max(mean_u, 64.0 * L.desc[r].n / (double)L.desc[r].ncell);
-    v.gcap = (int)align_up((size_t)(1.2 * mean_u + 64.0), 64);
+    v.gcap = (int)align_up((size_t)(1.08 * mean_u + 128.0), 32);
     v.gcap = std::min(v.gcap, 8192);
   }
   // the shared-memory limit is a property of the kernel function, shared by
@@ -558,6 +618,15 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   for (int gt : {1, 2, 4})
     for (int pr : {0, 1}) attr_ok = attr_ok && raise_smem((const void *)group_fn(gt, pr), group_smem(v.gcap));
   attr_ok = attr_ok && raise_smem((const void *)k_build_list_groups, list_smem(v.gcap));
+  if (L.box_nmax > 0) {
+    if (box_list_smem(L.box_nmax) > 227 * 1024 || box_smem(L.box_nmax, 0) > 227 * 1024) {
+      acg_destroy(e);
+      return fail(ACG_ERR_INVALID, "whole-box system too large for shared memory");
+    }
+    for (int gt : {1, 2, 4})
+      for (int pr : {0, 1}) attr_ok = attr_ok && raise_smem((const void *)box_fn(gt, pr), box_smem(L.box_nmax, pr));
+    attr_ok = attr_ok && raise_smem((const void *)k_build_list_box, box_list_smem(L.box_nmax));
+  }
   if (!attr_ok) {
     acg_destroy(e);
     return fail(ACG_ERR_CUDA, "cudaFuncSetAttribute (group kernels' shared memory) failed");
@@ -576,6 +645,9 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
            cudaSuccess) ||
       (!h_l.empty() &&
        cudaMemcpyAsync(tl, h_l.data(), h_l.size() * sizeof(int2), cudaMemcpyHostToDevice, e->stream) !=
+           cudaSuccess) ||
+      (!h_x.empty() &&
+       cudaMemcpyAsync(tx, h_x.data(), h_x.size() * sizeof(int2), cudaMemcpyHostToDevice, e->stream) !=
            cudaSuccess))
     return cleanup_fail(fail(ACG_ERR_CUDA, "initial upload failed"));
   std::vector<SysState> st(nsys);
@@ -1136,9 +1208,9 @@ int acg_bench_steps(acg_engine *e, int nchunks, size_t flush_bytes, double *ms, 
   // rebuild kernels with a non-empty grid (the node list of build_graph)
   long long steps_with_rebuild = 0;
   for (int r = 0; r < e->lay.nsys; r++) steps_with_rebuild = std::max(steps_with_rebuild, rb1[r] - rb0[r]);
-  const long long per_step = 1 + (e->ntiles_g > 0) + (e->ntiles_b > 0);
+  const long long per_step = 1 + (e->ntiles_g > 0) + (e->ntiles_x > 0) + (e->ntiles_b > 0);
   const long long per_rebuild = 3 * (e->ntiles_a > 0) + (e->lay.nsys > 0) + (e->ntiles_c > 0) +
-                                (e->ntiles_g > 0) + (e->ntiles_l > 0);
+                                (e->ntiles_g > 0) + (e->ntiles_x > 0) + (e->ntiles_l > 0);
   *ms = tot;
   if (launches) *launches = per_step * GRAPH_STEPS * nchunks + per_rebuild * steps_with_rebuild;
   return ACG_OK;

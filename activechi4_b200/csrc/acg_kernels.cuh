@@ -1138,8 +1138,82 @@ __device__ __forceinline__ void pair_rel(PairAcc &a, double dx, double dy, doubl
   }
 }
 
+// launch-bounds occupancy targets of the cell-group force kernel (blocks per
+// SM; measured best: 3 for both precisions, 80 registers without spills)
+#ifndef ACG_FORCE_MINB64
+#define ACG_FORCE_MINB64 3
+#endif
+#ifndef ACG_FORCE_MINB32
+#define ACG_FORCE_MINB32 3
+#endif
+
+// per-particle end of the force pass: active force (MDcode/cell_list+forces.c:
+// 207-218), forces stored, then the second half kick U2 (mode 0,
+// MDcode/time_evolve.c:558-567) or the pending thermostat scale (mode 1),
+// and the block's pe / virial / KE / active-virial partial sums
+__device__ __forceinline__ void particle_epilogue(const View &v, const SysDesc &d, const SysState &st, int i,
+                                                  int mode, const PairAcc &a, double &pe, double &vir,
+                                                  double &ke, double &va) {
+  const int ai = v.act[i];
+  double fx = a.fx, fy = a.fy, fz = a.fz;
+  if (ai >= 0) {
+    const char4 kk = v.kdir[d.aoff + ai];
+    const double kx = (double)kk.x, ky = (double)kk.y, kz = (double)kk.z;
+    fx += d.f0 * kx;
+    fy += d.f0 * ky;
+    fz += d.f0 * kz;
+    va += d.f0 * (kx * v.ux[i] + ky * v.uy[i] + kz * v.uz[i]);
+  }
+  v.fx[i] = fx;
+  v.fy[i] = fy;
+  v.fz[i] = fz;
+  if (mode != 2) {
+    const double vx0 = v.vx[i], vy0 = v.vy[i], vz0 = v.vz[i];
+    double px, py, pz;
+    if (mode == 0) {
+      px = __dadd_rn(vx0, __dmul_rn(fx, d.half_dt));
+      py = __dadd_rn(vy0, __dmul_rn(fy, d.half_dt));
+      pz = __dadd_rn(vz0, __dmul_rn(fz, d.half_dt));
+    } else {
+      const double s2 = st.s2;
+      px = __dmul_rn(vx0, s2);
+      py = __dmul_rn(vy0, s2);
+      pz = __dmul_rn(vz0, s2);
+    }
+    v.vx[i] = px;
+    v.vy[i] = py;
+    v.vz[i] = pz;
+    ke += px * px + py * py + pz * pz;
+  }
+  pe += a.pe;
+  vir += a.vir;
+}
+
+// block sums stored at the block's partial slot of the system; the last block
+// of the system to finish (a counter, no waiting) finalises it
+__device__ __forceinline__ void end_force_block(const View &v, int r, int slot, int mode, double pe, double vir,
+                                                double ke, double va) {
+  __shared__ double sh[32];
+  __shared__ int s_last;
+  const SysDesc &d = v.desc[r];
+  SysState &st = v.st[r];
+  pe = block_sum_dyn(pe, sh);
+  vir = block_sum_dyn(vir, sh);
+  ke = block_sum_dyn(ke, sh);
+  va = block_sum_dyn(va, sh);
+  if (threadIdx.x == 0) {
+    v.part_b[d.tile0_b + slot] = make_double4(pe, vir, ke, va);
+    __threadfence();
+    s_last = atomicAdd(&st.counter_b, 1u) == (unsigned)(d.ntile_b - 1);
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  finalize_system(v, r, mode);
+}
+
 template <int TPP, int PREC>
-__global__ void __launch_bounds__(BLOCK_G) k_force_groups(View v, int mode) {
+__global__ void __launch_bounds__(BLOCK_G, PREC ? ACG_FORCE_MINB32 : ACG_FORCE_MINB64) k_force_groups(View v, int mode) {
   // FP64: three double arrays; FP32: float4 {hi x, y, z, lo x} + float2
   // {lo y, lo z} (hi = the coordinate rounded to float, lo = the remainder),
   // 24 bytes per staged particle either way
@@ -1149,11 +1223,9 @@ __global__ void __launch_bounds__(BLOCK_G) k_force_groups(View v, int mode) {
   float4 *shi = reinterpret_cast<float4 *>(gsm_raw);
   float2 *slo = reinterpret_cast<float2 *>(gsm_raw + 16 * (size_t)v.gcap);
   __shared__ GroupStage S;
-  __shared__ double sh[32];
-  __shared__ int s_last;
   const int2 tile = v.tiles_g[blockIdx.x];
   const int r = tile.x, g = tile.y;
-  SysState &st = v.st[r];
+  const SysState &st = v.st[r];
   if (mode == 1 && !st.prime) return;
   const SysDesc &d = v.desc[r];
   GroupGeom G;
@@ -1198,21 +1270,6 @@ __global__ void __launch_bounds__(BLOCK_G) k_force_groups(View v, int mode) {
     const double4 pi = valid ? v.pos[i] : make_double4(0, 0, 0, 0);
     const int ti = (int)pi.w;
     const int nn = valid ? v.nbn[i] : 0;
-    // per-particle inputs of the epilogue, loaded before the pair loop
-    const int ai = valid && lane == 0 ? v.act[i] : -1;
-    double vx0 = 0.0, vy0 = 0.0, vz0 = 0.0, uxi = 0.0, uyi = 0.0, uzi = 0.0;
-    if (valid && lane == 0) {
-      if (mode != 2) {
-        vx0 = v.vx[i];
-        vy0 = v.vy[i];
-        vz0 = v.vz[i];
-      }
-      if (ai >= 0) {
-        uxi = v.ux[i];
-        uyi = v.uy[i];
-        uzi = v.uz[i];
-      }
-    }
     PairAcc a = {0.0, 0.0, 0.0, 0.0, 0.0};
     if (PREC == 1 && valid && staged && nn >= 0) {
       const float4 hi = shi[qs];
@@ -1309,51 +1366,274 @@ __global__ void __launch_bounds__(BLOCK_G) k_force_groups(View v, int mode) {
       a.vir += __shfl_xor_sync(0xffffffffu, a.vir, o);
     }
     if (!valid || lane != 0) continue;
-    double fx = a.fx, fy = a.fy, fz = a.fz;
-    if (ai >= 0) {  // active force (MDcode/cell_list+forces.c:207-218)
-      const char4 kk = v.kdir[d.aoff + ai];
-      const double kx = (double)kk.x, ky = (double)kk.y, kz = (double)kk.z;
-      fx += d.f0 * kx;
-      fy += d.f0 * ky;
-      fz += d.f0 * kz;
-      va += d.f0 * (kx * uxi + ky * uyi + kz * uzi);
-    }
-    v.fx[i] = fx;
-    v.fy[i] = fy;
-    v.fz[i] = fz;
-    if (mode != 2) {
-      double px, py, pz;
-      if (mode == 0) {  // U2 (MDcode/time_evolve.c:558-567)
-        px = __dadd_rn(vx0, __dmul_rn(fx, d.half_dt));
-        py = __dadd_rn(vy0, __dmul_rn(fy, d.half_dt));
-        pz = __dadd_rn(vz0, __dmul_rn(fz, d.half_dt));
-      } else {
-        const double s2 = st.s2;
-        px = __dmul_rn(vx0, s2);
-        py = __dmul_rn(vy0, s2);
-        pz = __dmul_rn(vz0, s2);
-      }
-      v.vx[i] = px;
-      v.vy[i] = py;
-      v.vz[i] = pz;
-      ke += px * px + py * py + pz * pz;
-    }
-    pe += a.pe;
-    vir += a.vir;
+    particle_epilogue(v, d, st, i, mode, a, pe, vir, ke, va);
   }
-  pe = block_sum_dyn(pe, sh);
-  vir = block_sum_dyn(vir, sh);
-  ke = block_sum_dyn(ke, sh);
-  va = block_sum_dyn(va, sh);
-  if (threadIdx.x == 0) {
-    v.part_b[blockIdx.x] = make_double4(pe, vir, ke, va);
-    __threadfence();
-    s_last = atomicAdd(&st.counter_b, 1u) == (unsigned)(d.ntile_b - 1);
+  end_force_block(v, r, g, mode, pe, vir, ke, va);
+}
+
+// ---------------------------------------------------------------------------
+// whole-box kernels: systems with 2 to 4 cells per side (N up to ~3.5k at
+// density 1.2).  A 2x2x2 cell group of such a box would stage the whole box
+// (and, at 3 cells per side, part of it twice) for each of its 8 groups; here
+// every block stages the system once and handles BOX_CELLS cells of it.
+// List entries are system-local slot indices (| type << 15); entry k of slot
+// s sits in chunk k/4 at uint2 index (k/4)*N + s.
+
+__device__ __forceinline__ uint16_t *box_list(const View &v, const SysDesc &d) {
+  return reinterpret_cast<uint16_t *>(v.nbl) + 2 * (size_t)d.poff * v.maxnb;
+}
+
+// 32-bit fixed point of a reduced coordinate (x * 2^32, two's-complement
+// wrap): the difference of two is the minimum-image separation, exactly
+__device__ __forceinline__ int fixed32(double x) {
+  return (int)(unsigned)(unsigned long long)__double2ll_rz(x * 4294967296.0);
+}
+
+// per-system cell starts (system-local slots) and the per-cell runs padded to
+// a multiple of four, for <= 64 cells
+__device__ __forceinline__ void box_cells(const View &v, const SysDesc &d, int *cst, int *pre4) {
+  const int nce = d.ncell;
+  __shared__ int wtot;
+  int x = 0;
+  if (threadIdx.x < MAX_BOX_CELLS) {
+    const int t = threadIdx.x, l = t & 31;
+    if (t < nce) {
+      cst[t] = v.cstart[d.coff + t];
+      x = (v.ccount[d.coff + t] + 3) & ~3;
+    }
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (l >= o) x += y;
+    }
+    if (t == 31) wtot = x;
   }
   __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  finalize_system(v, r, mode);
+  if (threadIdx.x < MAX_BOX_CELLS) {
+    const int incl = x + (threadIdx.x >= 32 ? wtot : 0);
+    if (threadIdx.x < nce) pre4[threadIdx.x + 1] = incl;
+    if (threadIdx.x == 0) {
+      pre4[0] = 0;
+      cst[nce] = d.n;
+    }
+  }
+  __syncthreads();
+}
+
+// lists of a whole box: one warp per cell of the block, one lane per particle;
+// the 27 neighbour cells (with their periodic image shifts; at 2 cells per side
+// a cell appears under two shifts, of which at most one can be in range since
+// L > 2 x the list cut) are tested against the staged reduced coordinates
+__global__ void __launch_bounds__(BLOCK_X) k_build_list_box(View v) {
+  extern __shared__ float4 xstg[];
+  __shared__ int cst[MAX_BOX_CELLS + 1], pre4[MAX_BOX_CELLS + 1];
+  const int2 tile = v.tiles_x[blockIdx.x];
+  const int r = tile.x, b = tile.y;
+  if (!v.st[r].rebuild) return;
+  const SysDesc &d = v.desc[r];
+  const int nc = d.nc, nce = d.ncell, n = d.n;
+  box_cells(v, d, cst, pre4);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (int c = warp; c < nce; c += nwarps) {
+    const int s0 = cst[c], m = cst[c + 1] - s0, p0 = pre4[c], m4 = pre4[c + 1] - p0;
+    for (int k = lane; k < m4; k += 32) {
+      float4 f;
+      if (k < m) {
+        const double4 p = v.pos_s[d.poff + s0 + k];
+        f = make_float4((float)p.x, (float)p.y, (float)p.z, __int_as_float((s0 + k) | ((int)p.w << 15)));
+      } else {
+        f = make_float4(1e18f, 1e18f, 1e18f, __int_as_float(0));
+      }
+      xstg[p0 + k] = f;
+    }
+  }
+  __syncthreads();
+  const double iL2 = 1.0 / (d.L * d.L);
+  float lc[3];
+  for (int k = 0; k < 3; k++) lc[k] = (float)(lcut2_of(d, k) * iL2 * (1.0 + 1e-5));
+  const bool one_cut = lc[0] == lc[1] && lc[1] == lc[2];
+  uint2 *lst = reinterpret_cast<uint2 *>(box_list(v, d));
+  const int maxnb = v.maxnb;
+  const int c = b * BOX_CELLS + warp;
+  if (c < nce) {
+    const int cx = c % nc, cy = (c / nc) % nc, cz = c / (nc * nc);
+    const int m = cst[c + 1] - cst[c];
+    for (int w0 = 0; w0 < m; w0 += 32) {
+      const int w = w0 + lane;
+      const bool valid = w < m;
+      const int sl = cst[c] + w, ps = pre4[c] + w;
+      const float4 fi = valid ? xstg[ps] : make_float4(-1e18f, -1e18f, -1e18f, __int_as_float(0));
+      const int ti = __float_as_int(fi.w) >> 15;
+      const float c0 = ti == 0 ? lc[0] : lc[1], c1 = ti == 0 ? lc[1] : lc[2];
+      unsigned long long pend = 0ull;
+      int nn = 0;
+      for (int dz = -1; dz <= 1; dz++)
+        for (int dy = -1; dy <= 1; dy++)
+          for (int dx = -1; dx <= 1; dx++) {
+            const int ax = cx + dx, ay = cy + dy, az = cz + dz;
+            const int sx = ax < 0 ? -1 : (ax >= nc ? 1 : 0), sy = ay < 0 ? -1 : (ay >= nc ? 1 : 0),
+                      sz = az < 0 ? -1 : (az >= nc ? 1 : 0);
+            const int c2 = (ax - sx * nc) + (ay - sy * nc) * nc + (az - sz * nc) * nc * nc;
+            // candidate image x_j + s: compare x_i - s with x_j
+            const float xi = fi.x - (float)sx, yi = fi.y - (float)sy, zi = fi.z - (float)sz;
+            const int q1 = pre4[c2 + 1];
+            for (int q = pre4[c2]; q < q1; q += 4) {
+              int code[4];
+              bool ok[4];
+#pragma unroll
+              for (int e = 0; e < 4; e++) {
+                const float4 fj = xstg[q + e];
+                const float ex = xi - fj.x, ey = yi - fj.y, ez = zi - fj.z;
+                const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+                code[e] = __float_as_int(fj.w);
+                const float cut = one_cut ? c0 : ((code[e] >> 15) ? c1 : c0);
+                ok[e] = r2 < cut && q + e != ps;
+              }
+#pragma unroll
+              for (int e = 0; e < 4; e++)
+                if (ok[e]) {
+                  pend |= (unsigned long long)(code[e] & 0xffff) << (16 * (nn & 3));
+                  nn++;
+                  if ((nn & 3) == 0) {
+                    if (nn <= maxnb)
+                      lst[(size_t)((nn >> 2) - 1) * n + sl] = make_uint2((unsigned)pend, (unsigned)(pend >> 32));
+                    pend = 0ull;
+                  }
+                }
+            }
+          }
+      if (valid) {
+        if ((nn & 3) && nn <= maxnb) lst[(size_t)(nn >> 2) * n + sl] = make_uint2((unsigned)pend, (unsigned)(pend >> 32));
+        const int i = d.poff + sl;
+        if (nn > maxnb) {
+          v.nbn[i] = -1;
+          atomicAdd(&v.st[r].overflow, 1);
+        } else {
+          v.nbn[i] = nn;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  const int ca = b * BOX_CELLS, cb = min(nce, ca + BOX_CELLS);
+  for (int sl = cst[ca] + threadIdx.x; sl < cst[cb]; sl += blockDim.x) copy_back(v, d.poff + sl);
+}
+
+// pair forces of a whole box from its lists.  FP32: staged 32-bit fixed-point
+// reduced coordinates, separation = wrapped integer difference x L/2^32 (one
+// rounding); FP64: staged reduced coordinates, minimum image d - rint(d).
+template <int TPP, int PREC>
+__global__ void __launch_bounds__(BLOCK_X) k_force_box(View v, int mode) {
+  extern __shared__ __align__(16) unsigned char xsm[];
+  const int2 tile = v.tiles_x[blockIdx.x];
+  const int r = tile.x, b = tile.y;
+  const SysState &st = v.st[r];
+  if (mode == 1 && !st.prime) return;
+  const SysDesc &d = v.desc[r];
+  const int n = d.n, nce = d.ncell;
+  int4 *sq = reinterpret_cast<int4 *>(xsm);
+  double *sx = reinterpret_cast<double *>(xsm), *sy = sx + n, *sz = sy + n;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    const double4 p = v.pos[d.poff + k];
+    if (PREC == 1)
+      sq[k] = make_int4(fixed32(p.x), fixed32(p.y), fixed32(p.z), (int)p.w);
+    else {
+      sx[k] = p.x;
+      sy[k] = p.y;
+      sz[k] = p.z;
+    }
+  }
+  const int ca = b * BOX_CELLS, cb = min(nce, ca + BOX_CELLS);
+  const int s_lo = v.cstart[d.coff + ca], s_hi = cb < nce ? v.cstart[d.coff + cb] : n;
+  __syncthreads();
+  const uint2 *lst = reinterpret_cast<const uint2 *>(box_list(v, d));
+  const double L = d.L;
+  const float scale = (float)(L * (1.0 / 4294967296.0));
+  double pe = 0.0, vir = 0.0, ke = 0.0, va = 0.0;
+  const int lane = threadIdx.x % TPP, nper = blockDim.x / TPP;
+  for (int t0 = s_lo; t0 < s_hi; t0 += nper) {
+    const int sl = t0 + threadIdx.x / TPP;
+    const bool valid = sl < s_hi;
+    const int i = d.poff + (valid ? sl : s_lo);
+    const int nn = valid ? v.nbn[i] : 0;
+    PairAcc a = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (valid && nn >= 0) {
+      const int nch = (nn + 3) >> 2;
+      const uint2 *lp = lst + sl;
+      uint2 w = lane < nch ? __ldg(lp + (size_t)lane * n) : make_uint2(0u, 0u);
+      if (PREC == 1) {
+        const int4 qi = sq[sl];
+        PairAccF fa = {0.f, 0.f, 0.f, 0.f, 0.f}, fb = {0.f, 0.f, 0.f, 0.f, 0.f};
+        for (int c = lane; c < nch; c += TPP) {
+          const uint2 wn = c + TPP < nch ? __ldg(lp + (size_t)(c + TPP) * n) : make_uint2(0u, 0u);
+          const int k0 = 4 * c;
+#pragma unroll
+          for (int e = 0; e < 4; e++) {
+            const int code = ((e < 2 ? w.x : w.y) >> (16 * (e & 1))) & 0xffff;
+            if (e == 0 || k0 + e < nn) {
+              const int4 qj = sq[code & 0x7fff];
+              const float dx = (float)(int)((unsigned)qi.x - (unsigned)qj.x) * scale;
+              const float dy = (float)(int)((unsigned)qi.y - (unsigned)qj.y) * scale;
+              const float dz = (float)(int)((unsigned)qi.z - (unsigned)qj.z) * scale;
+              pair_f32(e & 1 ? fb : fa, dx, dy, dz, qi.w + (code >> 15));
+            }
+          }
+          w = wn;
+        }
+        a.fx = (double)fa.fx + (double)fb.fx;
+        a.fy = (double)fa.fy + (double)fb.fy;
+        a.fz = (double)fa.fz + (double)fb.fz;
+        a.pe = (double)fa.pe + (double)fb.pe;
+        a.vir = (double)fa.vir + (double)fb.vir;
+      } else {
+        const double xi = sx[sl], yi = sy[sl], zi = sz[sl];
+        const int ti = (int)v.pos[i].w;
+        PairAcc bb = {0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int c = lane; c < nch; c += TPP) {
+          const uint2 wn = c + TPP < nch ? __ldg(lp + (size_t)(c + TPP) * n) : make_uint2(0u, 0u);
+          const int k0 = 4 * c;
+#pragma unroll
+          for (int e = 0; e < 4; e++) {
+            const int code = ((e < 2 ? w.x : w.y) >> (16 * (e & 1))) & 0xffff;
+            if (e == 0 || k0 + e < nn) {
+              const int q = code & 0x7fff;
+              pair_rel<0>(e & 1 ? bb : a, min_image(xi - sx[q]) * L, min_image(yi - sy[q]) * L,
+                          min_image(zi - sz[q]) * L, ti + (code >> 15));
+            }
+          }
+          w = wn;
+        }
+        a.fx += bb.fx;
+        a.fy += bb.fy;
+        a.fz += bb.fz;
+        a.pe += bb.pe;
+        a.vir += bb.vir;
+      }
+    } else if (valid) {
+      // list overflow: all particles of the 27 neighbour images (each pair once)
+      const double4 pi = v.pos[i];
+      const int ti = (int)pi.w;
+      const double L2 = L * L;
+      for (int k = lane; k < n; k += TPP) {
+        if (k == sl) continue;
+        const double4 pj = v.pos[d.poff + k];
+        if (PREC == 0)
+          pair_fp64(a, pi, ti, pj, L, L2);
+        else
+          pair_fp32(a, pi, ti, pj, L, L2);
+      }
+    }
+#pragma unroll
+    for (int o = TPP / 2; o > 0; o >>= 1) {
+      a.fx += __shfl_xor_sync(0xffffffffu, a.fx, o);
+      a.fy += __shfl_xor_sync(0xffffffffu, a.fy, o);
+      a.fz += __shfl_xor_sync(0xffffffffu, a.fz, o);
+      a.pe += __shfl_xor_sync(0xffffffffu, a.pe, o);
+      a.vir += __shfl_xor_sync(0xffffffffu, a.vir, o);
+    }
+    if (!valid || lane != 0) continue;
+    particle_epilogue(v, d, st, i, mode, a, pe, vir, ke, va);
+  }
+  end_force_block(v, r, b, mode, pe, vir, ke, va);
 }
 
 // ---------------------------------------------------------------------------

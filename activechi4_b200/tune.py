@@ -1,10 +1,10 @@
 """Launch-shape autotuner for an Engine.
 
 Times the force stage (acg_time_stage, forces only, so the trajectory is not
-changed) for each candidate launch shape of the two force kernels and keeps
-the fastest: threads per particle of the cell-group kernel (boxes with >= 3
-cells per side) and threads per particle x block size of the per-particle
-kernel (2-cell boxes).  Each candidate is timed over `reps` launches after a
+changed) for each candidate launch shape of the force kernels and keeps the
+fastest: threads per particle of the cell-group and whole-box kernels, and
+threads per particle x block size of the per-particle kernel (boxes with fewer
+than 3 cells per side that are too large for the whole-box kernels).  Each candidate is timed over `reps` launches after a
 warm launch.
 """
 from __future__ import annotations
@@ -17,8 +17,12 @@ SMALL_SHAPES = ((1, 64), (1, 128), (2, 128), (2, 256), (4, 128), (4, 256), (8, 2
 
 
 def autotune(e: Engine, reps: int = 20, verbose: bool = False) -> dict:
-    # boxes with 2 cells per side (Ncell = (int)((int)L / 2.85) = 2) use the per-particle kernel
-    has_small = any(int(int(box_length(e.n(r))) / 2.85) < 3 for r in range(e.nsys))
+    # the per-particle kernel serves boxes with fewer than 3 cells per side
+    # (Ncell = (int)((int)L / 2.85)) that are too large for the whole-box kernels
+    def per_particle(r):
+        nc = int(int(box_length(e.n(r))) / 2.85)
+        return nc < 2 or (nc < 3 and e.n(r) > 8192)
+    has_small = any(per_particle(r) for r in range(e.nsys))
     best_g, best_t = None, float("inf")
     for g in GROUP_TPP:
         e.set_group_tpp(g)
