@@ -89,7 +89,7 @@ int resolve(const acg_params &p, SysDesc &d) {
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-int plan(const acg_params *params, int nsys, Layout &lay) {
+int plan(const acg_params *params, int nsys, Layout &lay, int nsm) {
   if (!params || nsys < 1) return fail(ACG_ERR_INVALID, "need at least one system");
   lay = Layout();
   lay.nsys = nsys;
@@ -108,15 +108,25 @@ int plan(const acg_params *params, int nsys, Layout &lay) {
     d.ng = d.nc >= 3 && !d.box ? (d.nc + 1) / 2 : 0;
     d.goff = lay.ngroups;
     lay.ngroups += d.ng * d.ng * d.ng;
-    d.xoff = lay.nboxtiles;
-    if (d.box) {
-      lay.nboxtiles += (d.ncell + BOX_CELLS - 1) / BOX_CELLS;
-      lay.box_nmax = std::max(lay.box_nmax, d.n);
-    }
+    if (d.box) lay.box_nmax = std::max(lay.box_nmax, d.n);
     lay.nslots += (int)align_up((size_t)d.n, 32);
     lay.ncells += d.ncell;
     lay.nact += d.nact;
     dens_max = std::max(dens_max, (double)d.n / (d.L * d.L * d.L));
+  }
+  // whole-box partition: about two blocks per SM over all whole-box cells,
+  // 1 to BOX_CELLS cells per block (the per-system sums do not depend on it)
+  {
+    long long cells = 0;
+    for (int r = 0; r < nsys; r++)
+      if (lay.desc[r].box) cells += lay.desc[r].ncell;
+    const int cpb = (int)std::max(1LL, std::min((long long)BOX_CELLS, cells / (2LL * std::max(nsm, 1))));
+    for (int r = 0; r < nsys; r++) {
+      SysDesc &d = lay.desc[r];
+      d.cpb = cpb;
+      d.xoff = lay.nboxtiles;
+      if (d.box) lay.nboxtiles += (d.ncell + cpb - 1) / cpb;
+    }
   }
   // neighbour-row capacity: 1.45x the ideal-gas count within the widest list
   // cut plus margin; rare denser particles fall back to the cell scan
@@ -148,6 +158,7 @@ int plan(const acg_params *params, int nsys, Layout &lay) {
   add(4 * (Gn + 1));                      // gstart
   add(8 * ((size_t)lay.nboxtiles + 1));   // tiles_x
   add(32 * (Gn + lay.nboxtiles + S / 4 + nsys + 1));  // part_b
+  add(32 * S);                            // pacc
   add(64);                                // counters
   add(sizeof(ObsDesc) * nsys);            // observables
   add(8 * (S / BLOCK_A + nsys + 1) * OBS_EMAX * OBS_NV);  // part_o
@@ -165,6 +176,13 @@ namespace acg {
 int set_last_error(int code, const std::string &msg) { return fail(code, msg); }
 }  // namespace acg
 
+// whole-step kernel (one block per system) for engines whose systems are all
+// whole-box; off by default: one block per system leaves a lone small system
+// on one SM and balances a batch of uneven sizes poorly
+#ifndef ACG_FUSED_STEPS
+#define ACG_FUSED_STEPS 0
+#endif
+
 struct acg_engine {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -172,7 +190,8 @@ struct acg_engine {
   void *arena = nullptr;
   View v{};
   SysDesc *d_desc = nullptr;
-  int tpp = 4, block = 128, gtpp = 2;
+  int tpp = 4, block = 128, gtpp = 2, btpp = 2;  // btpp: whole-box kernels
+  bool fused = false;  // every system whole-box: one k_steps_box launch per step
   int ntiles_a = 0, ntiles_b = 0, ntiles_l = 0, ntiles_c = 0, ntiles_g = 0, ntiles_x = 0;
   int2 *d_tiles_b = nullptr;
   std::vector<int> dirty;  // systems whose forces/lists must be recomputed
@@ -216,6 +235,17 @@ GroupFn box_fn(int gtpp, int prec) {
 size_t box_smem(int nmax, int prec) { return (size_t)nmax * (prec ? sizeof(int4) : 3 * sizeof(double)); }
 size_t box_list_smem(int nmax) { return ((size_t)nmax + 3 * MAX_BOX_CELLS) * sizeof(float4); }
 
+using StepFn = void (*)(View, int);
+StepFn steps_fn(int gtpp, int prec) {
+  switch (gtpp) {
+    case 1: return prec ? (StepFn)k_steps_box<1, 1> : (StepFn)k_steps_box<1, 0>;
+    case 2: return prec ? (StepFn)k_steps_box<2, 1> : (StepFn)k_steps_box<2, 0>;
+    case 4: return prec ? (StepFn)k_steps_box<4, 1> : (StepFn)k_steps_box<4, 0>;
+  }
+  return nullptr;
+}
+size_t steps_smem(int nmax, int prec) { return std::max(box_list_smem(nmax), box_smem(nmax, prec)); }
+
 ForceFn force_fn(int tpp, int prec) {
 #define F(T)                                                                     \
   case T:                                                                        \
@@ -246,7 +276,7 @@ int build_tiles_b(acg_engine *e) {
     SysDesc &d = e->lay.desc[r];
     if (d.box) {
       d.tile0_b = ng_total + d.xoff;
-      d.ntile_b = (d.ncell + BOX_CELLS - 1) / BOX_CELLS;
+      d.ntile_b = (d.ncell + d.cpb - 1) / d.cpb;
     }
   }
   ng_total += e->lay.nboxtiles;
@@ -299,7 +329,7 @@ int launch_force(acg_engine *e, int mode) {
   const int prec = e->lay.desc[0].precision;
   if (e->ntiles_g) group_fn(e->gtpp, prec)<<<e->ntiles_g, BLOCK_G, group_smem(e->v.gcap), e->stream>>>(e->v, mode);
   if (e->ntiles_x)
-    box_fn(e->gtpp, prec)<<<e->ntiles_x, BLOCK_X, box_smem(e->lay.box_nmax, prec), e->stream>>>(e->v, mode);
+    box_fn(e->btpp, prec)<<<e->ntiles_x, BLOCK_X, box_smem(e->lay.box_nmax, prec), e->stream>>>(e->v, mode);
   if (e->ntiles_b)
     force_fn(e->tpp, prec)<<<e->ntiles_b, e->block, 0, e->stream>>>(e->v, mode, e->ntiles_g + e->ntiles_x);
   CK(cudaGetLastError());
@@ -307,6 +337,12 @@ int launch_force(acg_engine *e, int mode) {
 }
 
 int launch_step_eager(acg_engine *e) {
+  if (e->fused) {
+    const int prec = e->lay.desc[0].precision;
+    steps_fn(e->btpp, prec)<<<e->lay.nsys, BLOCK_F, steps_smem(e->lay.box_nmax, prec), e->stream>>>(e->v, 1);
+    CK(cudaGetLastError());
+    return ACG_OK;
+  }
   k_kick_drift<<<e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, 0, e->stream>>>(e->v, 0, 0, 0);
   CK(cudaGetLastError());
   int rc = launch_rebuild(e);
@@ -355,10 +391,29 @@ int build_graph(acg_engine *e, int K, cudaGraph_t *gout, cudaGraphExec_t *xout) 
   CK(cudaGraphCreate(&g, 0));
   View v = e->v;
   const int prec = e->lay.desc[0].precision;
+  if (e->fused) {
+    // one whole-step launch per step, all systems of the batch
+    StepFn sf = steps_fn(e->btpp, prec);
+    cudaGraphNode_t prev = nullptr;
+    int one = 1;
+    for (int s = 0; s < K; s++) {
+      void *a[] = {&v, &one};
+      cudaGraphNode_t nn;
+      int rc = add_kernel(g, prev ? &prev : nullptr, prev ? 1 : 0, &nn, (void *)sf, e->lay.nsys, BLOCK_F, a,
+                          steps_smem(e->lay.box_nmax, prec));
+      if (rc) return rc;
+      prev = nn;
+    }
+    cudaGraphExec_t x;
+    CK(cudaGraphInstantiate(&x, g, 0));
+    *gout = g;
+    *xout = x;
+    return ACG_OK;
+  }
   ForceFn ff = force_fn(e->tpp, prec);
   GroupFn gf = group_fn(e->gtpp, prec);
   cudaGraphNode_t prev = nullptr;
-  GroupFn xf = box_fn(e->gtpp, prec);
+  GroupFn xf = box_fn(e->btpp, prec);
   int mode0 = 0, use_cond = 1, tbase = e->ntiles_g + e->ntiles_x;
   for (int s = 0; s < K; s++) {
     cudaGraphConditionalHandle h, ho;
@@ -472,7 +527,8 @@ int acg_params_default(acg_params *p, int n) {
 
 int acg_footprint(const acg_params *params, int nsys, size_t *bytes) {
   Layout lay;
-  int rc = plan(params, nsys, lay);
+  // the most whole-box blocks any device would get (one cell per block)
+  int rc = plan(params, nsys, lay, 1 << 20);
   if (rc) return rc;
   if (bytes) *bytes = lay.bytes;
   return ACG_OK;
@@ -482,7 +538,12 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   if (!out) return fail(ACG_ERR_INVALID, "null out");
   *out = nullptr;
   acg_engine *e = new acg_engine();
-  int rc = plan(params, nsys, e->lay);
+  int nsm = 0;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || nsm < 1) {
+    cudaGetLastError();
+    nsm = 148;
+  }
+  int rc = plan(params, nsys, e->lay, nsm);
   if (rc) {
     delete e;
     return rc;
@@ -544,6 +605,7 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   const size_t Xn = (size_t)L.nboxtiles;
   int2 *tx = (int2 *)take(8 * (Xn + 1));
   v.part_b = (double4 *)take(32 * (Gn + Xn + S / 4 + nsys + 1));
+  v.pacc = (double4 *)take(32 * S);
   v.counter_a = (unsigned int *)take(64);
   v.obs = (ObsDesc *)take(sizeof(ObsDesc) * nsys);
   v.part_o = (double *)take(8 * (S / BLOCK_A + nsys + 1) * OBS_EMAX * OBS_NV);
@@ -569,7 +631,7 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
     if (d.ng > 0)
       for (int g = 0; g < d.ng * d.ng * d.ng; g++) h_g.push_back(make_int2(r, g));
     else if (d.box)
-      for (int b = 0; b < (d.ncell + BOX_CELLS - 1) / BOX_CELLS; b++) h_x.push_back(make_int2(r, b));
+      for (int b = 0; b < (d.ncell + d.cpb - 1) / d.cpb; b++) h_x.push_back(make_int2(r, b));
     else
       for (int s = 0; s < d.n; s += PART_L) h_l.push_back(make_int2(r, s));
   }
@@ -626,7 +688,14 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
     for (int gt : {1, 2, 4})
       for (int pr : {0, 1}) attr_ok = attr_ok && raise_smem((const void *)box_fn(gt, pr), box_smem(L.box_nmax, pr));
     attr_ok = attr_ok && raise_smem((const void *)k_build_list_box, box_list_smem(L.box_nmax));
+    for (int gt : {1, 2, 4})
+      for (int pr : {0, 1}) attr_ok = attr_ok && raise_smem((const void *)steps_fn(gt, pr), steps_smem(L.box_nmax, pr));
   }
+  // one cell per whole-box block (a lone small system): four threads per
+  // particle keep more list loads in flight
+  e->btpp = L.desc[0].cpb == 1 ? 4 : 2;
+  e->fused = ACG_FUSED_STEPS != 0;
+  for (int r = 0; r < nsys; r++) e->fused = e->fused && L.desc[r].box;
   if (!attr_ok) {
     acg_destroy(e);
     return fail(ACG_ERR_CUDA, "cudaFuncSetAttribute (group kernels' shared memory) failed");
@@ -994,6 +1063,7 @@ int acg_set_group_tpp(acg_engine *e, int gtpp) {
   CK(cudaSetDevice(e->device));
   CK(cudaStreamSynchronize(e->stream));
   e->gtpp = gtpp;
+  e->btpp = gtpp;
   drop_graphs(e);
   return ACG_OK;
 }
@@ -1208,11 +1278,11 @@ int acg_bench_steps(acg_engine *e, int nchunks, size_t flush_bytes, double *ms, 
   // rebuild kernels with a non-empty grid (the node list of build_graph)
   long long steps_with_rebuild = 0;
   for (int r = 0; r < e->lay.nsys; r++) steps_with_rebuild = std::max(steps_with_rebuild, rb1[r] - rb0[r]);
-  const long long per_step = 1 + (e->ntiles_g > 0) + (e->ntiles_x > 0) + (e->ntiles_b > 0);
+  const long long per_step = e->fused ? 1 : 1 + (e->ntiles_g > 0) + (e->ntiles_x > 0) + (e->ntiles_b > 0);
   const long long per_rebuild = 3 * (e->ntiles_a > 0) + (e->lay.nsys > 0) + (e->ntiles_c > 0) +
                                 (e->ntiles_g > 0) + (e->ntiles_x > 0) + (e->ntiles_l > 0);
   *ms = tot;
-  if (launches) *launches = per_step * GRAPH_STEPS * nchunks + per_rebuild * steps_with_rebuild;
+  if (launches) *launches = per_step * GRAPH_STEPS * nchunks + (e->fused ? 0 : per_rebuild * steps_with_rebuild);
   return ACG_OK;
 }
 

@@ -116,6 +116,63 @@ __device__ void shuffle_component(const View &v, int r, int comp, long long step
 }
 
 // ---------------------------------------------------------------------------
+// U3 U2 (pending thermostat scales and the half kick) and U1 for one
+// particle, in the reference's order of roundings; returns |x_u - x_old|^2
+// (reduced units) for the rebuild test
+__device__ __forceinline__ double kick_drift_one(const View &v, const SysDesc &d, int i, double s1, double s2) {
+  const double hdt = d.half_dt, dt = d.dt, il = d.invL;
+  // v_b * s1 + F dt/2
+  double px = __dadd_rn(__dmul_rn(__dmul_rn(v.vx[i], s2), s1), __dmul_rn(v.fx[i], hdt));
+  double py = __dadd_rn(__dmul_rn(__dmul_rn(v.vy[i], s2), s1), __dmul_rn(v.fy[i], hdt));
+  double pz = __dadd_rn(__dmul_rn(__dmul_rn(v.vz[i], s2), s1), __dmul_rn(v.fz[i], hdt));
+  double ddx = __dmul_rn(__dmul_rn(px, dt), il);
+  double ddy = __dmul_rn(__dmul_rn(py, dt), il);
+  double ddz = __dmul_rn(__dmul_rn(pz, dt), il);
+  double4 p = v.pos[i];
+  double ux = __dadd_rn(v.ux[i], ddx), uy = __dadd_rn(v.uy[i], ddy), uz = __dadd_rn(v.uz[i], ddz);
+  p.x = wrap_unit(__dadd_rn(p.x, ddx));
+  p.y = wrap_unit(__dadd_rn(p.y, ddy));
+  p.z = wrap_unit(__dadd_rn(p.z, ddz));
+  double ex = __dadd_rn(ux, -v.ox[i]), ey = __dadd_rn(uy, -v.oy[i]), ez = __dadd_rn(uz, -v.oz[i]);
+  v.vx[i] = px;
+  v.vy[i] = py;
+  v.vz[i] = pz;
+  v.ux[i] = ux;
+  v.uy[i] = uy;
+  v.uz[i] = uz;
+  v.pos[i] = p;
+  return __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
+}
+
+// rebuild decision of one system from its max squared displacement (reduced)
+__device__ __forceinline__ int rebuild_decision(const SysDesc &d, SysState &st, double maxd_red) {
+  const double m = __dmul_rn(__dmul_rn(maxd_red, d.L), d.L);
+  st.maxD_last = m;
+  const int rb = (__dmul_rn(d.rebuild_factor, m) > d.skin2) || st.force_rebuild;
+  st.rebuild = rb;
+  st.force_rebuild = 0;
+  return rb;
+}
+
+// observable events of one system due at the end of its current step
+// (frame = loop index step); returns whether there are any
+__device__ __forceinline__ int obs_due(const ObsDesc &o, SysState &st) {
+  if (o.n_events == 0) {
+    st.obs_lo = st.obs_hi = 0;
+    return 0;
+  }
+  const long long step = st.step;
+  int c = st.obs_cur;
+  while (c < o.n_events && o.ev_step[c] < step) c++;
+  const int lo = c;
+  while (c < o.n_events && o.ev_step[c] == step && c - lo < OBS_EMAX) c++;
+  st.obs_lo = lo;
+  st.obs_hi = c;
+  st.obs_cur = c;
+  return c > lo;
+}
+
+// ---------------------------------------------------------------------------
 // stage 1: kick + drift (+ shuffle blocks) + rebuild decision
 __global__ void __launch_bounds__(BLOCK_A) k_kick_drift(View v, int use_cond, cudaGraphConditionalHandle h,
                                                         cudaGraphConditionalHandle h_obs) {
@@ -129,32 +186,7 @@ __global__ void __launch_bounds__(BLOCK_A) k_kick_drift(View v, int use_cond, cu
     r = t.x;
     const SysDesc &d = v.desc[r];
     int loc = t.y + threadIdx.x;
-    if (loc < d.n) {
-      const int i = d.poff + loc;
-      const double s2 = v.st[r].s2, s1 = v.st[r].s1;
-      const double hdt = d.half_dt, dt = d.dt, il = d.invL;
-      // v_b * s1 + F dt/2, in the reference's order of roundings
-      double px = __dadd_rn(__dmul_rn(__dmul_rn(v.vx[i], s2), s1), __dmul_rn(v.fx[i], hdt));
-      double py = __dadd_rn(__dmul_rn(__dmul_rn(v.vy[i], s2), s1), __dmul_rn(v.fy[i], hdt));
-      double pz = __dadd_rn(__dmul_rn(__dmul_rn(v.vz[i], s2), s1), __dmul_rn(v.fz[i], hdt));
-      double ddx = __dmul_rn(__dmul_rn(px, dt), il);
-      double ddy = __dmul_rn(__dmul_rn(py, dt), il);
-      double ddz = __dmul_rn(__dmul_rn(pz, dt), il);
-      double4 p = v.pos[i];
-      double ux = __dadd_rn(v.ux[i], ddx), uy = __dadd_rn(v.uy[i], ddy), uz = __dadd_rn(v.uz[i], ddz);
-      p.x = wrap_unit(__dadd_rn(p.x, ddx));
-      p.y = wrap_unit(__dadd_rn(p.y, ddy));
-      p.z = wrap_unit(__dadd_rn(p.z, ddz));
-      double ex = __dadd_rn(ux, -v.ox[i]), ey = __dadd_rn(uy, -v.oy[i]), ez = __dadd_rn(uz, -v.oz[i]);
-      mymax = __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
-      v.vx[i] = px;
-      v.vy[i] = py;
-      v.vz[i] = pz;
-      v.ux[i] = ux;
-      v.uy[i] = uy;
-      v.uz[i] = uz;
-      v.pos[i] = p;
-    }
+    if (loc < d.n) mymax = kick_drift_one(v, d, d.poff + loc, v.st[r].s1, v.st[r].s2);
     // per-system block max (a tile never straddles systems)
     for (int o = 16; o > 0; o >>= 1) mymax = fmax(mymax, __shfl_down_sync(0xffffffffu, mymax, o));
     if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = mymax;
@@ -182,35 +214,12 @@ __global__ void __launch_bounds__(BLOCK_A) k_kick_drift(View v, int use_cond, cu
   __threadfence();
   int any = 0;
   for (int s = threadIdx.x; s < v.nsys; s += blockDim.x) {
-    const SysDesc &d = v.desc[s];
-    SysState &st = v.st[s];
-    unsigned long long bits = atomicExch(&st.maxd_bits, 0ull);
-    double m = __dmul_rn(__dmul_rn(__longlong_as_double((long long)bits), d.L), d.L);
-    st.maxD_last = m;
-    int rb = (__dmul_rn(d.rebuild_factor, m) > d.skin2) || st.force_rebuild;
-    st.rebuild = rb;
-    st.force_rebuild = 0;
-    any |= rb;
+    unsigned long long bits = atomicExch(&v.st[s].maxd_bits, 0ull);
+    any |= rebuild_decision(v.desc[s], v.st[s], __longlong_as_double((long long)bits));
   }
-  // observable events due at the end of this step (frame = loop index step)
+  // observable events due at the end of this step
   int any_obs = 0;
-  for (int s = threadIdx.x; s < v.nsys; s += blockDim.x) {
-    const ObsDesc &o = v.obs[s];
-    SysState &st = v.st[s];
-    if (o.n_events == 0) {
-      st.obs_lo = st.obs_hi = 0;
-      continue;
-    }
-    const long long step = st.step;
-    int c = st.obs_cur;
-    while (c < o.n_events && o.ev_step[c] < step) c++;
-    const int lo = c;
-    while (c < o.n_events && o.ev_step[c] == step && c - lo < OBS_EMAX) c++;
-    st.obs_lo = lo;
-    st.obs_hi = c;
-    st.obs_cur = c;
-    any_obs |= c > lo;
-  }
+  for (int s = threadIdx.x; s < v.nsys; s += blockDim.x) any_obs |= obs_due(v.obs[s], v.st[s]);
   any = __syncthreads_or(any);
   any_obs = __syncthreads_or(any_obs);
   if (threadIdx.x == 0) {
@@ -220,6 +229,52 @@ __global__ void __launch_bounds__(BLOCK_A) k_kick_drift(View v, int use_cond, cu
       cudaGraphSetConditional(h_obs, any_obs ? 1u : 0u);
     }
   }
+}
+
+// one particle's part of observable event `info`: store its origin snapshot
+// (kind 1) or its overlap, |dr|^2, sum dx^4, |dr|^4 and sum_q cos(q.dr)
+// against the origin (kind 0)
+__device__ __forceinline__ void obs_particle(const ObsDesc &o, int n, int info, int id, double ux, double uy,
+                                             double uz, double L, double val[OBS_NV]) {
+  const int kind = info & 1, slot = (info >> 1) & 4095;
+  double *sn = o.snap + ((size_t)slot * n + id) * 3;
+  if (kind == 1) {
+    sn[0] = ux;
+    sn[1] = uy;
+    sn[2] = uz;
+    return;
+  }
+  const double dx = ux - sn[0], dy = uy - sn[1], dz = uz - sn[2];
+  double mx = dx, my = dy, mz = dz;  // Analysis/overlap.c:67-78
+  if (mz >= 0.5) mz -= 1.0; else if (mz < -0.5) mz += 1.0;
+  if (my >= 0.5) my -= 1.0; else if (my < -0.5) my += 1.0;
+  if (mx >= 0.5) mx -= 1.0; else if (mx < -0.5) mx += 1.0;
+  const double r2q = L * L * (mx * mx + my * my + mz * mz);
+  val[0] = r2q < o.a2 ? 1.0 : 0.0;
+  const double r2 = L * L * (dx * dx + dy * dy + dz * dz);
+  val[1] = r2;
+  val[2] = L * L * L * L * (dx * dx * dx * dx + dy * dy * dy * dy + dz * dz * dz * dz);
+  val[3] = r2 * r2;
+  double fs = 0.0;
+  for (int q = 0; q < o.nq; q++)
+    fs += cos(6.283185307179586 * ((double)o.qvec[3 * q] * dx + (double)o.qvec[3 * q + 1] * dy +
+                                   (double)o.qvec[3 * q + 2] * dz));
+  val[4] = fs;
+}
+
+// add one event's sums over the system to its time bin
+__device__ __forceinline__ void obs_accumulate(const ObsDesc &o, int n, int info, const double sum[OBS_NV]) {
+  const int bin = info >> 13;
+  const double tot = (double)n;  // TotPart (Analysis/overlap.c:25)
+  const double Q = sum[0] / tot;
+  double *acc = o.acc + (size_t)bin * 8;
+  acc[0] += Q;  // c[time_index] (Analysis/overlap.c:90-93)
+  acc[1] += Q * Q;
+  acc[2] += sum[1] / tot;  // msd[0..2] (Analysis/msd_pos.c:88-91)
+  acc[3] += sum[2] / tot;
+  acc[4] += sum[3] / tot;
+  acc[5] += o.nq > 0 ? sum[4] / (tot * o.nq) : 0.0;
+  acc[6] += 1.0;
 }
 
 // In-place observables at the scheduled steps (replaces writing data_coor.out
@@ -247,33 +302,9 @@ __global__ void __launch_bounds__(BLOCK_A) k_observe(View v) {
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
   for (int e = lo; e < hi; e++) {
     const int info = o.ev_info[e];
-    const int kind = info & 1, slot = (info >> 1) & 4095;
-    double *sn = o.snap + ((size_t)slot * d.n + id) * 3;
+    const int kind = info & 1;
     double val[OBS_NV] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    if (kind == 1) {
-      if (valid) {
-        sn[0] = ux;
-        sn[1] = uy;
-        sn[2] = uz;
-      }
-    } else if (valid) {
-      const double dx = ux - sn[0], dy = uy - sn[1], dz = uz - sn[2];
-      double mx = dx, my = dy, mz = dz;  // Analysis/overlap.c:67-78
-      if (mz >= 0.5) mz -= 1.0; else if (mz < -0.5) mz += 1.0;
-      if (my >= 0.5) my -= 1.0; else if (my < -0.5) my += 1.0;
-      if (mx >= 0.5) mx -= 1.0; else if (mx < -0.5) mx += 1.0;
-      const double r2q = L * L * (mx * mx + my * my + mz * mz);
-      val[0] = r2q < o.a2 ? 1.0 : 0.0;
-      const double r2 = L * L * (dx * dx + dy * dy + dz * dz);
-      val[1] = r2;
-      val[2] = L * L * L * L * (dx * dx * dx * dx + dy * dy * dy * dy + dz * dz * dz * dz);
-      val[3] = r2 * r2;
-      double fs = 0.0;
-      for (int q = 0; q < o.nq; q++)
-        fs += cos(6.283185307179586 * ((double)o.qvec[3 * q] * dx + (double)o.qvec[3 * q + 1] * dy +
-                                       (double)o.qvec[3 * q + 2] * dz));
-      val[4] = fs;
-    }
+    if (valid) obs_particle(o, d.n, info, id, ux, uy, uz, L, val);
     if (kind == 0) {
 #pragma unroll
       for (int k = 0; k < OBS_NV; k++) {
@@ -301,22 +332,12 @@ __global__ void __launch_bounds__(BLOCK_A) k_observe(View v) {
     const int e = lo + threadIdx.x;
     const int info = o.ev_info[e];
     if ((info & 1) == 0) {
-      const int bin = info >> 13;
       double sum[OBS_NV] = {0.0, 0.0, 0.0, 0.0, 0.0};
       for (int b = 0; b < d.ntile_a; b++) {
         const double *pb = v.part_o + ((size_t)(d.tile0_a + b) * OBS_EMAX + threadIdx.x) * OBS_NV;
         for (int k = 0; k < OBS_NV; k++) sum[k] += __ldcg(pb + k);
       }
-      const double tot = (double)d.n;  // TotPart (Analysis/overlap.c:25)
-      const double Q = sum[0] / tot;
-      double *acc = o.acc + (size_t)bin * 8;
-      acc[0] += Q;  // c[time_index] (Analysis/overlap.c:90-93)
-      acc[1] += Q * Q;
-      acc[2] += sum[1] / tot;  // msd[0..2] (Analysis/msd_pos.c:88-91)
-      acc[3] += sum[2] / tot;
-      acc[4] += sum[3] / tot;
-      acc[5] += o.nq > 0 ? sum[4] / (tot * o.nq) : 0.0;
-      acc[6] += 1.0;
+      obs_accumulate(o, d.n, info, sum);
     }
   }
   __syncthreads();
@@ -616,13 +637,18 @@ __device__ __forceinline__ void pair_fp32(PairAcc &a, const double4 &pi, int ti,
 
 // finish one system after its last force block: fixed-order sums, then the
 // thermostat chain (runs in a single block)
+__device__ void finalize_sums(const SysDesc &d, SysState &st, int mode, double pe, double vir, double ke, double va);
+
 __device__ void finalize_system(const View &v, int r, int mode) {
   __shared__ double sh[32];
   const SysDesc &d = v.desc[r];
   SysState &st = v.st[r];
   double pe = 0.0, vir = 0.0, ke = 0.0, va = 0.0;
-  for (int k = threadIdx.x; k < d.ntile_b; k += blockDim.x) {
-    const double2 *pp = reinterpret_cast<const double2 *>(&v.part_b[d.tile0_b + k]);
+  const bool per_particle = d.box;
+  const int nparts = per_particle ? d.n : d.ntile_b;
+  for (int k = threadIdx.x; k < nparts; k += blockDim.x) {
+    const double2 *pp = per_particle ? reinterpret_cast<const double2 *>(&v.pacc[d.poff + k])
+                                     : reinterpret_cast<const double2 *>(&v.part_b[d.tile0_b + k]);
     const double2 p0 = __ldcg(pp), p1 = __ldcg(pp + 1);
     pe += p0.x;
     vir += p0.y;
@@ -634,6 +660,13 @@ __device__ void finalize_system(const View &v, int r, int mode) {
   ke = block_sum_dyn(ke, sh);
   va = block_sum_dyn(va, sh);
   if (threadIdx.x != 0) return;
+  finalize_sums(d, st, mode, pe, vir, ke, va);
+}
+
+// thermostat and scalars of one system from its sums (one thread): pe and
+// virial halved (every pair is counted from both sides), then for a step the
+// chain's second half on the new KE and its first half of the next step
+__device__ void finalize_sums(const SysDesc &d, SysState &st, int mode, double pe, double vir, double ke, double va) {
   st.pe = 0.5 * pe;
   st.virial = (0.5 * vir) / 3.0;
   st.vir_act = va;
@@ -936,6 +969,29 @@ __device__ __forceinline__ size_t group_entry(int k, int t, int M) {
   return ((size_t)(k >> 2) * M + t) * 4 + (k & 3);
 }
 
+// 16-bit list entries of one particle, packed four to a chunk in a 64-bit
+// shift register (the newest entry enters at the top, so after four the
+// first is in the low bits); whole chunks are stored as uint2 at
+// chunk * stride + row
+struct ListWriter {
+  unsigned lo = 0u, hi = 0u;
+  int n = 0;
+  __device__ __forceinline__ void add(unsigned code, uint2 *lst, size_t stride, int row, int maxnb) {
+    lo = __funnelshift_r(lo, hi, 16);
+    hi = (hi >> 16) | (code << 16);
+    n++;
+    if ((n & 3) == 0 && n <= maxnb) lst[(size_t)((n >> 2) - 1) * stride + row] = make_uint2(lo, hi);
+  }
+  // the last, partial chunk: its k pending entries sit in the top 16k bits
+  __device__ __forceinline__ void finish(uint2 *lst, size_t stride, int row, int maxnb) {
+    const int k = n & 3;
+    if (k && n <= maxnb) {
+      const unsigned long long p = (((unsigned long long)hi << 32) | lo) >> (16 * (4 - k));
+      lst[(size_t)(n >> 2) * stride + row] = make_uint2((unsigned)p, (unsigned)(p >> 32));
+    }
+  }
+};
+
 // one warp per centre cell, one lane per particle of that cell: every lane
 // tests the same staged candidate (a shared-memory broadcast).  Each union
 // cell's staged run is padded to a multiple of four with far-away dummies so
@@ -1001,8 +1057,7 @@ __global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
         const int ti = __float_as_int(fi.w) >> 15;
         // cut for a partner of type 0 / 1 (the sum of the two types indexes lc)
         const float c0 = ti == 0 ? lc[0] : lc[1], c1 = ti == 0 ? lc[1] : lc[2];
-        unsigned long long pend = 0ull;
-        int n = 0;
+        ListWriter lw;
         for (int dz = -1; dz <= 1; dz++)
           for (int dy = -1; dy <= 1; dy++)
             for (int dx = -1; dx <= 1; dx++) {
@@ -1022,18 +1077,12 @@ __global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
                 }
 #pragma unroll
                 for (int e = 0; e < 4; e++)
-                  if (ok[e]) {
-                    pend |= (unsigned long long)(code[e] & 0xffff) << (16 * (n & 3));
-                    n++;
-                    if ((n & 3) == 0) {
-                      if (n <= maxnb) lst[(size_t)((n >> 2) - 1) * M + t] = make_uint2((unsigned)pend, (unsigned)(pend >> 32));
-                      pend = 0ull;
-                    }
-                  }
+                  if (ok[e]) lw.add((unsigned)code[e] & 0xffffu, lst, M, t, maxnb);
               }
             }
         if (valid) {
-          if ((n & 3) && n <= maxnb) lst[(size_t)(n >> 2) * M + t] = make_uint2((unsigned)pend, (unsigned)(pend >> 32));
+          lw.finish(lst, M, t, maxnb);
+          const int n = lw.n;
           const int i = S.ustart[cu] + w;
           if (n > maxnb) {
             v.nbn[i] = -1;
@@ -1083,17 +1132,34 @@ struct PairAccF {
   float fx, fy, fz, pe, vir;
 };
 
-// FP32 pair term (separation in FP32 from the hi/lo staged coordinates)
-__device__ __forceinline__ void pair_f32(PairAccF &a, float dx, float dy, float dz, int tp) {
-  const float is2 = tp == 0 ? 1.0f : (tp == 1 ? 1.5625f : (float)(1.0 / (0.88 * 0.88)));
-  const float e4 = tp == 0 ? 4.0f : (tp == 1 ? 6.0f : 2.0f);
+// FP32 pair constants of particle i against a partner of type 0 and of type 1:
+// 1/sigma^2, 4 eps and 8 eps/sigma^2 (MDcode/cell_list+forces.c:19-20)
+struct PairParamsF {
+  float is2[2], e4[2], ge[2];
+  __device__ __forceinline__ explicit PairParamsF(int ti) {
+#pragma unroll
+    for (int tj = 0; tj < 2; tj++) {
+      const int tp = ti + tj;
+      is2[tj] = tp == 0 ? 1.0f : (tp == 1 ? 1.5625f : (float)(1.0 / (0.88 * 0.88)));
+      e4[tj] = tp == 0 ? 4.0f : (tp == 1 ? 6.0f : 2.0f);
+      ge[tj] = 2.0f * e4[tj] * is2[tj];
+    }
+  }
+};
+
+// FP32 pair term: U = 4 eps (s^12 - s^6) + C0 + C2 (r/sigma)^2 and its radial
+// force factor, written as s6 (s6 - 1) and s6 (6 s6 - 3) s2
+__device__ __forceinline__ void pair_f32(PairAccF &a, float dx, float dy, float dz, const PairParamsF &P,
+                                         bool tj) {
+  const float is2 = tj ? P.is2[1] : P.is2[0];
   const float dr2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
   const float rs2 = dr2 * is2;
   if (rs2 < (float)KA_RC2) {
+    const float e4 = tj ? P.e4[1] : P.e4[0], ge = tj ? P.ge[1] : P.ge[0];
     const float s2 = rcp_approx(rs2);
     const float s6 = s2 * s2 * s2;
-    a.pe = fmaf(e4, fmaf(s6, s6 - 1.0f, fmaf((float)KA_C2, rs2, (float)KA_C0)), a.pe);
-    const float g = (2.0f * e4 * is2) * fmaf(6.0f * s6 * (s6 - 0.5f), s2, -(float)KA_C2);
+    a.pe = fmaf(e4, fmaf(s6, s6, -s6) + fmaf((float)KA_C2, rs2, (float)KA_C0), a.pe);
+    const float g = ge * fmaf(s6 * fmaf(6.0f, s6, -3.0f), s2, -(float)KA_C2);
     a.fx = fmaf(g, dx, a.fx);
     a.fy = fmaf(g, dy, a.fy);
     a.fz = fmaf(g, dz, a.fz);
@@ -1274,6 +1340,7 @@ __global__ void __launch_bounds__(BLOCK_G, PREC ? ACG_FORCE_MINB32 : ACG_FORCE_M
     if (PREC == 1 && valid && staged && nn >= 0) {
       const float4 hi = shi[qs];
       const float2 li = slo[qs];
+      const PairParamsF P(ti);
       const int nch = (nn + 3) >> 2;
       const uint2 *lp = reinterpret_cast<const uint2 *>(lst) + t;
       PairAccF fa = {0.f, 0.f, 0.f, 0.f, 0.f}, fb = {0.f, 0.f, 0.f, 0.f, 0.f};
@@ -1291,7 +1358,7 @@ __global__ void __launch_bounds__(BLOCK_G, PREC ? ACG_FORCE_MINB32 : ACG_FORCE_M
             const float dx = (hi.x - hj.x) + (hi.w - hj.w);
             const float dy = (hi.y - hj.y) + (li.x - lj.x);
             const float dz = (hi.z - hj.z) + (li.y - lj.y);
-            pair_f32(e & 1 ? fb : fa, dx, dy, dz, ti + (code >> 15));
+            pair_f32(e & 1 ? fb : fa, dx, dy, dz, P, code >> 15);
           }
         }
         w = wn;
@@ -1375,7 +1442,8 @@ __global__ void __launch_bounds__(BLOCK_G, PREC ? ACG_FORCE_MINB32 : ACG_FORCE_M
 // whole-box kernels: systems with 2 to 4 cells per side (N up to ~3.5k at
 // density 1.2).  A 2x2x2 cell group of such a box would stage the whole box
 // (and, at 3 cells per side, part of it twice) for each of its 8 groups; here
-// every block stages the system once and handles BOX_CELLS cells of it.
+// every block stages the system once and handles d.cpb cells of it (1 to
+// BOX_CELLS, chosen per engine for about two blocks per SM).
 // List entries are system-local slot indices (| type << 15); entry k of slot
 // s sits in chunk k/4 at uint2 index (k/4)*N + s.
 
@@ -1419,53 +1487,33 @@ __device__ __forceinline__ void box_cells(const View &v, const SysDesc &d, int *
   __syncthreads();
 }
 
-// lists of a whole box: one warp per cell of the block, one lane per particle;
-// the 27 neighbour cells (with their periodic image shifts; at 2 cells per side
-// a cell appears under two shifts, of which at most one can be in range since
-// L > 2 x the list cut) are tested against the staged reduced coordinates
-__global__ void __launch_bounds__(BLOCK_X) k_build_list_box(View v) {
-  extern __shared__ float4 xstg[];
-  __shared__ int cst[MAX_BOX_CELLS + 1], pre4[MAX_BOX_CELLS + 1];
-  const int2 tile = v.tiles_x[blockIdx.x];
-  const int r = tile.x, b = tile.y;
-  if (!v.st[r].rebuild) return;
-  const SysDesc &d = v.desc[r];
-  const int nc = d.nc, nce = d.ncell, n = d.n;
-  box_cells(v, d, cst, pre4);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  for (int c = warp; c < nce; c += nwarps) {
-    const int s0 = cst[c], m = cst[c + 1] - s0, p0 = pre4[c], m4 = pre4[c + 1] - p0;
-    for (int k = lane; k < m4; k += 32) {
-      float4 f;
-      if (k < m) {
-        const double4 p = v.pos_s[d.poff + s0 + k];
-        f = make_float4((float)p.x, (float)p.y, (float)p.z, __int_as_float((s0 + k) | ((int)p.w << 15)));
-      } else {
-        f = make_float4(1e18f, 1e18f, 1e18f, __int_as_float(0));
-      }
-      xstg[p0 + k] = f;
-    }
-  }
-  __syncthreads();
+// lists of the particles of cell c of a whole box (one warp; lanes are the
+// particles of the cell, in rounds of 32) against the staged system: the 27
+// neighbour cells with their periodic image shifts (at 2 cells per side a cell
+// appears under two shifts, of which at most one can be in range since L > 2 x
+// the list cut), candidates in slot order within each cell
+__device__ __forceinline__ void box_list_cell(const View &v, const SysDesc &d, int r, const float4 *xstg,
+                                              const int *cst, const int *pre4, int c, int lane, int round0,
+                                              int rstep) {
+  const int nc = d.nc, n = d.n;
   const double iL2 = 1.0 / (d.L * d.L);
   float lc[3];
   for (int k = 0; k < 3; k++) lc[k] = (float)(lcut2_of(d, k) * iL2 * (1.0 + 1e-5));
   const bool one_cut = lc[0] == lc[1] && lc[1] == lc[2];
   uint2 *lst = reinterpret_cast<uint2 *>(box_list(v, d));
   const int maxnb = v.maxnb;
-  const int c = b * BOX_CELLS + warp;
-  if (c < nce) {
+  {
+
     const int cx = c % nc, cy = (c / nc) % nc, cz = c / (nc * nc);
     const int m = cst[c + 1] - cst[c];
-    for (int w0 = 0; w0 < m; w0 += 32) {
+    for (int w0 = 32 * round0; w0 < m; w0 += 32 * rstep) {
       const int w = w0 + lane;
       const bool valid = w < m;
       const int sl = cst[c] + w, ps = pre4[c] + w;
       const float4 fi = valid ? xstg[ps] : make_float4(-1e18f, -1e18f, -1e18f, __int_as_float(0));
       const int ti = __float_as_int(fi.w) >> 15;
       const float c0 = ti == 0 ? lc[0] : lc[1], c1 = ti == 0 ? lc[1] : lc[2];
-      unsigned long long pend = 0ull;
-      int nn = 0;
+      ListWriter lw;
       for (int dz = -1; dz <= 1; dz++)
         for (int dy = -1; dy <= 1; dy++)
           for (int dx = -1; dx <= 1; dx++) {
@@ -1490,19 +1538,12 @@ __global__ void __launch_bounds__(BLOCK_X) k_build_list_box(View v) {
               }
 #pragma unroll
               for (int e = 0; e < 4; e++)
-                if (ok[e]) {
-                  pend |= (unsigned long long)(code[e] & 0xffff) << (16 * (nn & 3));
-                  nn++;
-                  if ((nn & 3) == 0) {
-                    if (nn <= maxnb)
-                      lst[(size_t)((nn >> 2) - 1) * n + sl] = make_uint2((unsigned)pend, (unsigned)(pend >> 32));
-                    pend = 0ull;
-                  }
-                }
+                if (ok[e]) lw.add((unsigned)code[e] & 0xffffu, lst, n, sl, maxnb);
             }
           }
       if (valid) {
-        if ((nn & 3) && nn <= maxnb) lst[(size_t)(nn >> 2) * n + sl] = make_uint2((unsigned)pend, (unsigned)(pend >> 32));
+        lw.finish(lst, n, sl, maxnb);
+        const int nn = lw.n;
         const int i = d.poff + sl;
         if (nn > maxnb) {
           v.nbn[i] = -1;
@@ -1513,23 +1554,65 @@ __global__ void __launch_bounds__(BLOCK_X) k_build_list_box(View v) {
       }
     }
   }
+}
+
+// the system in cell order (after the permutation) as float4 {reduced x, y, z,
+// list code}, each cell's run padded to a multiple of four with far dummies
+__device__ __forceinline__ void box_stage_list(const View &v, const SysDesc &d, float4 *xstg, const int *cst,
+                                               const int *pre4) {
+  const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  for (int c = threadIdx.x >> 5; c < d.ncell; c += nwarps) {
+    const int s0 = cst[c], m = cst[c + 1] - s0, p0 = pre4[c], m4 = pre4[c + 1] - p0;
+    for (int k = lane; k < m4; k += 32) {
+      float4 f;
+      if (k < m) {
+        const double4 p = v.pos_s[d.poff + s0 + k];
+        f = make_float4((float)p.x, (float)p.y, (float)p.z, __int_as_float((s0 + k) | ((int)p.w << 15)));
+      } else {
+        f = make_float4(1e18f, 1e18f, 1e18f, __int_as_float(0));
+      }
+      xstg[p0 + k] = f;
+    }
+  }
+}
+
+// lists of a whole box: one warp per cell of the block, one lane per particle;
+// the 27 neighbour cells (with their periodic image shifts; at 2 cells per side
+// a cell appears under two shifts, of which at most one can be in range since
+// L > 2 x the list cut) are tested against the staged reduced coordinates
+__global__ void __launch_bounds__(BLOCK_X) k_build_list_box(View v) {
+  extern __shared__ float4 xstg[];
+  __shared__ int cst[MAX_BOX_CELLS + 1], pre4[MAX_BOX_CELLS + 1];
+  const int2 tile = v.tiles_x[blockIdx.x];
+  const int r = tile.x, b = tile.y;
+  if (!v.st[r].rebuild) return;
+  const SysDesc &d = v.desc[r];
+  const int nce = d.ncell;
+  box_cells(v, d, cst, pre4);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  box_stage_list(v, d, xstg, cst, pre4);
   __syncthreads();
-  const int ca = b * BOX_CELLS, cb = min(nce, ca + BOX_CELLS);
+  // work items (cell, round of 32 particles) of the block's cells, one warp each
+  const int ca = b * d.cpb, cb = min(nce, ca + d.cpb);
+  int item = 0;
+  for (int c = ca; c < cb; c++) {
+    const int rounds = (cst[c + 1] - cst[c] + 31) >> 5;
+    const int nw = blockDim.x >> 5;
+    // warps item..item+rounds-1 (mod nw) take this cell's rounds
+    const int first = item % nw;
+    const int k = (warp - first + nw) % nw;
+    if (k < rounds) box_list_cell(v, d, r, xstg, cst, pre4, c, lane, k, nw);
+    item += rounds;
+  }
+  __syncthreads();
   for (int sl = cst[ca] + threadIdx.x; sl < cst[cb]; sl += blockDim.x) copy_back(v, d.poff + sl);
 }
 
-// pair forces of a whole box from its lists.  FP32: staged 32-bit fixed-point
-// reduced coordinates, separation = wrapped integer difference x L/2^32 (one
-// rounding); FP64: staged reduced coordinates, minimum image d - rint(d).
-template <int TPP, int PREC>
-__global__ void __launch_bounds__(BLOCK_X) k_force_box(View v, int mode) {
-  extern __shared__ __align__(16) unsigned char xsm[];
-  const int2 tile = v.tiles_x[blockIdx.x];
-  const int r = tile.x, b = tile.y;
-  const SysState &st = v.st[r];
-  if (mode == 1 && !st.prime) return;
-  const SysDesc &d = v.desc[r];
-  const int n = d.n, nce = d.ncell;
+// the system's current positions staged for the pair loop: FP32 as 32-bit
+// fixed point {x, y, z, type}, FP64 as three arrays of reduced coordinates
+template <int PREC>
+__device__ __forceinline__ void box_stage_force(const View &v, const SysDesc &d, unsigned char *xsm) {
+  const int n = d.n;
   int4 *sq = reinterpret_cast<int4 *>(xsm);
   double *sx = reinterpret_cast<double *>(xsm), *sy = sx + n, *sz = sy + n;
   for (int k = threadIdx.x; k < n; k += blockDim.x) {
@@ -1542,19 +1625,22 @@ __global__ void __launch_bounds__(BLOCK_X) k_force_box(View v, int mode) {
       sz[k] = p.z;
     }
   }
-  const int ca = b * BOX_CELLS, cb = min(nce, ca + BOX_CELLS);
-  const int s_lo = v.cstart[d.coff + ca], s_hi = cb < nce ? v.cstart[d.coff + cb] : n;
-  __syncthreads();
+}
+
+// pair sums of system-local slot sl (particle i) from its list, TPP threads
+// per particle (summed across the TPP lanes on return; every thread of the
+// warp takes part)
+template <int TPP, int PREC>
+__device__ __forceinline__ PairAcc box_pairs(const View &v, const SysDesc &d, const unsigned char *xsm, bool valid,
+                                             int sl, int i, int lane) {
+  const int n = d.n;
+  const int4 *sq = reinterpret_cast<const int4 *>(xsm);
+  const double *sx = reinterpret_cast<const double *>(xsm), *sy = sx + n, *sz = sy + n;
   const uint2 *lst = reinterpret_cast<const uint2 *>(box_list(v, d));
   const double L = d.L;
   const float scale = (float)(L * (1.0 / 4294967296.0));
-  double pe = 0.0, vir = 0.0, ke = 0.0, va = 0.0;
-  const int lane = threadIdx.x % TPP, nper = blockDim.x / TPP;
-  for (int t0 = s_lo; t0 < s_hi; t0 += nper) {
-    const int sl = t0 + threadIdx.x / TPP;
-    const bool valid = sl < s_hi;
-    const int i = d.poff + (valid ? sl : s_lo);
-    const int nn = valid ? v.nbn[i] : 0;
+  const int nn = valid ? v.nbn[i] : 0;
+  {
     PairAcc a = {0.0, 0.0, 0.0, 0.0, 0.0};
     if (valid && nn >= 0) {
       const int nch = (nn + 3) >> 2;
@@ -1562,6 +1648,7 @@ __global__ void __launch_bounds__(BLOCK_X) k_force_box(View v, int mode) {
       uint2 w = lane < nch ? __ldg(lp + (size_t)lane * n) : make_uint2(0u, 0u);
       if (PREC == 1) {
         const int4 qi = sq[sl];
+        const PairParamsF P(qi.w);
         PairAccF fa = {0.f, 0.f, 0.f, 0.f, 0.f}, fb = {0.f, 0.f, 0.f, 0.f, 0.f};
         for (int c = lane; c < nch; c += TPP) {
           const uint2 wn = c + TPP < nch ? __ldg(lp + (size_t)(c + TPP) * n) : make_uint2(0u, 0u);
@@ -1574,7 +1661,7 @@ __global__ void __launch_bounds__(BLOCK_X) k_force_box(View v, int mode) {
               const float dx = (float)(int)((unsigned)qi.x - (unsigned)qj.x) * scale;
               const float dy = (float)(int)((unsigned)qi.y - (unsigned)qj.y) * scale;
               const float dz = (float)(int)((unsigned)qi.z - (unsigned)qj.z) * scale;
-              pair_f32(e & 1 ? fb : fa, dx, dy, dz, qi.w + (code >> 15));
+              pair_f32(e & 1 ? fb : fa, dx, dy, dz, P, code >> 15);
             }
           }
           w = wn;
@@ -1630,10 +1717,229 @@ __global__ void __launch_bounds__(BLOCK_X) k_force_box(View v, int mode) {
       a.pe += __shfl_xor_sync(0xffffffffu, a.pe, o);
       a.vir += __shfl_xor_sync(0xffffffffu, a.vir, o);
     }
+    return a;
+  }
+}
+
+// pair forces of a whole box from its lists.  FP32: staged 32-bit fixed-point
+// reduced coordinates, separation = wrapped integer difference x L/2^32 (one
+// rounding); FP64: staged reduced coordinates, minimum image d - rint(d).
+template <int TPP, int PREC>
+__global__ void __launch_bounds__(BLOCK_X) k_force_box(View v, int mode) {
+  extern __shared__ __align__(16) unsigned char xsm[];
+  const int2 tile = v.tiles_x[blockIdx.x];
+  const int r = tile.x, b = tile.y;
+  const SysState &st = v.st[r];
+  if (mode == 1 && !st.prime) return;
+  const SysDesc &d = v.desc[r];
+  const int n = d.n, nce = d.ncell;
+  box_stage_force<PREC>(v, d, xsm);
+  const int ca = b * d.cpb, cb = min(nce, ca + d.cpb);
+  const int s_lo = v.cstart[d.coff + ca], s_hi = cb < nce ? v.cstart[d.coff + cb] : n;
+  __syncthreads();
+  double pe = 0.0, vir = 0.0, ke = 0.0, va = 0.0;
+  const int lane = threadIdx.x % TPP, nper = blockDim.x / TPP;
+  for (int t0 = s_lo; t0 < s_hi; t0 += nper) {
+    const int sl = t0 + threadIdx.x / TPP;
+    const bool valid = sl < s_hi;
+    const int i = d.poff + (valid ? sl : s_lo);
+    PairAcc a = box_pairs<TPP, PREC>(v, d, xsm, valid, sl, i, lane);
     if (!valid || lane != 0) continue;
-    particle_epilogue(v, d, st, i, mode, a, pe, vir, ke, va);
+    // per-particle sums, added up in slot order by the finaliser, so the
+    // system's totals do not depend on how its cells are split into blocks
+    double pei = 0.0, viri = 0.0, kei = 0.0, vai = 0.0;
+    particle_epilogue(v, d, st, i, mode, a, pei, viri, kei, vai);
+    v.pacc[i] = make_double4(pei, viri, kei, vai);
   }
   end_force_block(v, r, b, mode, pe, vir, ke, va);
+}
+
+// ---------------------------------------------------------------------------
+// Whole timesteps of whole-box systems, one block per system: kick/drift and
+// direction shuffle, rebuild decision, cell build and lists when due, pair
+// forces with the second kick, thermostat chain, observables, with block
+// barriers between the phases.  Blocks never wait on one another, so a batch
+// of replicas advances by one launch per step.  Every phase runs the same
+// per-particle arithmetic as the per-phase kernels (shared device functions);
+// only the order of the per-system sums differs (one block sum instead of
+// per-block partials).
+constexpr int BLOCK_F = 512;
+
+template <int TPP, int PREC>
+__global__ void __launch_bounds__(BLOCK_F) k_steps_box(View v, int nsteps) {
+  extern __shared__ __align__(16) unsigned char fsm[];
+  __shared__ int cst[MAX_BOX_CELLS + 1], pre4[MAX_BOX_CELLS + 1], cnt[MAX_BOX_CELLS], fill[MAX_BOX_CELLS];
+  __shared__ double wred[BLOCK_F / 32];
+  __shared__ double s_max;
+  __shared__ int s_rb, s_obs, s_lo, s_hi;
+  __shared__ long long s_step;
+  const int r = blockIdx.x;
+  const SysDesc &d = v.desc[r];
+  SysState &st = v.st[r];
+  const ObsDesc &o = v.obs[r];
+  const int n = d.n, nce = d.ncell, poff = d.poff;
+  const int lane32 = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = BLOCK_F / 32;
+  for (int s = 0; s < nsteps; s++) {
+    if (threadIdx.x == 0) s_step = st.step;
+    __syncthreads();
+    const long long step = s_step;
+    // U3 U2 U1 and the block max of the displacement since the last rebuild
+    {
+      // written by thread 0 in the previous step's thermostat update
+      const double s1 = *reinterpret_cast<volatile const double *>(&st.s1);
+      const double s2 = *reinterpret_cast<volatile const double *>(&st.s2);
+      double m = 0.0;
+      for (int k = threadIdx.x; k < n; k += BLOCK_F) m = fmax(m, kick_drift_one(v, d, poff + k, s1, s2));
+      for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, off));
+      if (lane32 == 0) wred[warp] = m;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double mm = wred[0];
+        for (int w = 1; w < nwarp; w++) mm = fmax(mm, wred[w]);
+        s_max = mm;
+      }
+    }
+    // direction shuffle at the persistence steps (MDcode/main.c:245)
+    if (d.shuffle && d.nact > 0 && d.tau_p > 0 && (step % d.tau_p) == 0)
+      for (int comp = 0; comp < 3; comp++) {
+        shuffle_component(v, r, comp, step);
+        __syncthreads();
+      }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      s_rb = rebuild_decision(d, st, s_max);
+      s_obs = obs_due(o, st);
+      s_lo = st.obs_lo;
+      s_hi = st.obs_hi;
+      if (s_rb) st.overflow = 0;
+    }
+    __syncthreads();
+    if (s_rb) {
+      // cells: count, scan, scatter, order by particle index, permute
+      for (int c = threadIdx.x; c < nce; c += BLOCK_F) {
+        cnt[c] = 0;
+        fill[c] = 0;
+      }
+      __syncthreads();
+      for (int k = threadIdx.x; k < n; k += BLOCK_F) {
+        const int i = poff + k;
+        const double4 p = v.pos[i];
+        const int c = cell_coord(p.x, d.inv_cell, d.nc) + cell_coord(p.y, d.inv_cell, d.nc) * d.nc +
+                      cell_coord(p.z, d.inv_cell, d.nc) * d.nc * d.nc;
+        v.cell_tmp[i] = c;
+        atomicAdd(&cnt[c], 1);
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        int run = 0, run4 = 0;
+        for (int c = 0; c < nce; c++) {
+          cst[c] = run;
+          pre4[c] = run4;
+          run += cnt[c];
+          run4 += (cnt[c] + 3) & ~3;
+        }
+        cst[nce] = run;
+        pre4[nce] = run4;
+      }
+      __syncthreads();
+      for (int c = threadIdx.x; c < nce; c += BLOCK_F) {
+        v.cstart[d.coff + c] = cst[c];
+        v.ccount[d.coff + c] = cnt[c];
+      }
+      for (int k = threadIdx.x; k < n; k += BLOCK_F) {
+        const int i = poff + k;
+        const int c = v.cell_tmp[i];
+        v.perm_u[poff + cst[c] + atomicAdd(&fill[c], 1)] = i;
+      }
+      __syncthreads();
+      for (int c = warp; c < nce; c += nwarp) {
+        const int m = cnt[c], base = poff + cst[c];
+        for (int a0 = 0; a0 < m; a0 += 32) {
+          const int a = a0 + lane32;
+          int sa = -1, ida = 0x7fffffff;
+          if (a < m) {
+            sa = v.perm_u[base + a];
+            ida = v.id[sa];
+          }
+          int rank = 0;
+          for (int b0 = 0; b0 < m; b0 += 32) {
+            const int b = b0 + lane32;
+            const int idb = b < m ? v.id[v.perm_u[base + b]] : 0x7fffffff;
+#pragma unroll 8
+            for (int q = 0; q < 32; q++) rank += __shfl_sync(0xffffffffu, idb, q) < ida;
+          }
+          if (a < m) {
+            v.perm[base + rank] = sa;
+            v.cellof[base + rank] = c;
+          }
+        }
+      }
+      __syncthreads();
+      for (int k = threadIdx.x; k < n; k += BLOCK_F) {
+        const int i = poff + k, q = v.perm[i];
+        v.pos_s[i] = v.pos[q];
+        v.ux_s[i] = v.ux[q];
+        v.uy_s[i] = v.uy[q];
+        v.uz_s[i] = v.uz[q];
+        v.vx_s[i] = v.vx[q];
+        v.vy_s[i] = v.vy[q];
+        v.vz_s[i] = v.vz[q];
+        v.fx_s[i] = v.fx[q];
+        v.fy_s[i] = v.fy[q];
+        v.fz_s[i] = v.fz[q];
+        v.id_s[i] = v.id[q];
+        v.act_s[i] = v.act[q];
+      }
+      __syncthreads();
+      box_stage_list(v, d, reinterpret_cast<float4 *>(fsm), cst, pre4);
+      __syncthreads();
+      for (int c = warp; c < nce; c += nwarp)
+        box_list_cell(v, d, r, reinterpret_cast<const float4 *>(fsm), cst, pre4, c, lane32, 0, 1);
+      __syncthreads();
+      for (int k = threadIdx.x; k < n; k += BLOCK_F) copy_back(v, poff + k);
+      if (threadIdx.x == 0) st.rebuilds += 1;
+      __syncthreads();
+    }
+    // pair forces, active force, second half kick; sums; thermostat chain
+    box_stage_force<PREC>(v, d, fsm);
+    __syncthreads();
+    {
+      double pe = 0.0, vir = 0.0, ke = 0.0, va = 0.0;
+      const int lane = threadIdx.x % TPP;
+      for (int t0 = 0; t0 < n; t0 += BLOCK_F / TPP) {
+        const int sl = t0 + threadIdx.x / TPP;
+        const bool valid = sl < n;
+        const int i = poff + (valid ? sl : 0);
+        const PairAcc a = box_pairs<TPP, PREC>(v, d, fsm, valid, sl, i, lane);
+        if (valid && lane == 0) particle_epilogue(v, d, st, i, 0, a, pe, vir, ke, va);
+      }
+      pe = block_sum_dyn(pe, wred);
+      vir = block_sum_dyn(vir, wred);
+      ke = block_sum_dyn(ke, wred);
+      va = block_sum_dyn(va, wred);
+      if (threadIdx.x == 0) finalize_sums(d, st, 0, pe, vir, ke, va);
+    }
+    __syncthreads();
+    // observables due at this step
+    if (s_obs) {
+      for (int e = s_lo; e < s_hi; e++) {
+        const int info = o.ev_info[e];
+        double val[OBS_NV] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int k = threadIdx.x; k < n; k += BLOCK_F) {
+          const int i = poff + k;
+          double w[OBS_NV] = {0.0, 0.0, 0.0, 0.0, 0.0};
+          obs_particle(o, n, info, v.id[i], v.ux[i], v.uy[i], v.uz[i], d.L, w);
+          for (int q = 0; q < OBS_NV; q++) val[q] += w[q];
+        }
+        if ((info & 1) == 0) {
+          double sum[OBS_NV];
+          for (int q = 0; q < OBS_NV; q++) sum[q] = block_sum_dyn(val[q], wred);
+          if (threadIdx.x == 0) obs_accumulate(o, n, info, sum);
+        }
+        __syncthreads();
+      }
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------

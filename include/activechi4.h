@@ -216,8 +216,9 @@ int acg_measure_fp64_peak(int device, double *tflops);
  * particle in the force kernel (1,2,4,8,16,32); block: threads per block. */
 int acg_set_launch(acg_engine *e, int tpp, int block);
 int acg_get_launch(acg_engine *e, int *tpp, int *block);
-/* Threads per particle (1, 2 or 4) of the cell-group force kernel used for
- * boxes with >= 3 cells per side. */
+/* Threads per particle (1, 2 or 4) of the cell-group force kernel (boxes with
+ * >= 5 cells per side, or larger than the whole-box limit) and of the
+ * whole-box force kernel (2 to 4 cells per side, N <= 8192). */
 int acg_set_group_tpp(acg_engine *e, int gtpp);
 
 const char *acg_last_error(void);
