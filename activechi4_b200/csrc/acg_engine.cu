@@ -123,7 +123,8 @@ int plan(const acg_params *params, int nsys, Layout &lay, int nsm) {
     const int cpb = (int)std::max(1LL, std::min((long long)BOX_CELLS, cells / (2LL * std::max(nsm, 1))));
     for (int r = 0; r < nsys; r++) {
       SysDesc &d = lay.desc[r];
-      d.cpb = cpb;
+      // 2 cells per side: one cell (of up to ~100 particles) per block
+      d.cpb = d.nc == 2 ? 1 : cpb;
       d.xoff = lay.nboxtiles;
       if (d.box) lay.nboxtiles += (d.ncell + cpb - 1) / cpb;
     }
@@ -691,9 +692,9 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
     for (int gt : {1, 2, 4})
       for (int pr : {0, 1}) attr_ok = attr_ok && raise_smem((const void *)steps_fn(gt, pr), steps_smem(L.box_nmax, pr));
   }
-  // one cell per whole-box block (a lone small system): four threads per
-  // particle keep more list loads in flight
-  e->btpp = L.desc[0].cpb == 1 ? 4 : 2;
+  // threads per particle of the whole-box kernels: fixed (not derived from the
+  // batch), so an FP64 system sums its pairs in the same order alone and batched
+  e->btpp = 2;
   e->fused = ACG_FUSED_STEPS != 0;
   for (int r = 0; r < nsys; r++) e->fused = e->fused && L.desc[r].box;
   if (!attr_ok) {

@@ -1073,7 +1073,7 @@ __global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
                   const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
                   code[e] = __float_as_int(fj.w);
                   const float cut = one_cut ? c0 : ((code[e] >> 15) ? c1 : c0);
-                  ok[e] = r2 < cut && q + e != ps;
+                  ok[e] = valid && r2 < cut && q + e != ps;
                 }
 #pragma unroll
                 for (int e = 0; e < 4; e++)
@@ -1122,6 +1122,8 @@ __device__ __forceinline__ double rcp_nr(double x) {
   return fma(y, e, y);
 }
 
+// 1/x in FP32 from the hardware estimate (a Newton step on it changed the
+// measured force error by nothing: the FP32 rounding of r^2 dominates)
 __device__ __forceinline__ float rcp_approx(float x) {
   float y;
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
@@ -1131,6 +1133,21 @@ __device__ __forceinline__ float rcp_approx(float x) {
 struct PairAccF {
   float fx, fy, fz, pe, vir;
 };
+
+// the sums of one list chunk (at most two FP32 terms in each of fa, fb) moved
+// into the FP64 sums: the per-particle force is a sum of large terms of both
+// signs, whose FP32 rounding would otherwise grow with the list; and the FP64
+// sum of these chunk values is exact in practice, so it does not depend on how
+// the chunks are split over threads
+__device__ __forceinline__ void flush_chunk(PairAccF &fa, PairAccF &fb, PairAcc &a) {
+  a.fx += (double)(fa.fx + fb.fx);
+  a.fy += (double)(fa.fy + fb.fy);
+  a.fz += (double)(fa.fz + fb.fz);
+  a.pe += (double)(fa.pe + fb.pe);
+  a.vir += (double)(fa.vir + fb.vir);
+  fa = PairAccF{0.f, 0.f, 0.f, 0.f, 0.f};
+  fb = PairAccF{0.f, 0.f, 0.f, 0.f, 0.f};
+}
 
 // FP32 pair constants of particle i against a partner of type 0 and of type 1:
 // 1/sigma^2, 4 eps and 8 eps/sigma^2 (MDcode/cell_list+forces.c:19-20)
@@ -1361,13 +1378,9 @@ __global__ void __launch_bounds__(BLOCK_G, PREC ? ACG_FORCE_MINB32 : ACG_FORCE_M
             pair_f32(e & 1 ? fb : fa, dx, dy, dz, P, code >> 15);
           }
         }
+        flush_chunk(fa, fb, a);
         w = wn;
       }
-      a.fx = (double)fa.fx + (double)fb.fx;
-      a.fy = (double)fa.fy + (double)fb.fy;
-      a.fz = (double)fa.fz + (double)fb.fz;
-      a.pe = (double)fa.pe + (double)fb.pe;
-      a.vir = (double)fa.vir + (double)fb.vir;
     } else if (PREC == 0 && valid && staged && nn >= 0) {
       const double xi = sx[qs], yi = sy[qs], zi = sz[qs];
       const int nch = (nn + 3) >> 2;
@@ -1510,11 +1523,38 @@ __device__ __forceinline__ void box_list_cell(const View &v, const SysDesc &d, i
       const int w = w0 + lane;
       const bool valid = w < m;
       const int sl = cst[c] + w, ps = pre4[c] + w;
-      const float4 fi = valid ? xstg[ps] : make_float4(-1e18f, -1e18f, -1e18f, __int_as_float(0));
+      // a lane past the cell's particles gets NaN coordinates: it passes no test
+      const float nan = __int_as_float(0x7fc00000);
+      const float4 fi = valid ? xstg[ps] : make_float4(nan, nan, nan, __int_as_float(0));
       const int ti = __float_as_int(fi.w) >> 15;
       const float c0 = ti == 0 ? lc[0] : lc[1], c1 = ti == 0 ? lc[1] : lc[2];
       ListWriter lw;
-      for (int dz = -1; dz <= 1; dz++)
+      if (nc == 2) {
+        // two cells per side: every cell neighbours every other under two
+        // images, so test each particle once with the minimum image instead
+        // of 27 images of 8 cells
+        const int q1 = pre4[d.ncell];
+        for (int q = 0; q < q1; q += 4) {
+          int code[4];
+          bool ok[4];
+#pragma unroll
+          for (int e = 0; e < 4; e++) {
+            const float4 fj = xstg[q + e];
+            float ex = fi.x - fj.x, ey = fi.y - fj.y, ez = fi.z - fj.z;
+            ex -= rintf(ex);
+            ey -= rintf(ey);
+            ez -= rintf(ez);
+            const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+            code[e] = __float_as_int(fj.w);
+            const float cut = one_cut ? c0 : ((code[e] >> 15) ? c1 : c0);
+            ok[e] = valid && r2 < cut && q + e != ps;
+          }
+#pragma unroll
+          for (int e = 0; e < 4; e++)
+            if (ok[e]) lw.add((unsigned)code[e] & 0xffffu, lst, n, sl, maxnb);
+        }
+      }
+      for (int dz = -1; dz <= 1 && nc > 2; dz++)
         for (int dy = -1; dy <= 1; dy++)
           for (int dx = -1; dx <= 1; dx++) {
             const int ax = cx + dx, ay = cy + dy, az = cz + dz;
@@ -1534,7 +1574,7 @@ __device__ __forceinline__ void box_list_cell(const View &v, const SysDesc &d, i
                 const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
                 code[e] = __float_as_int(fj.w);
                 const float cut = one_cut ? c0 : ((code[e] >> 15) ? c1 : c0);
-                ok[e] = r2 < cut && q + e != ps;
+                ok[e] = valid && r2 < cut && q + e != ps;
               }
 #pragma unroll
               for (int e = 0; e < 4; e++)
@@ -1557,7 +1597,7 @@ __device__ __forceinline__ void box_list_cell(const View &v, const SysDesc &d, i
 }
 
 // the system in cell order (after the permutation) as float4 {reduced x, y, z,
-// list code}, each cell's run padded to a multiple of four with far dummies
+// list code}, each cell's run padded to a multiple of four with NaN dummies
 __device__ __forceinline__ void box_stage_list(const View &v, const SysDesc &d, float4 *xstg, const int *cst,
                                                const int *pre4) {
   const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
@@ -1569,7 +1609,9 @@ __device__ __forceinline__ void box_stage_list(const View &v, const SysDesc &d, 
         const double4 p = v.pos_s[d.poff + s0 + k];
         f = make_float4((float)p.x, (float)p.y, (float)p.z, __int_as_float((s0 + k) | ((int)p.w << 15)));
       } else {
-        f = make_float4(1e18f, 1e18f, 1e18f, __int_as_float(0));
+        // padding: NaN coordinates fail every distance test
+        const float nan = __int_as_float(0x7fc00000);
+        f = make_float4(nan, nan, nan, __int_as_float(0));
       }
       xstg[p0 + k] = f;
     }
@@ -1664,13 +1706,9 @@ __device__ __forceinline__ PairAcc box_pairs(const View &v, const SysDesc &d, co
               pair_f32(e & 1 ? fb : fa, dx, dy, dz, P, code >> 15);
             }
           }
+          flush_chunk(fa, fb, a);
           w = wn;
         }
-        a.fx = (double)fa.fx + (double)fb.fx;
-        a.fy = (double)fa.fy + (double)fb.fy;
-        a.fz = (double)fa.fz + (double)fb.fz;
-        a.pe = (double)fa.pe + (double)fb.pe;
-        a.vir = (double)fa.vir + (double)fb.vir;
       } else {
         const double xi = sx[sl], yi = sy[sl], zi = sz[sl];
         const int ti = (int)v.pos[i].w;

@@ -66,8 +66,24 @@ def qvectors(L: float, q: float, count: int = 48, tol: float = 0.1):
     """Integer vectors n with |2 pi n / L| within tol of q (up to `count`,
     nearest first, sign-symmetric pairs kept together)."""
     nmax = int(np.ceil((q + tol) * L / (2 * np.pi))) + 1
+    r_lo = max(q - tol, 0.0) * L / (2 * np.pi)
+    r_hi = (q + tol) * L / (2 * np.pi)
+    # only the columns (nx, ny) that reach the shell, and the nz range there
     g = np.arange(-nmax, nmax + 1)
-    n = np.stack(np.meshgrid(g, g, g, indexing="ij"), axis=-1).reshape(-1, 3)
+    nx, ny = (a.ravel() for a in np.meshgrid(g, g, indexing="ij"))
+    rho2 = (nx * nx + ny * ny).astype(np.float64)
+    keep = rho2 <= r_hi * r_hi + 1.0
+    nx, ny, rho2 = nx[keep], ny[keep], rho2[keep]
+    zmax = np.floor(np.sqrt(np.maximum(r_hi * r_hi - rho2, 0.0)) + 1.0).astype(np.int64)
+    zmin = np.maximum(np.ceil(np.sqrt(np.maximum(r_lo * r_lo - rho2, 0.0))) - 1.0, 0.0).astype(np.int64)
+    rows = []
+    for sgn in (1, -1):
+        lo = zmin if sgn > 0 else np.maximum(zmin, 1)  # z = 0 once
+        cnt = np.maximum(zmax - lo + 1, 0)
+        base = np.repeat(lo, cnt)
+        off = np.arange(cnt.sum()) - np.repeat(np.cumsum(cnt) - cnt, cnt)
+        rows.append(np.stack([np.repeat(nx, cnt), np.repeat(ny, cnt), sgn * (base + off)], axis=1))
+    n = np.concatenate(rows)
     qq = 2 * np.pi * np.sqrt((n * n).sum(axis=1)) / L
     sel = np.abs(qq - q) <= tol
     n, qq = n[sel], qq[sel]

@@ -68,6 +68,16 @@ def request_footprint(req: RunRequest) -> int:
     return footprint([request_params(req)]) + req.max_live_origins * req.n * 24 + (4 << 20)
 
 
+_QCACHE: dict = {}
+
+
+def _qvectors_cached(L: float, q: float, count: int):
+    key = (L, q, count)
+    if key not in _QCACHE:
+        _QCACHE[key] = qvectors(L, q, count)
+    return _QCACHE[key]
+
+
 def start_run(req: RunRequest, device: int = 0) -> Engine:
     e = Engine(request_params(req), device=device)
     st = lattice_state(req.n, req.T, seed=req.seed)
@@ -76,7 +86,7 @@ def start_run(req: RunRequest, device: int = 0) -> Engine:
     q = e.thermo(0)["q"]
     e.set_nhc(0, np.zeros(3), np.sqrt(req.T * q) * rng.standard_normal(3))
     e.obs_configure(0, req.steps, min(req.num_origins, max(1, req.steps // 2)), 1.4, 0, 0.3,
-                    qvectors(st.L, req.q, 24), req.max_live_origins)
+                    _qvectors_cached(st.L, req.q, 24), req.max_live_origins)
     return e
 
 

@@ -283,6 +283,22 @@ def served_run(args, device, plain_value):
     return st
 
 
+def reduce_across_ranks(x, dist, device, op="max"):
+    """x reduced over the ranks (max or min) of the default process group;
+    x itself without one."""
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.MIN)
+    return float(t.item())
+
+
+def replica_throughput(world, n, steps, max_ms):
+    """Particle-steps/s of `world` replicas of n particles, each `steps` steps,
+    timed by the slowest rank."""
+    return world * n * steps / (max_ms * 1e-3)
+
+
 def run_ours(args):
     import torch
     rank = int(os.environ.get("RANK", "0"))
@@ -316,12 +332,9 @@ def run_ours(args):
     with ClockSampler(local) as clk:
         dev_ms, launches = e.bench_steps(nchunks, 256 << 20)
     barrier()
-    t = torch.tensor([dev_ms], dtype=torch.float64, device=f"cuda:{local}")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
+    max_ms = reduce_across_ranks(dev_ms, dist, f"cuda:{local}", "max")
     steps = 32 * nchunks
-    value = world * n * steps / (max_ms * 1e-3)
+    value = replica_throughput(world, n, steps, max_ms)
 
     # dominant kernel: pair forces (timed alone, force-only mode, warm L2)
     t_force = e.time_stage(1, reps=64)
@@ -343,9 +356,7 @@ def run_ours(args):
     if world == 1 and args.workload in ("all", "serve"):
         extra["served"] = served_run(args, local, value)
     if dist is not None:
-        te = torch.tensor([e2e_val], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(te, op=dist.ReduceOp.MIN)
-        e2e_val = float(te.item()) * world
+        e2e_val = reduce_across_ranks(e2e_val, dist, f"cuda:{local}", "min") * world
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -61,3 +61,58 @@ def test_fp32_forces_and_nve_drift(cuda_lib, g4000):
     assert force_err(out[1][0], out[0][0]) <= 1e-5
     assert rel(out[1][1], out[0][1]) <= 1e-5
     assert out[0][2] < 1e-4 and out[1][2] < 1e-4
+
+
+def test_batch_equals_alone(cuda_lib):
+    """Replicas advanced inside one batch engine give bit-identical states,
+    energies and observables to the same systems advanced alone (the batch
+    splits whole boxes into blocks differently; the sums do not depend on it)."""
+    from activechi4_b200.batch import make_engine, replica_set
+    reps = replica_set(count=6, n_min=600, n_max=9000, seed=5)
+    p_eta = np.array([0.1, -0.05, 0.02])
+    e = make_engine(reps)
+    for r in range(e.nsys):
+        e.set_nhc(r, np.zeros(3), p_eta)
+        e.obs_configure(r, 300, 3, 1.4, 0, 0.3, None, 4)
+    # rebuilds during set-up (each load primes the lists) are not part of the run
+    rb0 = [e.thermo(r)["rebuilds"] for r in range(e.nsys)]
+    e.step(300)
+    for r, (p, st) in enumerate(reps):
+        a = make_engine([(p, st)])
+        a.set_nhc(0, np.zeros(3), p_eta)
+        a.obs_configure(0, 300, 3, 1.4, 0, 0.3, None, 4)
+        ra0 = a.thermo(0)["rebuilds"]
+        a.step(300)
+        for u, w in zip(a.get_state(0), e.get_state(r)):
+            assert np.array_equal(u, w)
+        ta, tb = a.thermo(0), e.thermo(r)
+        assert ta["pe"] == tb["pe"] and ta["ke"] == tb["ke"]
+        assert ta["rebuilds"] - ra0 == tb["rebuilds"] - rb0[r]
+        assert np.array_equal(a.obs_sums(0)[1], e.obs_sums(r)[1])
+        a.close()
+    e.close()
+
+
+def test_restart_files_round_trip(cuda_lib, tmp_path):
+    """A GPU run saved in the reference's restart/active files and resumed in
+    a fresh engine the way initialise_restart_state does gives the same forces
+    as the saved state (to the files' 14 decimals)."""
+    from activechi4_b200 import Engine, default_params, formats
+    from activechi4_b200.init import lattice_state
+    n = 4000
+    e = Engine(default_params(n, T=0.45, f0=1.0))
+    e.set_state(0, lattice_state(n, 0.8, seed=9))
+    e.step(200)
+    formats.save_run(e, 0, tmp_path / "restart_file.dat", tmp_path / "ActiveDirection.dat",
+                     tmp_path / "ActiveFileIndex.dat", iteration=200)
+    st, it, _ = formats.load_restart_state(tmp_path / "restart_file.dat", tmp_path / "ActiveFileIndex.dat",
+                                           tmp_path / "ActiveDirection.dat", n)
+    assert it == 200
+    e.compute_forces()
+    F0 = e.get_state(0)[3]
+    b = Engine(default_params(n, T=0.45, f0=1.0, L=st.L))
+    b.set_state(0, st)
+    b.compute_forces()
+    F1 = b.get_state(0)[3]
+    assert force_err(F1, F0) < 1e-9
+    assert np.array_equal(b.get_directions(0), e.get_directions(0))
