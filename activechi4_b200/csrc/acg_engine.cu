@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -202,6 +203,14 @@ struct acg_engine {
   int gsteps = 0;
   cudaGraphExec_t gexec1 = nullptr;
   cudaGraph_t graph1 = nullptr;
+  // device-loop graphs of acg_step: two copies of the LOOP_STEPS-step body
+  // used in turn (a launch never waits for the other copy) and a 1-step body
+  // for the remainder; counts[0..2] are their block counters
+  cudaGraphExec_t wexec[3] = {nullptr, nullptr, nullptr};
+  cudaGraph_t wgraph[3] = {nullptr, nullptr, nullptr};
+  long long *counts = nullptr;
+  int wturn = 0;
+  bool no_while = false;  // the device loop could not be built: launch per 32 steps
   void *flush = nullptr;  // bench-only L2 flush buffer
   size_t flush_bytes = 0;
   std::vector<std::vector<void *>> obs_bufs;  // per system: device buffers of the observables
@@ -308,6 +317,52 @@ void drop_graphs(acg_engine *e) {
   e->gexec = e->gexec1 = nullptr;
   e->graph = e->graph1 = nullptr;
   e->gsteps = 0;
+  for (int k = 0; k < 3; k++) {
+    if (e->wexec[k]) cudaGraphExecDestroy(e->wexec[k]);
+    if (e->wgraph[k]) cudaGraphDestroy(e->wgraph[k]);
+    e->wexec[k] = nullptr;
+    e->wgraph[k] = nullptr;
+  }
+}
+
+// Destroying a graph with conditional nodes waits until the whole device is
+// idle, which would stall every other engine's work each time one engine is
+// destroyed (a served run ending).  Destroyed engines therefore hand their
+// graphs to this list; acg_release_retired (or the list growing past
+// RETIRE_MAX) destroys them when the caller chooses.
+struct Retired {
+  int device;
+  cudaGraphExec_t exec;
+  cudaGraph_t graph;
+};
+std::mutex g_retire_mu;
+std::vector<Retired> g_retired;
+constexpr size_t RETIRE_MAX = 256;
+
+void release_retired_locked() {
+  int cur = 0;
+  cudaGetDevice(&cur);
+  for (auto &r : g_retired) {
+    cudaSetDevice(r.device);
+    if (r.exec) cudaGraphExecDestroy(r.exec);
+    if (r.graph) cudaGraphDestroy(r.graph);
+  }
+  g_retired.clear();
+  cudaSetDevice(cur);
+}
+
+void retire_graphs(acg_engine *e) {
+  std::lock_guard<std::mutex> lk(g_retire_mu);
+  g_retired.push_back({e->device, e->gexec, e->graph});
+  g_retired.push_back({e->device, e->gexec1, e->graph1});
+  e->gexec = e->gexec1 = nullptr;
+  e->graph = e->graph1 = nullptr;
+  for (int k = 0; k < 3; k++) {
+    g_retired.push_back({e->device, e->wexec[k], e->wgraph[k]});
+    e->wexec[k] = nullptr;
+    e->wgraph[k] = nullptr;
+  }
+  if (g_retired.size() > RETIRE_MAX) release_retired_locked();
 }
 
 // ---- launches --------------------------------------------------------------
@@ -387,33 +442,14 @@ int add_kernel(cudaGraph_t g, const cudaGraphNode_t *dep, size_t ndep, cudaGraph
   return ACG_OK;
 }
 
-int build_graph(acg_engine *e, int K, cudaGraph_t *gout, cudaGraphExec_t *xout) {
-  cudaGraph_t g;
-  CK(cudaGraphCreate(&g, 0));
+// K timesteps appended to graph g after node *prev (none when null); *prev
+// becomes the last node.  The conditional handles belong to g.
+int add_steps(acg_engine *e, cudaGraph_t g, int K, cudaGraphNode_t *prev_io) {
   View v = e->v;
   const int prec = e->lay.desc[0].precision;
-  if (e->fused) {
-    // one whole-step launch per step, all systems of the batch
-    StepFn sf = steps_fn(e->btpp, prec);
-    cudaGraphNode_t prev = nullptr;
-    int one = 1;
-    for (int s = 0; s < K; s++) {
-      void *a[] = {&v, &one};
-      cudaGraphNode_t nn;
-      int rc = add_kernel(g, prev ? &prev : nullptr, prev ? 1 : 0, &nn, (void *)sf, e->lay.nsys, BLOCK_F, a,
-                          steps_smem(e->lay.box_nmax, prec));
-      if (rc) return rc;
-      prev = nn;
-    }
-    cudaGraphExec_t x;
-    CK(cudaGraphInstantiate(&x, g, 0));
-    *gout = g;
-    *xout = x;
-    return ACG_OK;
-  }
+  cudaGraphNode_t prev = *prev_io;
   ForceFn ff = force_fn(e->tpp, prec);
   GroupFn gf = group_fn(e->gtpp, prec);
-  cudaGraphNode_t prev = nullptr;
   GroupFn xf = box_fn(e->btpp, prec);
   int mode0 = 0, use_cond = 1, tbase = e->ntiles_g + e->ntiles_x;
   for (int s = 0; s < K; s++) {
@@ -484,8 +520,87 @@ int build_graph(acg_engine *e, int K, cudaGraph_t *gout, cudaGraphExec_t *xout) 
     if (rc) return rc;
     prev = no;
   }
+  *prev_io = prev;
+  return ACG_OK;
+}
+
+int build_graph(acg_engine *e, int K, cudaGraph_t *gout, cudaGraphExec_t *xout) {
+  cudaGraph_t g;
+  CK(cudaGraphCreate(&g, 0));
+  View v = e->v;
+  const int prec = e->lay.desc[0].precision;
+  if (e->fused) {
+    // one whole-step launch per step, all systems of the batch
+    StepFn sf = steps_fn(e->btpp, prec);
+    cudaGraphNode_t prev = nullptr;
+    int one = 1;
+    for (int s = 0; s < K; s++) {
+      void *a[] = {&v, &one};
+      cudaGraphNode_t nn;
+      int rc = add_kernel(g, prev ? &prev : nullptr, prev ? 1 : 0, &nn, (void *)sf, e->lay.nsys, BLOCK_F, a,
+                          steps_smem(e->lay.box_nmax, prec));
+      if (rc) return rc;
+      prev = nn;
+    }
+    cudaGraphExec_t x;
+    CK(cudaGraphInstantiate(&x, g, 0));
+    *gout = g;
+    *xout = x;
+    return ACG_OK;
+  }
+  cudaGraphNode_t prev = nullptr;
+  int rc = add_steps(e, g, K, &prev);
+  if (rc) return rc;
   cudaGraphExec_t x;
   CK(cudaGraphInstantiate(&x, g, 0));
+  *gout = g;
+  *xout = x;
+  return ACG_OK;
+}
+
+// A graph that runs K-step blocks in a device-side loop: a WHILE conditional
+// node whose body holds K steps and a control kernel that counts the blocks
+// left in *count (set before each launch) and ends the loop at zero.  One
+// launch runs any number of blocks, so the host never re-launches a graph
+// that is still running (which blocks the calling thread until it ends).
+int build_while_graph(acg_engine *e, int K, long long *count, cudaGraph_t *gout, cudaGraphExec_t *xout) {
+  cudaGraph_t g;
+  CK(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle hw;
+  CK(cudaGraphConditionalHandleCreate(&hw, g, 1, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams wp = {};
+  wp.type = cudaGraphNodeTypeConditional;
+  wp.conditional.handle = hw;
+  wp.conditional.type = cudaGraphCondTypeWhile;
+  wp.conditional.size = 1;
+  cudaGraphNode_t nw;
+  if (cudaGraphAddNode(&nw, g, nullptr, 0, &wp) != cudaSuccess) {
+    cudaGetLastError();
+    cudaGraphDestroy(g);
+    return ACG_ERR_CUDA;
+  }
+  cudaGraph_t body = wp.conditional.phGraph_out[0];
+  cudaGraphNode_t prev = nullptr;
+  int rc = add_steps(e, body, K, &prev);
+  if (rc) {
+    cudaGetLastError();
+    cudaGraphDestroy(g);
+    return rc;
+  }
+  cudaGraphNode_t nl;
+  void *la[] = {&count, &hw};
+  rc = add_kernel(body, &prev, 1, &nl, (void *)k_loop_ctl, 1, 32, la);
+  if (rc) {
+    cudaGetLastError();
+    cudaGraphDestroy(g);
+    return rc;
+  }
+  cudaGraphExec_t x;
+  if (cudaGraphInstantiate(&x, g, 0) != cudaSuccess) {
+    cudaGetLastError();
+    cudaGraphDestroy(g);
+    return ACG_ERR_CUDA;
+  }
   *gout = g;
   *xout = x;
   return ACG_OK;
@@ -556,7 +671,11 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
     return fail(ACG_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(ce));
   }
   ce = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
-  if (ce == cudaSuccess) ce = cudaMalloc(&e->arena, e->lay.bytes);
+  // stream-ordered: allocating and freeing an engine's memory does not wait
+  // for the work of other engines on the device (a served run's start and end
+  // do not stall the runs in flight)
+  if (ce == cudaSuccess) ce = cudaMallocAsync(&e->arena, e->lay.bytes, e->stream);
+  if (ce == cudaSuccess) ce = cudaMallocAsync((void **)&e->counts, 4 * sizeof(long long), e->stream);
   if (ce != cudaSuccess) {
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
@@ -744,13 +863,23 @@ int acg_destroy(acg_engine *e) {
   if (!e) return ACG_OK;
   cudaSetDevice(e->device);
   if (e->stream) cudaStreamSynchronize(e->stream);
-  drop_graphs(e);
+  retire_graphs(e);
   for (auto &bs : e->obs_bufs)
-    for (void *b : bs) cudaFree(b);
+    for (void *b : bs) cudaFreeAsync(b, e->stream);
   if (e->flush) cudaFree(e->flush);
-  if (e->arena) cudaFree(e->arena);
-  if (e->stream) cudaStreamDestroy(e->stream);
+  if (e->arena) cudaFreeAsync(e->arena, e->stream);
+  if (e->counts) cudaFreeAsync(e->counts, e->stream);
+  if (e->stream) {
+    cudaStreamSynchronize(e->stream);
+    cudaStreamDestroy(e->stream);
+  }
   delete e;
+  return ACG_OK;
+}
+
+int acg_release_retired(void) {
+  std::lock_guard<std::mutex> lk(g_retire_mu);
+  release_retired_locked();
   return ACG_OK;
 }
 
@@ -765,6 +894,28 @@ int acg_system_size(acg_engine *e, int sys, int *n, int *nact) {
 }
 
 void *acg_stream(acg_engine *e) { return e ? (void *)e->stream : nullptr; }
+
+int acg_set_priority(acg_engine *e, int level) {
+  if (!e) return fail(ACG_ERR_INVALID, "null engine");
+  CK(cudaSetDevice(e->device));
+  int least = 0, greatest = 0;
+  CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  // level 0 = the default (least urgent); each level up moves one step
+  // towards `greatest` (numerically lower), clamped to the device's range
+  const int prio = std::max(greatest, least - std::max(level, 0));
+  cudaStream_t s = nullptr;
+  CK(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, prio));
+  // work and stream-ordered memory of the old stream finish before the new
+  // stream runs anything
+  cudaEvent_t ev;
+  CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  CK(cudaEventRecord(ev, e->stream));
+  CK(cudaStreamWaitEvent(s, ev, 0));
+  CK(cudaEventDestroy(ev));
+  CK(cudaStreamDestroy(e->stream));
+  e->stream = s;
+  return ACG_OK;
+}
 
 int acg_set_state(acg_engine *e, int sys, const double *x, const double *xu, const double *p,
                   const int *type, const int *act_tag) {
@@ -934,6 +1085,29 @@ int acg_step(acg_engine *e, int nsteps) {
   CK(cudaSetDevice(e->device));
   int rc = prime(e);
   if (rc) return rc;
+  if (!e->fused && !e->no_while) {
+    // device loop: one launch for the GRAPH_STEPS-step blocks, one for the rest
+    const long long q = nsteps / GRAPH_STEPS, r = nsteps % GRAPH_STEPS;
+    const int need[3] = {q > 0 && e->wturn == 0, q > 0 && e->wturn == 1, r > 0};
+    for (int k = 0; k < 3 && !e->no_while; k++)
+      if (need[k] && !e->wexec[k] &&
+          build_while_graph(e, k < 2 ? GRAPH_STEPS : 1, e->counts + k, &e->wgraph[k], &e->wexec[k]) != ACG_OK)
+        e->no_while = true;
+    if (!e->no_while) {
+      if (q > 0) {
+        k_set_count<<<1, 32, 0, e->stream>>>(e->counts + e->wturn, q);
+        CK(cudaGetLastError());
+        CK(cudaGraphLaunch(e->wexec[e->wturn], e->stream));
+        e->wturn ^= 1;
+      }
+      if (r > 0) {
+        k_set_count<<<1, 32, 0, e->stream>>>(e->counts + 2, r);
+        CK(cudaGetLastError());
+        CK(cudaGraphLaunch(e->wexec[2], e->stream));
+      }
+      return ACG_OK;
+    }
+  }
   if (nsteps >= GRAPH_STEPS && !e->gexec) {
     rc = build_graph(e, GRAPH_STEPS, &e->graph, &e->gexec);
     if (rc) return rc;
@@ -1178,10 +1352,10 @@ int acg_obs_configure(acg_engine *e, int sys, const acg_obs_config *c) {
     h_step[i] = ev[i].step;
     h_info[i] = ev[i].kind | (ev[i].slot << 1) | (ev[i].bin << 13);
   }
-  for (void *b : e->obs_bufs[sys]) cudaFree(b);
+  for (void *b : e->obs_bufs[sys]) cudaFreeAsync(b, e->stream);
   e->obs_bufs[sys].clear();
   auto dalloc = [&](size_t bytes, void **p) {
-    cudaError_t ce = cudaMalloc(p, bytes > 0 ? bytes : 8);
+    cudaError_t ce = cudaMallocAsync(p, bytes > 0 ? bytes : 8, e->stream);
     if (ce == cudaSuccess) e->obs_bufs[sys].push_back(*p);
     return ce;
   };

@@ -1981,6 +1981,20 @@ __global__ void __launch_bounds__(BLOCK_F) k_steps_box(View v, int nsteps) {
 }
 
 // ---------------------------------------------------------------------------
+// device-side step loop control (a graph's WHILE node): one block of steps done
+__global__ void k_loop_ctl(long long *count, cudaGraphConditionalHandle h) {
+  if (threadIdx.x == 0) {
+    const long long c = *count - 1;
+    *count = c;
+    cudaGraphSetConditional(h, c > 0 ? 1u : 0u);
+  }
+}
+
+__global__ void k_set_count(long long *count, long long n) {
+  if (threadIdx.x == 0) *count = n;
+}
+
+// ---------------------------------------------------------------------------
 // state upload / download (caller order <-> slots)
 __global__ void k_load(View v, int r) {
   const SysDesc &d = v.desc[r];

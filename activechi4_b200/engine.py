@@ -47,6 +47,11 @@ def measure_fp64_peak(device: int = 0) -> float:
     return t.value
 
 
+def release_retired():
+    """Destroy the CUDA graphs of closed engines (waits for the device)."""
+    check(_abi.lib().acg_release_retired())
+
+
 def observables_from_sums(offset, sums, dt=0.005) -> dict:
     """Per-bin averages from summed (Q, Q^2, msd, msd_d4, msd_r4, Fs, count);
     sums of several replicas with equal parameters may be added first (chi4
@@ -275,6 +280,11 @@ class Engine:
         nl = C.c_int64()
         check(self._lib.acg_bench_steps(self.h, int(nchunks), int(flush_bytes), C.byref(ms), C.byref(nl)))
         return ms.value, nl.value
+
+    def set_priority(self, level: int):
+        """Stream priority among engines on the device (0 = default, higher
+        first)."""
+        check(self._lib.acg_set_priority(self.h, int(level)))
 
     @property
     def stream(self) -> int:

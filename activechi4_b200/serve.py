@@ -22,7 +22,7 @@ import time
 
 import numpy as np
 
-from .engine import Engine, default_params, footprint, qvectors
+from .engine import Engine, default_params, footprint, qvectors, release_retired
 from .init import lattice_state
 
 
@@ -78,8 +78,15 @@ def _qvectors_cached(L: float, q: float, count: int):
     return _QCACHE[key]
 
 
-def start_run(req: RunRequest, device: int = 0) -> Engine:
+def start_run(req: RunRequest, device: int = 0, setup_priority: int = 0) -> Engine:
+    """A request's engine, loaded and primed.  With `setup_priority` > 0 the
+    set-up work (upload, first lists and forces, observable buffers) runs at
+    that stream priority, so it does not wait behind the queued steps of the
+    runs already on the device (the set-up reads results back, which would
+    otherwise block the host for as long as that queue takes)."""
     e = Engine(request_params(req), device=device)
+    if setup_priority > 0:
+        e.set_priority(setup_priority)
     st = lattice_state(req.n, req.T, seed=req.seed)
     e.set_state(0, st)
     rng = np.random.default_rng(req.seed)
@@ -96,9 +103,13 @@ def finish_run(e: Engine, req: RunRequest, arrival, admitted, finished) -> RunRe
 
 
 class Server:
-    """Admit-as-memory-frees scheduler over per-run engines and streams."""
+    """Admit-as-memory-frees scheduler over per-run engines and streams.
 
-    def __init__(self, device=0, hbm_budget=None, max_active=32, chunk_work=2.0e7):
+    Each active run keeps `depth` chunks of steps queued on its stream (a CUDA
+    event marks the end of each), so the GPU has work from every run while the
+    host admits new requests or builds their graphs."""
+
+    def __init__(self, device=0, hbm_budget=None, max_active=16, chunk_work=2.0e7, depth=2, size_priority=True):
         self.device = device
         if hbm_budget is None:
             import torch
@@ -107,12 +118,28 @@ class Server:
         self.budget = int(hbm_budget)
         self.max_active = max_active
         self.chunk_work = chunk_work
+        self.depth = max(1, int(depth))
+        self.size_priority = size_priority
 
     def _chunk(self, n, left):
         k = int(max(32, min(8192, round(self.chunk_work / max(n, 1) / 32) * 32)))
         return min(k, left)
 
+    def _feed(self, run):
+        """Queue chunks until `depth` are in flight or the run is fully queued."""
+        import torch
+        while len(run["inflight"]) < self.depth and run["left"] > 0:
+            k = self._chunk(run["req"].n, run["left"])
+            run["engine"].step(k)
+            ev = torch.cuda.Event()
+            ev.record(run["stream"])
+            run["inflight"].append(ev)
+            run["left"] -= k
+
     def run(self, requests, clock=time.perf_counter):
+        import collections
+
+        import torch
         pending = sorted(requests, key=lambda r: r.arrival)
         queue, active, results = [], {}, []
         used = 0
@@ -127,30 +154,38 @@ class Server:
                 if used + fp > self.budget and active:
                     break
                 req = queue.pop(0)
-                e = start_run(req, self.device)
+                e = start_run(req, self.device, setup_priority=5)
+                # stepping priority: by size if asked (larger systems first:
+                # their kernels fill the GPU, latency-bound small runs use
+                # the gaps), else the default
+                e.set_priority(int(np.clip(2.0 * (math.log10(req.n) - 3.0), 0, 4)) if self.size_priority else 0)
                 used += fp
-                left = req.steps
-                k = self._chunk(req.n, left)
-                e.step(k)
-                active[req.rid] = [e, req, left - k, clock() - t0, fp]
+                run = {"engine": e, "req": req, "left": req.steps, "adm": clock() - t0, "fp": fp,
+                       "stream": torch.cuda.ExternalStream(e.stream, device=torch.device("cuda", self.device)),
+                       "inflight": collections.deque()}
+                self._feed(run)
+                active[req.rid] = run
             progressed = False
             for rid in list(active):
-                e, req, left, adm, fp = active[rid]
-                if not e.poll():
-                    continue
-                progressed = True
-                if left == 0:
-                    results.append(finish_run(e, req, req.arrival, adm, clock() - t0))
+                run = active[rid]
+                while run["inflight"] and run["inflight"][0].query():
+                    run["inflight"].popleft()
+                    progressed = True
+                if run["left"] == 0 and not run["inflight"]:
+                    e, req = run["engine"], run["req"]
+                    e.sync()
+                    results.append(finish_run(e, req, req.arrival, run["adm"], clock() - t0))
                     e.close()
-                    used -= fp
+                    used -= run["fp"]
                     del active[rid]
                 else:
-                    k = self._chunk(req.n, left)
-                    e.step(k)
-                    active[rid][2] = left - k
+                    self._feed(run)
+            if not active:
+                release_retired()  # nothing in flight: destroying graphs stalls nothing
             if not progressed:
                 nxt = pending[0].arrival - (clock() - t0) if (pending and not queue and not active) else 2e-4
                 time.sleep(max(5e-5, min(nxt, 2e-3)))
+        release_retired()
         return sorted(results, key=lambda r: r.rid)
 
 

@@ -271,7 +271,7 @@ def served_run(args, device, plain_value):
     one on the plain FP64 path."""
     from activechi4_b200.serve import Server, latency_stats, poisson_requests, run_serial
     reqs = poisson_requests(args.requests, rate=20.0, scale=0.01, seed=5, precision=1)
-    res = Server(device=device, max_active=32).run(reqs)
+    res = Server(device=device).run(reqs)
     st = latency_stats(res)
     ser, wall = run_serial(reqs, device=device, precision=0)
     work = sum(r.n * r.steps for r in reqs)

@@ -99,6 +99,13 @@ int acg_params_default(acg_params *p, int n);
  * the device. */
 int acg_create(const acg_params *params, int nsys, int device, acg_engine **out);
 int acg_destroy(acg_engine *e);
+/* Destroy the CUDA graphs of engines destroyed so far.  acg_destroy frees an
+ * engine's memory in stream order but only retires its graphs: destroying a
+ * graph that holds conditional nodes waits for the whole device, which would
+ * stall other engines' work.  Call this when the device may idle (the run
+ * server does when no run is active); it also happens by itself once 256
+ * graphs are retired.  No counterpart in the reference. */
+int acg_release_retired(void);
 
 /* Bytes of device memory acg_create would allocate for these systems
  * (admission control for serving). */
@@ -193,6 +200,12 @@ int acg_obs_sums(acg_engine *e, int sys, int *nbins, int64_t *offset, double *su
 int acg_num_systems(acg_engine *e);
 int acg_system_size(acg_engine *e, int sys, int *n, int *nact);
 void *acg_stream(acg_engine *e);
+/* Scheduling priority of the engine's stream among the work of other engines
+ * on the same device: 0 = default, higher levels are scheduled first (clamped
+ * to the device's range).  No counterpart in the reference (one program per
+ * rank); the run server uses it to keep large runs from being crowded out by
+ * many small ones. */
+int acg_set_priority(acg_engine *e, int level);
 
 /* Kernel timing for profiling: average device time in ms of `reps`
  * back-to-back launches of one stage over all systems, timed with CUDA events
