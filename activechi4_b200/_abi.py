@@ -82,6 +82,7 @@ _SIGS = {
     "acg_stream": (C.c_void_p, [C.c_void_p]),
     "acg_set_priority": (C.c_int, [C.c_void_p, C.c_int]),
     "acg_release_retired": (C.c_int, []),
+    "acg_prepare": (C.c_int, [C.c_void_p]),
     "acg_time_stage": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)]),
     "acg_set_launch": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "acg_get_launch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -334,6 +334,7 @@ struct Retired {
   int device;
   cudaGraphExec_t exec;
   cudaGraph_t graph;
+  cudaStream_t stream;  // the stream the graph last ran in, destroyed with it
 };
 std::mutex g_retire_mu;
 std::vector<Retired> g_retired;
@@ -346,6 +347,7 @@ void release_retired_locked() {
     cudaSetDevice(r.device);
     if (r.exec) cudaGraphExecDestroy(r.exec);
     if (r.graph) cudaGraphDestroy(r.graph);
+    if (r.stream) cudaStreamDestroy(r.stream);
   }
   g_retired.clear();
   cudaSetDevice(cur);
@@ -353,15 +355,18 @@ void release_retired_locked() {
 
 void retire_graphs(acg_engine *e) {
   std::lock_guard<std::mutex> lk(g_retire_mu);
-  g_retired.push_back({e->device, e->gexec, e->graph});
-  g_retired.push_back({e->device, e->gexec1, e->graph1});
+  g_retired.push_back({e->device, e->gexec, e->graph, nullptr});
+  g_retired.push_back({e->device, e->gexec1, e->graph1, nullptr});
   e->gexec = e->gexec1 = nullptr;
   e->graph = e->graph1 = nullptr;
   for (int k = 0; k < 3; k++) {
-    g_retired.push_back({e->device, e->wexec[k], e->wgraph[k]});
+    g_retired.push_back({e->device, e->wexec[k], e->wgraph[k], nullptr});
     e->wexec[k] = nullptr;
     e->wgraph[k] = nullptr;
   }
+  // the stream goes with the graphs (destroying it while they live made the
+  // next graph instantiation on the device wait for all device work)
+  g_retired.push_back({e->device, nullptr, nullptr, e->stream});
   if (g_retired.size() > RETIRE_MAX) release_retired_locked();
 }
 
@@ -863,16 +868,13 @@ int acg_destroy(acg_engine *e) {
   if (!e) return ACG_OK;
   cudaSetDevice(e->device);
   if (e->stream) cudaStreamSynchronize(e->stream);
-  retire_graphs(e);
   for (auto &bs : e->obs_bufs)
     for (void *b : bs) cudaFreeAsync(b, e->stream);
   if (e->flush) cudaFree(e->flush);
   if (e->arena) cudaFreeAsync(e->arena, e->stream);
   if (e->counts) cudaFreeAsync(e->counts, e->stream);
-  if (e->stream) {
-    cudaStreamSynchronize(e->stream);
-    cudaStreamDestroy(e->stream);
-  }
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  retire_graphs(e);  // graphs and stream: destroyed by acg_release_retired
   delete e;
   return ACG_OK;
 }
@@ -1123,6 +1125,19 @@ int acg_step(acg_engine *e, int nsteps) {
     left -= GRAPH_STEPS;
   }
   while (left-- > 0) CK(cudaGraphLaunch(e->gexec1, e->stream));
+  return ACG_OK;
+}
+
+int acg_prepare(acg_engine *e) {
+  if (!e) return fail(ACG_ERR_INVALID, "null engine");
+  CK(cudaSetDevice(e->device));
+  int rc = prime(e);
+  if (rc) return rc;
+  if (e->fused || e->no_while) return ACG_OK;
+  for (int k = 0; k < 3 && !e->no_while; k++)
+    if (!e->wexec[k] &&
+        build_while_graph(e, k < 2 ? GRAPH_STEPS : 1, e->counts + k, &e->wgraph[k], &e->wexec[k]) != ACG_OK)
+      e->no_while = true;
   return ACG_OK;
 }
 

@@ -281,6 +281,11 @@ class Engine:
         check(self._lib.acg_bench_steps(self.h, int(nchunks), int(flush_bytes), C.byref(ms), C.byref(nl)))
         return ms.value, nl.value
 
+    def prepare(self):
+        """Prime and build the step graphs now (may wait for queued device
+        work; safe to call from another thread)."""
+        check(self._lib.acg_prepare(self.h))
+
     def set_priority(self, level: int):
         """Stream priority among engines on the device (0 = default, higher
         first)."""

@@ -122,7 +122,10 @@ class Server:
         self.size_priority = size_priority
 
     def _chunk(self, n, left):
-        k = int(max(32, min(8192, round(self.chunk_work / max(n, 1) / 32) * 32)))
+        # about chunk_work particle-steps, and no more than ~20 ms of device
+        # time for small systems, whose steps cost ~50 us whatever their size
+        k = min(self.chunk_work / max(n, 1), 0.02 / 5e-5)
+        k = int(max(32, min(8192, round(k / 32) * 32)))
         return min(k, left)
 
     def _feed(self, run):
@@ -163,6 +166,9 @@ class Server:
                 run = {"engine": e, "req": req, "left": req.steps, "adm": clock() - t0, "fp": fp,
                        "stream": torch.cuda.ExternalStream(e.stream, device=torch.device("cuda", self.device)),
                        "inflight": collections.deque()}
+                # graphs built now (this can wait for the work queued on the
+                # device, which the time-bounded chunks keep short)
+                e.prepare()
                 self._feed(run)
                 active[req.rid] = run
             progressed = False

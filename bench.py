@@ -270,6 +270,9 @@ def served_run(args, device, plain_value):
     pair forces, in-place Q/chi4/MSD/Fs; against the same requests run one by
     one on the plain FP64 path."""
     from activechi4_b200.serve import Server, latency_stats, poisson_requests, run_serial
+    # a short untimed burst first (other seeds): a running server has its
+    # kernels loaded and its allocator pool grown
+    Server(device=device).run(poisson_requests(12, rate=20.0, scale=0.01, seed=99, precision=1))
     reqs = poisson_requests(args.requests, rate=20.0, scale=0.01, seed=5, precision=1)
     res = Server(device=device).run(reqs)
     st = latency_stats(res)

@@ -157,6 +157,12 @@ int acg_step(acg_engine *e, int nsteps);
 /* The same steps launched kernel by kernel without a CUDA graph (every
  * rebuild kernel is launched and skips the systems that need no rebuild). */
 int acg_step_eager(acg_engine *e, int nsteps);
+/* Prime the engine and build the CUDA graphs acg_step launches, without
+ * stepping.  Instantiating a graph can wait for the work already queued on
+ * the device, so a host that drives several engines may call this from a
+ * second thread while it keeps feeding the others.  No counterpart in the
+ * reference. */
+int acg_prepare(acg_engine *e);
 int acg_sync(acg_engine *e);
 /* Non-blocking: *done = 1 when all work queued on the engine has finished. */
 int acg_poll(acg_engine *e, int *done);
