@@ -325,6 +325,16 @@ void drop_graphs(acg_engine *e) {
   }
 }
 
+// what decides the node structure of an engine's device-loop graph: graphs of
+// the same shape differ only in node parameters (pointers, grids, shared
+// memory) and can be updated in place instead of instantiated anew
+std::string graph_shape(const acg_engine *e, int K) {
+  char b[160];
+  snprintf(b, sizeof(b), "K%d g%d x%d b%d l%d p%d t%d/%d/%d/%d", K, e->ntiles_g > 0, e->ntiles_x > 0,
+           e->ntiles_b > 0, e->ntiles_l > 0, e->lay.desc[0].precision, e->tpp, e->gtpp, e->btpp, e->block);
+  return b;
+}
+
 // Destroying a graph with conditional nodes waits until the whole device is
 // idle, which would stall every other engine's work each time one engine is
 // destroyed (a served run ending).  Destroyed engines therefore hand their
@@ -334,7 +344,8 @@ struct Retired {
   int device;
   cudaGraphExec_t exec;
   cudaGraph_t graph;
-  cudaStream_t stream;  // the stream the graph last ran in, destroyed with it
+  cudaStream_t stream;
+  std::string shape;  // device-loop graphs: reusable by an engine of the same shape
 };
 std::mutex g_retire_mu;
 std::vector<Retired> g_retired;
@@ -355,18 +366,15 @@ void release_retired_locked() {
 
 void retire_graphs(acg_engine *e) {
   std::lock_guard<std::mutex> lk(g_retire_mu);
-  g_retired.push_back({e->device, e->gexec, e->graph, nullptr});
-  g_retired.push_back({e->device, e->gexec1, e->graph1, nullptr});
+  g_retired.push_back({e->device, e->gexec, e->graph, nullptr, ""});
+  g_retired.push_back({e->device, e->gexec1, e->graph1, nullptr, ""});
   e->gexec = e->gexec1 = nullptr;
   e->graph = e->graph1 = nullptr;
   for (int k = 0; k < 3; k++) {
-    g_retired.push_back({e->device, e->wexec[k], e->wgraph[k], nullptr});
+    if (e->wexec[k]) g_retired.push_back({e->device, e->wexec[k], e->wgraph[k], nullptr, graph_shape(e, k < 2 ? GRAPH_STEPS : 1)});
     e->wexec[k] = nullptr;
     e->wgraph[k] = nullptr;
   }
-  // the stream goes with the graphs (destroying it while they live made the
-  // next graph instantiation on the device wait for all device work)
-  g_retired.push_back({e->device, nullptr, nullptr, e->stream});
   if (g_retired.size() > RETIRE_MAX) release_retired_locked();
 }
 
@@ -600,8 +608,28 @@ int build_while_graph(acg_engine *e, int K, long long *count, cudaGraph_t *gout,
     cudaGraphDestroy(g);
     return rc;
   }
-  cudaGraphExec_t x;
-  if (cudaGraphInstantiate(&x, g, 0) != cudaSuccess) {
+  // an executable graph of the same shape left by a destroyed engine is
+  // updated with this graph's parameters (instantiating a new one can wait
+  // for all work queued on the device)
+  cudaGraphExec_t x = nullptr;
+  {
+    const std::string shape = graph_shape(e, K);
+    std::lock_guard<std::mutex> lk(g_retire_mu);
+    for (size_t i = 0; i < g_retired.size(); i++) {
+      Retired &r = g_retired[i];
+      if (!r.exec || r.device != e->device || r.shape != shape) continue;
+      cudaGraphExecUpdateResultInfo info;
+      if (cudaGraphExecUpdate(r.exec, g, &info) == cudaSuccess) {
+        x = r.exec;
+        if (r.graph) cudaGraphDestroy(r.graph);
+        g_retired.erase(g_retired.begin() + i);
+      } else {
+        cudaGetLastError();
+      }
+      break;
+    }
+  }
+  if (!x && cudaGraphInstantiate(&x, g, 0) != cudaSuccess) {
     cudaGetLastError();
     cudaGraphDestroy(g);
     return ACG_ERR_CUDA;
@@ -873,8 +901,11 @@ int acg_destroy(acg_engine *e) {
   if (e->flush) cudaFree(e->flush);
   if (e->arena) cudaFreeAsync(e->arena, e->stream);
   if (e->counts) cudaFreeAsync(e->counts, e->stream);
-  if (e->stream) cudaStreamSynchronize(e->stream);
-  retire_graphs(e);  // graphs and stream: destroyed by acg_release_retired
+  if (e->stream) {
+    cudaStreamSynchronize(e->stream);
+    cudaStreamDestroy(e->stream);
+  }
+  retire_graphs(e);  // destroyed by acg_release_retired, or reused
   delete e;
   return ACG_OK;
 }

@@ -194,3 +194,19 @@ def test_nonfinite_state_is_reported(cuda_lib, g1000):
     with pytest.raises(AcgError) as ei:
         e.thermo()
     assert ei.value.code == -4
+
+
+def test_reused_step_graph_matches_eager(cuda_lib, g1000):
+    """A closed engine leaves its device-loop step graph for reuse by the next
+    engine of the same shape (updated in place, not instantiated anew); the
+    reusing engine must step exactly like the eager launches."""
+    a = engine_for(g1000, shuffle=1, tau_p_steps=20)
+    a.step(70)
+    a.close()
+    b = engine_for(g1000, shuffle=1, tau_p_steps=20)
+    c = engine_for(g1000, shuffle=1, tau_p_steps=20)
+    b.step(70)
+    c.step_eager(70)
+    for u, w in zip(b.get_state(), c.get_state()):
+        assert np.array_equal(u, w)
+    assert b.thermo()["rebuilds"] == c.thermo()["rebuilds"]
