@@ -21,7 +21,7 @@ F0_SET = (0.0, 0.5, 1.0, 2.0)
 TAU_SET = (20, 200, 2000)
 
 
-def replica_set(count=256, n_min=500, n_max=4000, seed=0, precision=1):
+def replica_set(count=256, n_min=500, n_max=4000, seed=0, precision=1, skin=0.35):
     rng = np.random.default_rng(seed)
     out = []
     for r in range(count):
@@ -30,7 +30,7 @@ def replica_set(count=256, n_min=500, n_max=4000, seed=0, precision=1):
         f0 = float(rng.choice(F0_SET))
         tau = int(rng.choice(TAU_SET))
         p = default_params(n, T=T, f0=f0, tau_p_steps=tau, precision=precision, seed=1000 + r,
-                           list_mode=1, rebuild_factor=4.0)
+                           list_mode=1, rebuild_factor=4.0, skin=skin)
         out.append((p, lattice_state(n, T, seed=seed * 100000 + r)))
     return out
 

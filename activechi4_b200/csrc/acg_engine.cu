@@ -127,7 +127,7 @@ int plan(const acg_params *params, int nsys, Layout &lay, int nsm) {
       // 2 cells per side: one cell (of up to ~100 particles) per block
       d.cpb = d.nc == 2 ? 1 : cpb;
       d.xoff = lay.nboxtiles;
-      if (d.box) lay.nboxtiles += (d.ncell + cpb - 1) / cpb;
+      if (d.box) lay.nboxtiles += (d.ncell + d.cpb - 1) / d.cpb;
     }
   }
   // neighbour-row capacity: 1.45x the ideal-gas count within the widest list
@@ -804,6 +804,10 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
                    [&](int2 a, int2 b) { return e->lay.desc[a.x].n > e->lay.desc[b.x].n; });
   e->ntiles_x = (int)h_x.size();
   v.ntiles_x = e->ntiles_x;
+  if (e->ntiles_x != L.nboxtiles) {  // the arena holds exactly nboxtiles tiles and partials
+    acg_destroy(e);
+    return fail(ACG_ERR_INVALID, "internal: whole-box tile count differs from the layout");
+  }
   e->ntiles_a = (int)h_a.size();
   e->ntiles_l = (int)h_l.size();
   e->ntiles_c = (int)h_c.size();

@@ -116,3 +116,30 @@ def test_restart_files_round_trip(cuda_lib, tmp_path):
     F1 = b.get_state(0)[3]
     assert force_err(F1, F0) < 1e-9
     assert np.array_equal(b.get_directions(0), e.get_directions(0))
+
+
+def test_large_batch_finite_and_equal_alone(cuda_lib):
+    """The batched workload's 256 replicas (whole boxes split several cells
+    per block, two-cell boxes one cell per block) stay finite, and replicas of
+    each box kind match the same system run alone."""
+    from activechi4_b200.batch import make_engine, replica_set
+    from activechi4_b200.init import box_length
+    reps = replica_set(count=256, seed=11, precision=1)
+    p_eta = np.array([0.1, -0.05, 0.02])
+    e = make_engine(reps)
+    for r in range(e.nsys):
+        e.set_nhc(r, np.zeros(3), p_eta)
+    e.step(96)
+    for r in range(e.nsys):
+        th = e.thermo(r)
+        assert np.isfinite(th["ke"]) and 0.0 < th["inst_T"] < 10.0, (r, th["inst_T"])
+    nc = [int(int(box_length(p.n)) / 2.85) for p, _ in reps]
+    picks = [nc.index(k) for k in (2, 3, 4) if k in nc]
+    for r in picks:
+        a = make_engine([reps[r]])
+        a.set_nhc(0, np.zeros(3), p_eta)
+        a.step(96)
+        for u, w in zip(a.get_state(0), e.get_state(r)):
+            assert np.array_equal(u, w)
+        a.close()
+    e.close()
