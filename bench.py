@@ -256,6 +256,10 @@ def batched_run(args, device):
     ms, launches = e.bench_steps(nchunks, 256 << 20)
     ntot = sum(e.n(r) for r in range(e.nsys))
     steps = 32 * nchunks
+    # a speed measured on a system that blew up is no measurement
+    temps = [e.thermo(r)["inst_T"] for r in range(e.nsys)]
+    if not all(math.isfinite(t) and 0.0 < t < 10.0 for t in temps):
+        raise RuntimeError("batched replicas left the physical range during the timed run")
     e.close()
     return {"value": ntot * steps / (ms * 1e-3), "unit": "particle-steps/s", "replicas": len(reps),
             "particles": ntot, "steps": steps, "ms_per_step": ms / steps, "dtype": "f32-pair/f64-state",
@@ -276,6 +280,8 @@ def served_run(args, device, plain_value):
     reqs = poisson_requests(args.requests, rate=20.0, scale=0.01, seed=5, precision=1)
     res = Server(device=device).run(reqs)
     st = latency_stats(res)
+    if not all(math.isfinite(r.pe) and math.isfinite(r.ke) for r in res):
+        raise RuntimeError("a served run produced non-finite energies")
     ser, wall = run_serial(reqs, device=device, precision=0)
     work = sum(r.n * r.steps for r in reqs)
     st.update({"serial_fp64_particle_steps_per_s": work / wall, "serial_fp64_wall_s": wall,
@@ -349,6 +355,8 @@ def run_ours(args):
     fp64_ach = PAIRS_PER_PARTICLE * FLOPS_PER_PAIR * n / (t_force * 1e-3) / 1e12
     traffic = ncu_traffic()
     th = e.thermo(0)
+    if not (math.isfinite(th["ke"]) and 0.0 < th["inst_T"] < 10.0):
+        raise RuntimeError("the timed system left the physical range")
 
     e2e_val, h2d, d2h = e2e_run(e, st, nchunks)
     e.close()
