@@ -388,7 +388,7 @@ int launch_rebuild(acg_engine *e) {
   k_cells_order<<<e->ntiles_c, 32 * CELLS_PER_TILE, 0, s>>>(v);
   k_permute<<<e->ntiles_a, BLOCK_R, 0, s>>>(v);
   if (e->ntiles_g) k_build_list_groups<<<e->ntiles_g, BLOCK_G, list_smem(v.gcap), s>>>(v);
-  if (e->ntiles_x) k_build_list_box<<<e->ntiles_x, BLOCK_X, box_list_smem(e->lay.box_nmax), s>>>(v);
+  if (e->ntiles_x) k_build_list_box<<<e->ntiles_x * LIST_SPLIT, BLOCK_X, box_list_smem(e->lay.box_nmax), s>>>(v);
   if (e->ntiles_l) k_build_list<<<e->ntiles_l, BLOCK_L, 0, s>>>(v);
   CK(cudaGetLastError());
   return ACG_OK;
@@ -492,7 +492,7 @@ int add_steps(acg_engine *e, cudaGraph_t g, int K, cudaGraphNode_t *prev_io) {
               {(void *)k_cells_order, e->ntiles_c, 32 * CELLS_PER_TILE, 0},
               {(void *)k_permute, e->ntiles_a, BLOCK_R, 0},
               {(void *)k_build_list_groups, e->ntiles_g, BLOCK_G, list_smem(v.gcap)},
-              {(void *)k_build_list_box, e->ntiles_x, BLOCK_X, box_list_smem(e->lay.box_nmax)},
+              {(void *)k_build_list_box, e->ntiles_x * LIST_SPLIT, BLOCK_X, box_list_smem(e->lay.box_nmax)},
               {(void *)k_build_list, e->ntiles_l, BLOCK_L, 0}};
     cudaGraphNode_t bp = nullptr;
     for (auto &k : rb) {

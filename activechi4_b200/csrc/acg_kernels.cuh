@@ -1618,36 +1618,110 @@ __device__ __forceinline__ void box_stage_list(const View &v, const SysDesc &d, 
   }
 }
 
-// lists of a whole box: one warp per cell of the block, one lane per particle;
-// the 27 neighbour cells (with their periodic image shifts; at 2 cells per side
-// a cell appears under two shifts, of which at most one can be in range since
-// L > 2 x the list cut) are tested against the staged reduced coordinates
+// lists of up to 8 particles of cell c of a whole box (particles w0.. of the
+// cell), four lanes per particle: the four lanes of a particle test four
+// consecutive staged candidates at a time and a ballot ranks the partners
+// found, so the entries keep the staged order (the 27 neighbour cells with
+// their periodic image shifts, slot order within a cell; at 2 cells per side
+// every particle of the box once under the minimum image).  The lists are the
+// ones one lane per particle would write, in a quarter of the serial chain.
+__device__ __forceinline__ void box_list_group(const View &v, const SysDesc &d, int r, const float4 *xstg,
+                                               const int *cst, const int *pre4, int c, int w0, int lane) {
+  const int nc = d.nc, n = d.n;
+  const double iL2 = 1.0 / (d.L * d.L);
+  float lc[3];
+  for (int k = 0; k < 3; k++) lc[k] = (float)(lcut2_of(d, k) * iL2 * (1.0 + 1e-5));
+  uint16_t *lst = box_list(v, d);
+  const int maxnb = v.maxnb;
+  const int sub = lane & 3, grp = lane >> 2;
+  const int m = cst[c + 1] - cst[c];
+  const int w = w0 + grp;
+  const bool valid = w < m;
+  const int sl = cst[c] + w, ps = pre4[c] + w;
+  // a lane past the cell's particles gets NaN coordinates: it passes no test
+  const float nan = __int_as_float(0x7fc00000);
+  const float4 fi = valid ? xstg[ps] : make_float4(nan, nan, nan, __int_as_float(0));
+  const int ti = __float_as_int(fi.w) >> 15;
+  const float c0 = ti == 0 ? lc[0] : lc[1], c1 = ti == 0 ? lc[1] : lc[2];
+  const unsigned below = (1u << sub) - 1u;
+  int cnt = 0;
+  // one staged candidate per lane; the run [q0, q1) is a multiple of four long
+  auto scan = [&](int q0, int q1, float xi, float yi, float zi, bool wrap) {
+    for (int q = q0 + sub; q < q1; q += 4) {
+      const float4 fj = xstg[q];
+      float ex = xi - fj.x, ey = yi - fj.y, ez = zi - fj.z;
+      if (wrap) {
+        ex -= rintf(ex);
+        ey -= rintf(ey);
+        ez -= rintf(ez);
+      }
+      const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+      const int code = __float_as_int(fj.w);
+      const bool ok = valid && r2 < ((code >> 15) ? c1 : c0) && q != ps;
+      const unsigned gm = (__ballot_sync(0xffffffffu, ok) >> (4 * grp)) & 15u;
+      if (ok) {
+        const int k = cnt + __popc(gm & below);
+        if (k < maxnb) lst[((size_t)(k >> 2) * n + sl) * 4 + (k & 3)] = (uint16_t)(code & 0xffff);
+      }
+      cnt += __popc(gm);
+    }
+  };
+  if (nc == 2) {
+    // two cells per side: every cell neighbours every other under two
+    // images, so each particle is tested once with the minimum image
+    scan(0, pre4[d.ncell], fi.x, fi.y, fi.z, true);
+  } else {
+    const int cx = c % nc, cy = (c / nc) % nc, cz = c / (nc * nc);
+    for (int dz = -1; dz <= 1; dz++)
+      for (int dy = -1; dy <= 1; dy++)
+        for (int dx = -1; dx <= 1; dx++) {
+          const int ax = cx + dx, ay = cy + dy, az = cz + dz;
+          const int sx = ax < 0 ? -1 : (ax >= nc ? 1 : 0), sy = ay < 0 ? -1 : (ay >= nc ? 1 : 0),
+                    sz = az < 0 ? -1 : (az >= nc ? 1 : 0);
+          const int c2 = (ax - sx * nc) + (ay - sy * nc) * nc + (az - sz * nc) * nc * nc;
+          // candidate image x_j + s: compare x_i - s with x_j
+          scan(pre4[c2], pre4[c2 + 1], fi.x - (float)sx, fi.y - (float)sy, fi.z - (float)sz, false);
+        }
+  }
+  if (valid && sub == 0) {
+    const int i = d.poff + sl;
+    if (cnt > maxnb) {
+      v.nbn[i] = -1;
+      atomicAdd(&v.st[r].overflow, 1);
+    } else {
+      v.nbn[i] = cnt;
+    }
+  }
+}
+
+// lists of a whole box.  A tile's cells are shared by LIST_SPLIT blocks: the
+// work items (cell, 8 particles) of the tile go round the LIST_SPLIT x 8 warps,
+// so a system that rebuilds while others do not still spreads over many SMs;
+// every block stages the system once.
 __global__ void __launch_bounds__(BLOCK_X) k_build_list_box(View v) {
   extern __shared__ float4 xstg[];
   __shared__ int cst[MAX_BOX_CELLS + 1], pre4[MAX_BOX_CELLS + 1];
-  const int2 tile = v.tiles_x[blockIdx.x];
+  const int2 tile = v.tiles_x[blockIdx.x / LIST_SPLIT];
+  const int part = blockIdx.x % LIST_SPLIT;
   const int r = tile.x, b = tile.y;
   if (!v.st[r].rebuild) return;
   const SysDesc &d = v.desc[r];
   const int nce = d.ncell;
   box_cells(v, d, cst, pre4);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int W = LIST_SPLIT * nw, gw = part * nw + (threadIdx.x >> 5);
   box_stage_list(v, d, xstg, cst, pre4);
   __syncthreads();
-  // work items (cell, round of 32 particles) of the block's cells, one warp each
   const int ca = b * d.cpb, cb = min(nce, ca + d.cpb);
   int item = 0;
   for (int c = ca; c < cb; c++) {
-    const int rounds = (cst[c + 1] - cst[c] + 31) >> 5;
-    const int nw = blockDim.x >> 5;
-    // warps item..item+rounds-1 (mod nw) take this cell's rounds
-    const int first = item % nw;
-    const int k = (warp - first + nw) % nw;
-    if (k < rounds) box_list_cell(v, d, r, xstg, cst, pre4, c, lane, k, nw);
-    item += rounds;
+    const int groups = (cst[c + 1] - cst[c] + 7) >> 3;
+    // warp gw takes the cell's groups g with (item + g) % W == gw
+    for (int g = (gw - item % W + W) % W; g < groups; g += W) box_list_group(v, d, r, xstg, cst, pre4, c, 8 * g, lane);
+    item += groups;
   }
-  __syncthreads();
-  for (int sl = cst[ca] + threadIdx.x; sl < cst[cb]; sl += blockDim.x) copy_back(v, d.poff + sl);
+  const int stride = LIST_SPLIT * blockDim.x;
+  for (int sl = cst[ca] + part * blockDim.x + threadIdx.x; sl < cst[cb]; sl += stride) copy_back(v, d.poff + sl);
 }
 
 // the system's current positions staged for the pair loop: FP32 as 32-bit
