@@ -38,6 +38,7 @@ constexpr int LIST_SPLIT = 4;     // blocks sharing a whole-box tile in the list
 constexpr int MAX_BOX_NC = 4;     // whole-box mode for 2..4 cells per side
 constexpr int MAX_BOX_CELLS = MAX_BOX_NC * MAX_BOX_NC * MAX_BOX_NC;
 constexpr int MAX_BOX_N = 8192;   // whole-box staging limit (FP64: 192 KB of shared memory)
+constexpr int MAX_SUB3 = 1000;    // list sub-cells of a whole box (side >= 1.45 and L < 15: <= 10^3)
 
 // A cell group: up to 2 x 2 x 2 cells (clipped at the box edge) and the union
 // of their neighbour cells, up to 4 x 4 x 4, in which union cell (ux,uy,uz)
@@ -69,7 +70,7 @@ struct SysDesc {
   int tile0_b, ntile_b, tau_p, thermostat;
   int shuffle, list_mode, precision, goff;  // goff: offset of the system's groups
   int tile0_a, ntile_a, box, xoff;            // kick/drift tiles; box: whole-box kernels (2..4 cells per side), xoff: first box tile
-  int cpb, pad4, pad5, pad6;                  // cpb: cells per whole-box block
+  int cpb, msub, pad5, pad6;                  // cpb: cells per whole-box block
   double L, invL, inv_cell;  // inv_cell: cells per unit reduced length (InvCellSize)
   double T, f0, dt, half_dt, skin2, rebuild_factor, dof;
   double q[NHC_M];

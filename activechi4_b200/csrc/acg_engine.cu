@@ -37,6 +37,7 @@ constexpr int GRAPH_STEPS = 32;
 
 struct Layout {
   int nsys = 0, nslots = 0, ncells = 0, nact = 0, maxnb = 0, ngroups = 0, nboxtiles = 0, box_nmax = 0;
+  int box_m3max = 0;  // most list sub-cells of a whole-box system (0: none uses them)
   std::vector<SysDesc> desc;
   size_t bytes = 0;
 };
@@ -110,6 +111,20 @@ int plan(const acg_params *params, int nsys, Layout &lay, int nsm) {
     d.goff = lay.ngroups;
     lay.ngroups += d.ng * d.ng * d.ng;
     if (d.box) lay.box_nmax = std::max(lay.box_nmax, d.n);
+    // list sub-cells of a whole box: side >= 1.45 and >= half the widest list
+    // cut, so a partner is at most two sub-cells away on each axis; at least 5
+    // per side (each of the 5 x 5 x 5 neighbours once), else the cell path
+    d.msub = 0;
+    if (d.box) {
+      double rl = 0;
+      for (int t = 0; t < 3; t++) rl = std::max(rl, std::sqrt(d.lcut2[t]));
+      const double h = std::max(1.45, 0.5 * rl * (1.0 + 1e-9));
+      const int m = (int)(d.L / h);
+      if (m >= 5 && m * m * m <= MAX_SUB3) {
+        d.msub = m;
+        lay.box_m3max = std::max(lay.box_m3max, m * m * m);
+      }
+    }
     lay.nslots += (int)align_up((size_t)d.n, 32);
     lay.ncells += d.ncell;
     lay.nact += d.nact;
@@ -243,7 +258,14 @@ GroupFn box_fn(int gtpp, int prec) {
 }
 // whole-box staging: int4 fixed point (FP32) or three doubles (FP64) per particle
 size_t box_smem(int nmax, int prec) { return (size_t)nmax * (prec ? sizeof(int4) : 3 * sizeof(double)); }
-size_t box_list_smem(int nmax) { return ((size_t)nmax + 3 * MAX_BOX_CELLS) * sizeof(float4); }
+// whole-box list build: the staged system padded per cell (cell path, also the
+// fused kernel's) or, for the sub-cell path, the system in sub-cell order, two
+// 16-bit arrays of n and the sub-cell starts and fill counters
+size_t box_list_smem_cells(int nmax) { return ((size_t)nmax + 3 * MAX_BOX_CELLS) * sizeof(float4); }
+size_t box_list_smem(int nmax, int m3max) {
+  const size_t sub = m3max > 0 ? (size_t)nmax * (sizeof(float4) + 2 * sizeof(uint16_t)) + (2 * (size_t)m3max + 1) * sizeof(int) : 0;
+  return std::max(box_list_smem_cells(nmax), sub);
+}
 
 using StepFn = void (*)(View, int);
 StepFn steps_fn(int gtpp, int prec) {
@@ -254,7 +276,7 @@ StepFn steps_fn(int gtpp, int prec) {
   }
   return nullptr;
 }
-size_t steps_smem(int nmax, int prec) { return std::max(box_list_smem(nmax), box_smem(nmax, prec)); }
+size_t steps_smem(int nmax, int prec) { return std::max(box_list_smem_cells(nmax), box_smem(nmax, prec)); }
 
 ForceFn force_fn(int tpp, int prec) {
 #define F(T)                                                                     \
@@ -388,7 +410,7 @@ int launch_rebuild(acg_engine *e) {
   k_cells_order<<<e->ntiles_c, 32 * CELLS_PER_TILE, 0, s>>>(v);
   k_permute<<<e->ntiles_a, BLOCK_R, 0, s>>>(v);
   if (e->ntiles_g) k_build_list_groups<<<e->ntiles_g, BLOCK_G, list_smem(v.gcap), s>>>(v);
-  if (e->ntiles_x) k_build_list_box<<<e->ntiles_x * LIST_SPLIT, BLOCK_X, box_list_smem(e->lay.box_nmax), s>>>(v);
+  if (e->ntiles_x) k_build_list_box<<<e->ntiles_x * LIST_SPLIT, BLOCK_X, box_list_smem(e->lay.box_nmax, e->lay.box_m3max), s>>>(v);
   if (e->ntiles_l) k_build_list<<<e->ntiles_l, BLOCK_L, 0, s>>>(v);
   CK(cudaGetLastError());
   return ACG_OK;
@@ -492,7 +514,7 @@ int add_steps(acg_engine *e, cudaGraph_t g, int K, cudaGraphNode_t *prev_io) {
               {(void *)k_cells_order, e->ntiles_c, 32 * CELLS_PER_TILE, 0},
               {(void *)k_permute, e->ntiles_a, BLOCK_R, 0},
               {(void *)k_build_list_groups, e->ntiles_g, BLOCK_G, list_smem(v.gcap)},
-              {(void *)k_build_list_box, e->ntiles_x * LIST_SPLIT, BLOCK_X, box_list_smem(e->lay.box_nmax)},
+              {(void *)k_build_list_box, e->ntiles_x * LIST_SPLIT, BLOCK_X, box_list_smem(e->lay.box_nmax, e->lay.box_m3max)},
               {(void *)k_build_list, e->ntiles_l, BLOCK_L, 0}};
     cudaGraphNode_t bp = nullptr;
     for (auto &k : rb) {
@@ -838,13 +860,13 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
     for (int pr : {0, 1}) attr_ok = attr_ok && raise_smem((const void *)group_fn(gt, pr), group_smem(v.gcap));
   attr_ok = attr_ok && raise_smem((const void *)k_build_list_groups, list_smem(v.gcap));
   if (L.box_nmax > 0) {
-    if (box_list_smem(L.box_nmax) > 227 * 1024 || box_smem(L.box_nmax, 0) > 227 * 1024) {
+    if (box_list_smem(L.box_nmax, L.box_m3max) > 227 * 1024 || box_smem(L.box_nmax, 0) > 227 * 1024) {
       acg_destroy(e);
       return fail(ACG_ERR_INVALID, "whole-box system too large for shared memory");
     }
     for (int gt : {1, 2, 4})
       for (int pr : {0, 1}) attr_ok = attr_ok && raise_smem((const void *)box_fn(gt, pr), box_smem(L.box_nmax, pr));
-    attr_ok = attr_ok && raise_smem((const void *)k_build_list_box, box_list_smem(L.box_nmax));
+    attr_ok = attr_ok && raise_smem((const void *)k_build_list_box, box_list_smem(L.box_nmax, L.box_m3max));
     for (int gt : {1, 2, 4})
       for (int pr : {0, 1}) attr_ok = attr_ok && raise_smem((const void *)steps_fn(gt, pr), steps_smem(L.box_nmax, pr));
   }

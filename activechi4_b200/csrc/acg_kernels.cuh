@@ -1694,10 +1694,169 @@ __device__ __forceinline__ void box_list_group(const View &v, const SysDesc &d, 
   }
 }
 
-// lists of a whole box.  A tile's cells are shared by LIST_SPLIT blocks: the
-// work items (cell, 8 particles) of the tile go round the LIST_SPLIT x 8 warps,
-// so a system that rebuilds while others do not still spreads over many SMs;
-// every block stages the system once.
+// Lists of a whole box from list sub-cells (d.msub per side, side >= half the
+// widest list cut): a partner is at most two sub-cells away on each axis, so the
+// candidates of a particle are the 5 x 5 x 5 sub-cells around its own, 25 rows
+// of 5 sub-cells that are contiguous in sub-cell order (a row that crosses the
+// box edge is two runs with their image shifts) -- about a quarter of the
+// volume of the 27 reference cells of a small box.
+//
+// Each block sorts the system into sub-cell order in shared memory (a counting
+// sort; members of a sub-cell in slot order, so the order does not depend on
+// the atomics) and builds the lists of a range of centre sub-cells, eight lanes
+// per particle: the lanes of a particle test eight consecutive candidates and a
+// ballot ranks the partners found, so entries keep the sorted order.
+__device__ __forceinline__ int subcell_of(double x, int m) { return min(max((int)(x * (double)m), 0), m - 1); }
+
+__device__ __forceinline__ void box_list_sub(const View &v, const SysDesc &d, int r, const float4 *xs,
+                                             const int *sst, int S, int w0, int lane) {
+  const int m = d.msub, n = d.n;
+  const double iL2 = 1.0 / (d.L * d.L);
+  float lc[3];
+  for (int k = 0; k < 3; k++) lc[k] = (float)(lcut2_of(d, k) * iL2 * (1.0 + 1e-5));
+  uint16_t *lst = box_list(v, d);
+  const int maxnb = v.maxnb;
+  const int sub = lane & 7, grp = lane >> 3;
+  const int w = w0 + grp;
+  const bool valid = w < sst[S + 1] - sst[S];
+  const int ps = sst[S] + w;
+  const float nan = __int_as_float(0x7fc00000);
+  const float4 fi = valid ? xs[ps] : make_float4(nan, nan, nan, __int_as_float(0));
+  const int codei = __float_as_int(fi.w);
+  const int sl = codei & 0x7fff, ti = codei >> 15;
+  const float c0 = ti == 0 ? lc[0] : lc[1], c1 = ti == 0 ? lc[1] : lc[2];
+  const unsigned below = (1u << sub) - 1u;
+  int cnt = 0;
+  // candidates [q0, q1) of the sorted system, eight at a time
+  auto scan = [&](int q0, int q1, float xi, float yi, float zi) {
+    const int iters = (q1 - q0 + 7) >> 3;
+    for (int it = 0, q = q0 + sub; it < iters; it++, q += 8) {
+      const bool live = q < q1;
+      const float4 fj = live ? xs[q] : make_float4(nan, nan, nan, __int_as_float(0));
+      const float ex = xi - fj.x, ey = yi - fj.y, ez = zi - fj.z;
+      const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+      const int code = __float_as_int(fj.w);
+      const bool ok = valid && live && r2 < ((code >> 15) ? c1 : c0) && q != ps;
+      const unsigned gm = (__ballot_sync(0xffffffffu, ok) >> (8 * grp)) & 255u;
+      if (ok) {
+        const int k = cnt + __popc(gm & below);
+        if (k < maxnb) lst[((size_t)(k >> 2) * n + sl) * 4 + (k & 3)] = (uint16_t)(code & 0xffff);
+      }
+      cnt += __popc(gm);
+    }
+  };
+  const int a = S % m, b = (S / m) % m, c = S / (m * m);
+  for (int dz = -2; dz <= 2; dz++) {
+    int az = c + dz;
+    const int sz = az < 0 ? -1 : (az >= m ? 1 : 0);
+    az -= sz * m;
+    for (int dy = -2; dy <= 2; dy++) {
+      int ay = b + dy;
+      const int sy = ay < 0 ? -1 : (ay >= m ? 1 : 0);
+      ay -= sy * m;
+      const int row = m * (ay + m * az);
+      // candidate image x_j + s: compare x_i - s with x_j
+      const float yi = fi.y - (float)sy, zi = fi.z - (float)sz;
+      int xa = a - 2;
+      const int xb = a + 3;
+      if (xa < 0) {
+        scan(sst[row + m + xa], sst[row + m], fi.x + 1.0f, yi, zi);
+        xa = 0;
+      }
+      if (xb > m) {
+        scan(sst[row + xa], sst[row + m], fi.x, yi, zi);
+        scan(sst[row], sst[row + xb - m], fi.x - 1.0f, yi, zi);
+      } else {
+        scan(sst[row + xa], sst[row + xb], fi.x, yi, zi);
+      }
+    }
+  }
+  if (valid && sub == 0) {
+    const int i = d.poff + sl;
+    if (cnt > maxnb) {
+      v.nbn[i] = -1;
+      atomicAdd(&v.st[r].overflow, 1);
+    } else {
+      v.nbn[i] = cnt;
+    }
+  }
+}
+
+// block gp of G: sort the system into sub-cell order, then the lists of the
+// centre sub-cells [gp M3 / G, (gp + 1) M3 / G)
+__device__ void box_list_subcells(const View &v, const SysDesc &d, int r, int gp, int G, unsigned char *smem) {
+  const int n = d.n, m = d.msub, M3 = m * m * m;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  float4 *xs = reinterpret_cast<float4 *>(smem);
+  uint16_t *key = reinterpret_cast<uint16_t *>(xs + n);  // sub-cell of slot s
+  uint16_t *ord = key + n;                               // slot at sorted position (unordered in a sub-cell)
+  int *sst = reinterpret_cast<int *>(ord + n);           // [M3 + 1] sub-cell starts
+  int *fill = sst + M3 + 1;                              // [M3]
+  const double4 *pp = v.pos_s + d.poff;
+  for (int k = threadIdx.x; k < M3; k += blockDim.x) fill[k] = 0;
+  __syncthreads();
+  for (int s = threadIdx.x; s < n; s += blockDim.x) {
+    const double4 p = pp[s];
+    const int k = subcell_of(p.x, m) + m * (subcell_of(p.y, m) + m * subcell_of(p.z, m));
+    key[s] = (uint16_t)k;
+    atomicAdd(&fill[k], 1);
+  }
+  __syncthreads();
+  {
+    // exclusive scan of the counts: a run of sub-cells per thread, then warps
+    __shared__ int wsum[32];
+    const int per = (M3 + blockDim.x - 1) / blockDim.x;
+    const int k0 = min((int)threadIdx.x * per, M3), k1 = min(k0 + per, M3);
+    int loc = 0;
+    for (int k = k0; k < k1; k++) loc += fill[k];
+    int incl = loc;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    int before = 0;
+    for (int w = 0; w < warp; w++) before += wsum[w];
+    int run = before + incl - loc;
+    for (int k = k0; k < k1; k++) {
+      const int c = fill[k];
+      sst[k] = run;
+      fill[k] = 0;
+      run += c;
+    }
+    if (threadIdx.x == blockDim.x - 1) sst[M3] = run;
+    __syncthreads();
+  }
+  for (int s = threadIdx.x; s < n; s += blockDim.x) {
+    const int k = key[s];
+    ord[sst[k] + atomicAdd(&fill[k], 1)] = (uint16_t)s;
+  }
+  __syncthreads();
+  // final place of a member: its sub-cell's start + the members of lower slot
+  for (int q = threadIdx.x; q < n; q += blockDim.x) {
+    const int s = ord[q], k = key[s];
+    const int q0 = sst[k], q1 = sst[k + 1];
+    int rank = 0;
+    for (int t = q0; t < q1; t++) rank += ord[t] < s;
+    const double4 p = pp[s];
+    xs[q0 + rank] = make_float4((float)p.x, (float)p.y, (float)p.z, __int_as_float(s | ((int)p.w << 15)));
+  }
+  __syncthreads();
+  const int S0 = (int)((long long)gp * M3 / G), S1 = (int)((long long)(gp + 1) * M3 / G);
+  int item = 0;
+  for (int S = S0; S < S1; S++) {
+    const int groups = (sst[S + 1] - sst[S] + 3) >> 2;
+    for (int g = (warp - item % nw + nw) % nw; g < groups; g += nw) box_list_sub(v, d, r, xs, sst, S, 4 * g, lane);
+    item += groups;
+  }
+}
+
+// lists of a whole box, each tile shared by LIST_SPLIT blocks so that a system
+// that rebuilds while others do not still spreads over many SMs: with list
+// sub-cells, the system's centre sub-cells are split over its tiles' blocks;
+// otherwise the work items (cell, 8 particles) of the tile go round the
+// LIST_SPLIT x 8 warps.  Every block stages the system once.
 __global__ void __launch_bounds__(BLOCK_X) k_build_list_box(View v) {
   extern __shared__ float4 xstg[];
   __shared__ int cst[MAX_BOX_CELLS + 1], pre4[MAX_BOX_CELLS + 1];
@@ -1709,16 +1868,21 @@ __global__ void __launch_bounds__(BLOCK_X) k_build_list_box(View v) {
   const int nce = d.ncell;
   box_cells(v, d, cst, pre4);
   const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  const int W = LIST_SPLIT * nw, gw = part * nw + (threadIdx.x >> 5);
-  box_stage_list(v, d, xstg, cst, pre4);
-  __syncthreads();
   const int ca = b * d.cpb, cb = min(nce, ca + d.cpb);
-  int item = 0;
-  for (int c = ca; c < cb; c++) {
-    const int groups = (cst[c + 1] - cst[c] + 7) >> 3;
-    // warp gw takes the cell's groups g with (item + g) % W == gw
-    for (int g = (gw - item % W + W) % W; g < groups; g += W) box_list_group(v, d, r, xstg, cst, pre4, c, 8 * g, lane);
-    item += groups;
+  if (d.msub >= 5) {
+    box_list_subcells(v, d, r, b * LIST_SPLIT + part, d.ntile_b * LIST_SPLIT, reinterpret_cast<unsigned char *>(xstg));
+  } else {
+    const int W = LIST_SPLIT * nw, gw = part * nw + (threadIdx.x >> 5);
+    box_stage_list(v, d, xstg, cst, pre4);
+    __syncthreads();
+    int item = 0;
+    for (int c = ca; c < cb; c++) {
+      const int groups = (cst[c + 1] - cst[c] + 7) >> 3;
+      // warp gw takes the cell's groups g with (item + g) % W == gw
+      for (int g = (gw - item % W + W) % W; g < groups; g += W)
+        box_list_group(v, d, r, xstg, cst, pre4, c, 8 * g, lane);
+      item += groups;
+    }
   }
   const int stride = LIST_SPLIT * blockDim.x;
   for (int sl = cst[ca] + part * blockDim.x + threadIdx.x; sl < cst[cb]; sl += stride) copy_back(v, d.poff + sl);
