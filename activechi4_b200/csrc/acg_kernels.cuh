@@ -1696,88 +1696,109 @@ __device__ __forceinline__ void box_list_group(const View &v, const SysDesc &d, 
 
 // Lists of a whole box from list sub-cells (d.msub per side, side >= half the
 // widest list cut): a partner is at most two sub-cells away on each axis, so the
-// candidates of a particle are the 5 x 5 x 5 sub-cells around its own, 25 rows
-// of 5 sub-cells that are contiguous in sub-cell order (a row that crosses the
-// box edge is two runs with their image shifts) -- about a quarter of the
-// volume of the 27 reference cells of a small box.
+// candidates of a particle are the 5 x 5 x 5 sub-cells around its own, rows of
+// sub-cells that are contiguous in sub-cell order (a row that crosses the box
+// edge is two runs with their image shifts) -- about a quarter of the volume of
+// the 27 reference cells of a small box.
 //
 // Each block sorts the system into sub-cell order in shared memory (a counting
 // sort; members of a sub-cell in slot order, so the order does not depend on
-// the atomics) and builds the lists of a range of centre sub-cells, eight lanes
-// per particle: the lanes of a particle test eight consecutive candidates and a
-// ballot ranks the partners found, so entries keep the sorted order.
+// the atomics), then its warps take bricks of 2 x 2 x d.bz sub-cells, one lane
+// per particle, and scan the union of the brick's neighbourhoods.
 __device__ __forceinline__ int subcell_of(double x, int m) { return min(max((int)(x * (double)m), 0), m - 1); }
 
-__device__ __forceinline__ void box_list_sub(const View &v, const SysDesc &d, int r, const float4 *xs,
-                                             const int *sst, int S, int w0, int lane) {
-  const int m = d.msub, n = d.n;
+// lists of the particles of brick B (2 x 2 x d.bz sub-cells), one lane per
+// particle in rounds of 32: every lane tests the same candidate (a shared-memory
+// broadcast) from the union of the brick's sub-cells' 5 x 5 x 5 neighbourhoods,
+// rows of up to 6 sub-cells contiguous in sub-cell order.  Where the union is
+// wider than the box (5 sub-cells per side) a sub-cell comes under two image
+// shifts, of which at most one can be in range (L > 2 x the list cut).
+__device__ __forceinline__ void box_list_brick(const View &v, const SysDesc &d, int r, const float4 *xs,
+                                               const int *sst, int B, int lane) {
+  const int m = d.msub, bz = d.bz, n = d.n;
+  const int nbx = (m + 1) >> 1;
+  const int Bx = B % nbx, By = (B / nbx) % nbx, Bz = B / (nbx * nbx);
+  const int x0 = 2 * Bx, x1 = min(x0 + 2, m), y0 = 2 * By, y1 = min(y0 + 2, m), z0 = bz * Bz,
+            z1 = min(z0 + bz, m);
   const double iL2 = 1.0 / (d.L * d.L);
   float lc[3];
   for (int k = 0; k < 3; k++) lc[k] = (float)(lcut2_of(d, k) * iL2 * (1.0 + 1e-5));
-  uint16_t *lst = box_list(v, d);
+  uint2 *lst = reinterpret_cast<uint2 *>(box_list(v, d));
   const int maxnb = v.maxnb;
-  const int sub = lane & 7, grp = lane >> 3;
-  const int w = w0 + grp;
-  const bool valid = w < sst[S + 1] - sst[S];
-  const int ps = sst[S] + w;
   const float nan = __int_as_float(0x7fc00000);
-  const float4 fi = valid ? xs[ps] : make_float4(nan, nan, nan, __int_as_float(0));
-  const int codei = __float_as_int(fi.w);
-  const int sl = codei & 0x7fff, ti = codei >> 15;
-  const float c0 = ti == 0 ? lc[0] : lc[1], c1 = ti == 0 ? lc[1] : lc[2];
-  const unsigned below = (1u << sub) - 1u;
-  int cnt = 0;
-  // candidates [q0, q1) of the sorted system, eight at a time
-  auto scan = [&](int q0, int q1, float xi, float yi, float zi) {
-    const int iters = (q1 - q0 + 7) >> 3;
-    for (int it = 0, q = q0 + sub; it < iters; it++, q += 8) {
-      const bool live = q < q1;
-      const float4 fj = live ? xs[q] : make_float4(nan, nan, nan, __int_as_float(0));
-      const float ex = xi - fj.x, ey = yi - fj.y, ez = zi - fj.z;
-      const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
-      const int code = __float_as_int(fj.w);
-      const bool ok = valid && live && r2 < ((code >> 15) ? c1 : c0) && q != ps;
-      const unsigned gm = (__ballot_sync(0xffffffffu, ok) >> (8 * grp)) & 255u;
-      if (ok) {
-        const int k = cnt + __popc(gm & below);
-        if (k < maxnb) lst[((size_t)(k >> 2) * n + sl) * 4 + (k & 3)] = (uint16_t)(code & 0xffff);
-      }
-      cnt += __popc(gm);
+  int total = 0;
+  for (int z = z0; z < z1; z++)
+    for (int y = y0; y < y1; y++) {
+      const int row = m * (y + m * z);
+      total += sst[row + x1] - sst[row + x0];
     }
-  };
-  const int a = S % m, b = (S / m) % m, c = S / (m * m);
-  for (int dz = -2; dz <= 2; dz++) {
-    int az = c + dz;
-    const int sz = az < 0 ? -1 : (az >= m ? 1 : 0);
-    az -= sz * m;
-    for (int dy = -2; dy <= 2; dy++) {
-      int ay = b + dy;
-      const int sy = ay < 0 ? -1 : (ay >= m ? 1 : 0);
-      ay -= sy * m;
-      const int row = m * (ay + m * az);
-      // candidate image x_j + s: compare x_i - s with x_j
-      const float yi = fi.y - (float)sy, zi = fi.z - (float)sz;
-      int xa = a - 2;
-      const int xb = a + 3;
-      if (xa < 0) {
-        scan(sst[row + m + xa], sst[row + m], fi.x + 1.0f, yi, zi);
-        xa = 0;
+  for (int k0 = 0; k0 < total; k0 += 32) {
+    // this lane's particle: entry k of the brick's runs (z, y) of x0..x1-1
+    int k = k0 + lane, ps = -1;
+    for (int z = z0; z < z1; z++)
+      for (int y = y0; y < y1; y++) {
+        const int row = m * (y + m * z);
+        const int q0 = sst[row + x0], len = sst[row + x1] - q0;
+        if (ps < 0) {
+          if (k < len) ps = q0 + k;
+          else k -= len;
+        }
       }
-      if (xb > m) {
-        scan(sst[row + xa], sst[row + m], fi.x, yi, zi);
-        scan(sst[row], sst[row + xb - m], fi.x - 1.0f, yi, zi);
+    const bool valid = ps >= 0;
+    // a lane past the brick's particles gets NaN coordinates: it passes no test
+    const float4 fi = valid ? xs[ps] : make_float4(nan, nan, nan, __int_as_float(0));
+    const int codei = __float_as_int(fi.w);
+    const int sl = codei & 0x7fff, ti = codei >> 15;
+    const float c0 = ti == 0 ? lc[0] : lc[1], c1 = ti == 0 ? lc[1] : lc[2];
+    ListWriter lw;
+    auto run = [&](int q0, int q1, float xi, float yi, float zi) {
+      for (int q = q0; q < q1; q += 4) {
+        int code[4];
+        bool ok[4];
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          const int qe = q + e;
+          const float4 fj = qe < q1 ? xs[qe] : make_float4(nan, nan, nan, __int_as_float(0));
+          const float ex = xi - fj.x, ey = yi - fj.y, ez = zi - fj.z;
+          const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+          code[e] = __float_as_int(fj.w);
+          ok[e] = r2 < ((code[e] >> 15) ? c1 : c0) && qe != ps;
+        }
+#pragma unroll
+        for (int e = 0; e < 4; e++)
+          if (ok[e]) lw.add((unsigned)code[e] & 0xffffu, lst, n, sl, maxnb);
+      }
+    };
+    for (int zz = z0 - 2; zz < z1 + 2; zz++) {
+      const int sz = zz < 0 ? -1 : (zz >= m ? 1 : 0), az = zz - sz * m;
+      for (int yy = y0 - 2; yy < y1 + 2; yy++) {
+        const int sy = yy < 0 ? -1 : (yy >= m ? 1 : 0), ay = yy - sy * m;
+        const int row = m * (ay + m * az);
+        // candidate image x_j + s: compare x_i - s with x_j
+        const float yi = fi.y - (float)sy, zi = fi.z - (float)sz;
+        int xa = x0 - 2;
+        const int xb = x1 + 2;
+        if (xa < 0) {
+          run(sst[row + m + xa], sst[row + m], fi.x + 1.0f, yi, zi);
+          xa = 0;
+        }
+        if (xb > m) {
+          run(sst[row + xa], sst[row + m], fi.x, yi, zi);
+          run(sst[row], sst[row + xb - m], fi.x - 1.0f, yi, zi);
+        } else {
+          run(sst[row + xa], sst[row + xb], fi.x, yi, zi);
+        }
+      }
+    }
+    if (valid) {
+      lw.finish(lst, n, sl, maxnb);
+      const int i = d.poff + sl;
+      if (lw.n > maxnb) {
+        v.nbn[i] = -1;
+        atomicAdd(&v.st[r].overflow, 1);
       } else {
-        scan(sst[row + xa], sst[row + xb], fi.x, yi, zi);
+        v.nbn[i] = lw.n;
       }
-    }
-  }
-  if (valid && sub == 0) {
-    const int i = d.poff + sl;
-    if (cnt > maxnb) {
-      v.nbn[i] = -1;
-      atomicAdd(&v.st[r].overflow, 1);
-    } else {
-      v.nbn[i] = cnt;
     }
   }
 }
@@ -1843,13 +1864,11 @@ __device__ void box_list_subcells(const View &v, const SysDesc &d, int r, int gp
     xs[q0 + rank] = make_float4((float)p.x, (float)p.y, (float)p.z, __int_as_float(s | ((int)p.w << 15)));
   }
   __syncthreads();
-  const int S0 = (int)((long long)gp * M3 / G), S1 = (int)((long long)(gp + 1) * M3 / G);
-  int item = 0;
-  for (int S = S0; S < S1; S++) {
-    const int groups = (sst[S + 1] - sst[S] + 3) >> 2;
-    for (int g = (warp - item % nw + nw) % nw; g < groups; g += nw) box_list_sub(v, d, r, xs, sst, S, 4 * g, lane);
-    item += groups;
-  }
+  // bricks of 2 x 2 x d.bz sub-cells, one warp each (global warp gw of the
+  // system's G blocks takes bricks gw, gw + W, ...)
+  const int nbx = (m + 1) >> 1, nbz = (m + d.bz - 1) / d.bz, NB = nbx * nbx * nbz;
+  const int W = G * nw;
+  for (int B = gp * nw + warp; B < NB; B += W) box_list_brick(v, d, r, xs, sst, B, lane);
 }
 
 // lists of a whole box, each tile shared by LIST_SPLIT blocks so that a system
