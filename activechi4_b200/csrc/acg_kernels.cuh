@@ -1162,6 +1162,15 @@ struct PairParamsF {
       ge[tj] = 2.0f * e4[tj] * is2[tj];
     }
   }
+  // for separations counted in units of u: 1/sigma^2 u^2 and 8 eps/sigma^2 u,
+  // so forces come out in absolute units and the virial in units of 1/u
+  __device__ __forceinline__ PairParamsF(int ti, float u) : PairParamsF(ti) {
+#pragma unroll
+    for (int tj = 0; tj < 2; tj++) {
+      is2[tj] *= u * u;
+      ge[tj] *= u;
+    }
+  }
 };
 
 // FP32 pair term: U = 4 eps (s^12 - s^6) + C0 + C2 (r/sigma)^2 and its radial
@@ -1946,8 +1955,9 @@ __device__ __forceinline__ PairAcc box_pairs(const View &v, const SysDesc &d, co
       const uint2 *lp = lst + sl;
       uint2 w = lane < nch ? __ldg(lp + (size_t)lane * n) : make_uint2(0u, 0u);
       if (PREC == 1) {
+        // separations in fixed-point units (L / 2^32), folded into the constants
         const int4 qi = sq[sl];
-        const PairParamsF P(qi.w);
+        const PairParamsF P(qi.w, scale);
         PairAccF fa = {0.f, 0.f, 0.f, 0.f, 0.f}, fb = {0.f, 0.f, 0.f, 0.f, 0.f};
         for (int c = lane; c < nch; c += TPP) {
           const uint2 wn = c + TPP < nch ? __ldg(lp + (size_t)(c + TPP) * n) : make_uint2(0u, 0u);
@@ -1957,15 +1967,16 @@ __device__ __forceinline__ PairAcc box_pairs(const View &v, const SysDesc &d, co
             const int code = ((e < 2 ? w.x : w.y) >> (16 * (e & 1))) & 0xffff;
             if (e == 0 || k0 + e < nn) {
               const int4 qj = sq[code & 0x7fff];
-              const float dx = (float)(int)((unsigned)qi.x - (unsigned)qj.x) * scale;
-              const float dy = (float)(int)((unsigned)qi.y - (unsigned)qj.y) * scale;
-              const float dz = (float)(int)((unsigned)qi.z - (unsigned)qj.z) * scale;
+              const float dx = (float)(int)((unsigned)qi.x - (unsigned)qj.x);
+              const float dy = (float)(int)((unsigned)qi.y - (unsigned)qj.y);
+              const float dz = (float)(int)((unsigned)qi.z - (unsigned)qj.z);
               pair_f32(e & 1 ? fb : fa, dx, dy, dz, P, code >> 15);
             }
           }
           flush_chunk(fa, fb, a);
           w = wn;
         }
+        a.vir *= (double)scale;
       } else {
         const double xi = sx[sl], yi = sy[sl], zi = sz[sl];
         const int ti = (int)v.pos[i].w;
