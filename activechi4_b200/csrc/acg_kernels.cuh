@@ -1916,18 +1916,21 @@ __global__ void __launch_bounds__(BLOCK_X) k_build_list_box(View v) {
   for (int sl = cst[ca] + part * blockDim.x + threadIdx.x; sl < cst[cb]; sl += stride) copy_back(v, d.poff + sl);
 }
 
-// the system's current positions staged for the pair loop: FP32 as 32-bit
-// fixed point {x, y, z, type}, FP64 as three arrays of reduced coordinates
+// the system's current positions staged for the pair loop: FP32 as three
+// arrays of 32-bit fixed point (a partner's type comes with its list entry),
+// FP64 as three arrays of reduced coordinates
 template <int PREC>
 __device__ __forceinline__ void box_stage_force(const View &v, const SysDesc &d, unsigned char *xsm) {
   const int n = d.n;
-  int4 *sq = reinterpret_cast<int4 *>(xsm);
+  int *qx = reinterpret_cast<int *>(xsm), *qy = qx + n, *qz = qy + n;
   double *sx = reinterpret_cast<double *>(xsm), *sy = sx + n, *sz = sy + n;
   for (int k = threadIdx.x; k < n; k += blockDim.x) {
     const double4 p = v.pos[d.poff + k];
-    if (PREC == 1)
-      sq[k] = make_int4(fixed32(p.x), fixed32(p.y), fixed32(p.z), (int)p.w);
-    else {
+    if (PREC == 1) {
+      qx[k] = fixed32(p.x);
+      qy[k] = fixed32(p.y);
+      qz[k] = fixed32(p.z);
+    } else {
       sx[k] = p.x;
       sy[k] = p.y;
       sz[k] = p.z;
@@ -1942,7 +1945,7 @@ template <int TPP, int PREC>
 __device__ __forceinline__ PairAcc box_pairs(const View &v, const SysDesc &d, const unsigned char *xsm, bool valid,
                                              int sl, int i, int lane) {
   const int n = d.n;
-  const int4 *sq = reinterpret_cast<const int4 *>(xsm);
+  const int *qx = reinterpret_cast<const int *>(xsm), *qy = qx + n, *qz = qy + n;
   const double *sx = reinterpret_cast<const double *>(xsm), *sy = sx + n, *sz = sy + n;
   const uint2 *lst = reinterpret_cast<const uint2 *>(box_list(v, d));
   const double L = d.L;
@@ -1956,8 +1959,8 @@ __device__ __forceinline__ PairAcc box_pairs(const View &v, const SysDesc &d, co
       uint2 w = lane < nch ? __ldg(lp + (size_t)lane * n) : make_uint2(0u, 0u);
       if (PREC == 1) {
         // separations in fixed-point units (L / 2^32), folded into the constants
-        const int4 qi = sq[sl];
-        const PairParamsF P(qi.w, scale);
+        const unsigned xi = qx[sl], yi = qy[sl], zi = qz[sl];
+        const PairParamsF P((int)v.pos[i].w, scale);
         PairAccF fa = {0.f, 0.f, 0.f, 0.f, 0.f}, fb = {0.f, 0.f, 0.f, 0.f, 0.f};
         for (int c = lane; c < nch; c += TPP) {
           const uint2 wn = c + TPP < nch ? __ldg(lp + (size_t)(c + TPP) * n) : make_uint2(0u, 0u);
@@ -1966,10 +1969,10 @@ __device__ __forceinline__ PairAcc box_pairs(const View &v, const SysDesc &d, co
           for (int e = 0; e < 4; e++) {
             const int code = ((e < 2 ? w.x : w.y) >> (16 * (e & 1))) & 0xffff;
             if (e == 0 || k0 + e < nn) {
-              const int4 qj = sq[code & 0x7fff];
-              const float dx = (float)(int)((unsigned)qi.x - (unsigned)qj.x);
-              const float dy = (float)(int)((unsigned)qi.y - (unsigned)qj.y);
-              const float dz = (float)(int)((unsigned)qi.z - (unsigned)qj.z);
+              const int j = code & 0x7fff;
+              const float dx = (float)(int)(xi - (unsigned)qx[j]);
+              const float dy = (float)(int)(yi - (unsigned)qy[j]);
+              const float dz = (float)(int)(zi - (unsigned)qz[j]);
               pair_f32(e & 1 ? fb : fa, dx, dy, dz, P, code >> 15);
             }
           }
