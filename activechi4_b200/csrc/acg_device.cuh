@@ -34,7 +34,8 @@ constexpr int BLOCK_G = 256;      // threads of the group kernels
 constexpr int MAX_UNION = 64;     // 4 x 4 x 4 union cells of a 2 x 2 x 2 group
 constexpr int BLOCK_X = 256;      // threads of the whole-box kernels
 constexpr int BOX_CELLS = 8;      // most cells per whole-box block
-constexpr int LIST_SPLIT = 2;     // blocks sharing a whole-box tile in the list build
+constexpr int LIST_SPLIT = 4;     // blocks sharing a whole-box tile in the list build
+constexpr int BLOCK_SORT = 512;    // threads of the per-system sub-cell sort
 constexpr int MAX_BOX_NC = 4;     // whole-box mode for 2..4 cells per side
 constexpr int MAX_BOX_CELLS = MAX_BOX_NC * MAX_BOX_NC * MAX_BOX_NC;
 constexpr int MAX_BOX_N = 8192;   // whole-box staging limit (FP64: 192 KB of shared memory)
@@ -70,7 +71,7 @@ struct SysDesc {
   int tile0_b, ntile_b, tau_p, thermostat;
   int shuffle, list_mode, precision, goff;  // goff: offset of the system's groups
   int tile0_a, ntile_a, box, xoff;            // kick/drift tiles; box: whole-box kernels (2..4 cells per side), xoff: first box tile
-  int cpb, msub, bz, pad6;                    // cpb: cells per whole-box block; msub: list sub-cells per side, bz: their list bricks' depth
+  int cpb, msub, bz, soff;                    // cpb: cells per whole-box block; msub: list sub-cells per side, bz: their list bricks' depth, soff: first sub-cell start
   double L, invL, inv_cell;  // inv_cell: cells per unit reduced length (InvCellSize)
   double T, f0, dt, half_dt, skin2, rebuild_factor, dof;
   double q[NHC_M];
@@ -124,6 +125,8 @@ struct View {
   double *ux_s, *uy_s, *uz_s, *vx_s, *vy_s, *vz_s, *fx_s, *fy_s, *fz_s;
   int *id_s, *act_s;
   int *cell_tmp, *perm_u, *perm;
+  float4 *xsub;     // whole-box systems with list sub-cells: the system in sub-cell order {x, y, z, list code}
+  int *ssub;        // their sub-cell starts [msub^3 + 1] per system
   int *ccount_b, *cfill, *cstart, *ccount;
   const int2 *tiles_a, *tiles_b, *tiles_l, *tiles_c, *tiles_g, *tiles_x;
   int *gstart;      // per group: first centre particle (prefix over the system's groups)

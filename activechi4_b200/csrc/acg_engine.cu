@@ -39,6 +39,7 @@ struct Layout {
   int nsys = 0, nslots = 0, ncells = 0, nact = 0, maxnb = 0, ngroups = 0, nboxtiles = 0, box_nmax = 0;
   int box_m3max = 0;  // most list sub-cells of a whole-box system (0: none uses them)
   int box_cell_nmax = 0;  // most particles of a whole-box system listed from its cells
+  int nsub = 0;           // sub-cell starts of all whole-box systems with list sub-cells
   std::vector<SysDesc> desc;
   size_t bytes = 0;
 };
@@ -128,6 +129,8 @@ int plan(const acg_params *params, int nsys, Layout &lay, int nsm) {
         const double hs = d.L / m;
         d.bz = 8.0 * hs * hs * hs * d.n / (d.L * d.L * d.L) > 28.0 ? 1 : 2;
         lay.box_m3max = std::max(lay.box_m3max, m * m * m);
+        d.soff = lay.nsub;
+        lay.nsub += m * m * m + 1;
       }
       if (!d.msub) lay.box_cell_nmax = std::max(lay.box_cell_nmax, d.n);
     }
@@ -188,6 +191,8 @@ int plan(const acg_params *params, int nsys, Layout &lay, int nsm) {
   add(72 * S);                            // stage_d
   add(8 * S);                             // stage_i
   add(24 * S);                            // stage_f
+  add(16 * S);                            // xsub
+  add(4 * ((size_t)lay.nsub + 1));        // ssub
   lay.bytes = b;
   return ACG_OK;
 }
@@ -265,14 +270,11 @@ GroupFn box_fn(int gtpp, int prec) {
 // whole-box staging: int4 fixed point (FP32) or three doubles (FP64) per particle
 size_t box_smem(int nmax, int prec) { return (size_t)nmax * 3 * (prec ? sizeof(int) : sizeof(double)); }
 // whole-box list build: the staged system padded per cell (cell path, also the
-// fused kernel's) or, for the sub-cell path, the system in sub-cell order, two
-// 16-bit arrays of n and the sub-cell starts and fill counters
+// fused kernel's); the sub-cell path reads the sorted system from memory.  The
+// sub-cell sort: two 16-bit arrays of n and the sub-cell starts and counters.
 size_t box_list_smem_cells(int nmax) { return ((size_t)nmax + 3 * MAX_BOX_CELLS) * sizeof(float4); }
-size_t box_list_smem(int nmax, int m3max, int cell_nmax) {
-  const size_t sub = m3max > 0 ? (size_t)nmax * (sizeof(float4) + 2 * sizeof(uint16_t)) + (2 * (size_t)m3max + 1) * sizeof(int) : 0;
-  return std::max(cell_nmax > 0 ? box_list_smem_cells(cell_nmax) : 0, sub);
-}
-
+size_t box_list_smem(int cell_nmax) { return cell_nmax > 0 ? box_list_smem_cells(cell_nmax) : 0; }
+size_t sort_sub_smem(int nmax, int m3max) { return (size_t)nmax * 2 * sizeof(uint16_t) + (2 * (size_t)m3max + 1) * sizeof(int); }
 using StepFn = void (*)(View, int);
 StepFn steps_fn(int gtpp, int prec) {
   switch (gtpp) {
@@ -415,8 +417,9 @@ int launch_rebuild(acg_engine *e) {
   k_cells_scatter<<<e->ntiles_a, BLOCK_R, 0, s>>>(v);
   k_cells_order<<<e->ntiles_c, 32 * CELLS_PER_TILE, 0, s>>>(v);
   k_permute<<<e->ntiles_a, BLOCK_R, 0, s>>>(v);
+  if (e->lay.box_m3max) k_sort_sub<<<e->lay.nsys, BLOCK_SORT, sort_sub_smem(e->lay.box_nmax, e->lay.box_m3max), s>>>(v);
   if (e->ntiles_g) k_build_list_groups<<<e->ntiles_g, BLOCK_G, list_smem(v.gcap), s>>>(v);
-  if (e->ntiles_x) k_build_list_box<<<e->ntiles_x * LIST_SPLIT, BLOCK_X, box_list_smem(e->lay.box_nmax, e->lay.box_m3max, e->lay.box_cell_nmax), s>>>(v);
+  if (e->ntiles_x) k_build_list_box<<<e->ntiles_x * LIST_SPLIT, BLOCK_X, box_list_smem(e->lay.box_cell_nmax), s>>>(v);
   if (e->ntiles_l) k_build_list<<<e->ntiles_l, BLOCK_L, 0, s>>>(v);
   CK(cudaGetLastError());
   return ACG_OK;
@@ -519,8 +522,10 @@ int add_steps(acg_engine *e, cudaGraph_t g, int K, cudaGraphNode_t *prev_io) {
               {(void *)k_cells_scatter, e->ntiles_a, BLOCK_R, 0},
               {(void *)k_cells_order, e->ntiles_c, 32 * CELLS_PER_TILE, 0},
               {(void *)k_permute, e->ntiles_a, BLOCK_R, 0},
+              {(void *)k_sort_sub, e->lay.box_m3max ? e->lay.nsys : 0, BLOCK_SORT,
+               sort_sub_smem(e->lay.box_nmax, e->lay.box_m3max)},
               {(void *)k_build_list_groups, e->ntiles_g, BLOCK_G, list_smem(v.gcap)},
-              {(void *)k_build_list_box, e->ntiles_x * LIST_SPLIT, BLOCK_X, box_list_smem(e->lay.box_nmax, e->lay.box_m3max, e->lay.box_cell_nmax)},
+              {(void *)k_build_list_box, e->ntiles_x * LIST_SPLIT, BLOCK_X, box_list_smem(e->lay.box_cell_nmax)},
               {(void *)k_build_list, e->ntiles_l, BLOCK_L, 0}};
     cudaGraphNode_t bp = nullptr;
     for (auto &k : rb) {
@@ -793,6 +798,8 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   v.stage_d = (double *)take(72 * S);
   v.stage_i = (int *)take(8 * S);
   v.stage_f = (double *)take(24 * S);
+  v.xsub = (float4 *)take(16 * S);
+  v.ssub = (int *)take(4 * ((size_t)L.nsub + 1));
   v.tiles_a = ta;
   v.tiles_b = e->d_tiles_b;
   v.tiles_l = tl;
@@ -866,13 +873,14 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
     for (int pr : {0, 1}) attr_ok = attr_ok && raise_smem((const void *)group_fn(gt, pr), group_smem(v.gcap));
   attr_ok = attr_ok && raise_smem((const void *)k_build_list_groups, list_smem(v.gcap));
   if (L.box_nmax > 0) {
-    if (box_list_smem(L.box_nmax, L.box_m3max, L.box_cell_nmax) > 227 * 1024 || box_smem(L.box_nmax, 0) > 227 * 1024) {
+    if (box_list_smem(L.box_cell_nmax) > 227 * 1024 || box_smem(L.box_nmax, 0) > 227 * 1024) {
       acg_destroy(e);
       return fail(ACG_ERR_INVALID, "whole-box system too large for shared memory");
     }
     for (int gt : {1, 2, 4})
       for (int pr : {0, 1}) attr_ok = attr_ok && raise_smem((const void *)box_fn(gt, pr), box_smem(L.box_nmax, pr));
-    attr_ok = attr_ok && raise_smem((const void *)k_build_list_box, box_list_smem(L.box_nmax, L.box_m3max, L.box_cell_nmax));
+    attr_ok = attr_ok && raise_smem((const void *)k_build_list_box, box_list_smem(L.box_cell_nmax));
+    attr_ok = attr_ok && raise_smem((const void *)k_sort_sub, sort_sub_smem(L.box_nmax, L.box_m3max));
     for (int gt : {1, 2, 4})
       for (int pr : {0, 1}) attr_ok = attr_ok && raise_smem((const void *)steps_fn(gt, pr), steps_smem(L.box_nmax, pr));
   }

@@ -1710,15 +1710,15 @@ __device__ __forceinline__ void box_list_group(const View &v, const SysDesc &d, 
 // edge is two runs with their image shifts) -- about a quarter of the volume of
 // the 27 reference cells of a small box.
 //
-// Each block sorts the system into sub-cell order in shared memory (a counting
-// sort; members of a sub-cell in slot order, so the order does not depend on
-// the atomics), then its warps take bricks of 2 x 2 x d.bz sub-cells, one lane
-// per particle, and scan the union of the brick's neighbourhoods.
+// k_sort_sub puts each rebuilding system in sub-cell order (in memory); the
+// warps of the list blocks take bricks of 2 x 2 x d.bz sub-cells, one lane per
+// particle, and scan the union of the brick's neighbourhoods.
 __device__ __forceinline__ int subcell_of(double x, int m) { return min(max((int)(x * (double)m), 0), m - 1); }
 
 // lists of the particles of brick B (2 x 2 x d.bz sub-cells), one lane per
-// particle in rounds of 32: every lane tests the same candidate (a shared-memory
-// broadcast) from the union of the brick's sub-cells' 5 x 5 x 5 neighbourhoods,
+// particle in rounds of 32: every lane tests the same candidate (a broadcast
+// load of the sorted system) from the union of the brick's sub-cells' 5 x 5 x 5
+// neighbourhoods,
 // rows of up to 6 sub-cells contiguous in sub-cell order.  Where the union is
 // wider than the box (5 sub-cells per side) a sub-cell comes under two image
 // shifts, of which at most one can be in range (L > 2 x the list cut).
@@ -1767,7 +1767,7 @@ __device__ __forceinline__ void box_list_brick(const View &v, const SysDesc &d, 
 #pragma unroll
         for (int e = 0; e < 4; e++) {
           const int qe = q + e;
-          const float4 fj = qe < q1 ? xs[qe] : make_float4(nan, nan, nan, __int_as_float(0));
+          const float4 fj = qe < q1 ? __ldg(xs + qe) : make_float4(nan, nan, nan, __int_as_float(0));
           const float ex = xi - fj.x, ey = yi - fj.y, ez = zi - fj.z;
           const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
           code[e] = __float_as_int(fj.w);
@@ -1812,17 +1812,25 @@ __device__ __forceinline__ void box_list_brick(const View &v, const SysDesc &d, 
   }
 }
 
-// block gp of G: sort the system into sub-cell order, then the lists of the
-// centre sub-cells [gp M3 / G, (gp + 1) M3 / G)
-__device__ void box_list_subcells(const View &v, const SysDesc &d, int r, int gp, int G, unsigned char *smem) {
+// one block per whole-box system with list sub-cells (rebuilding systems
+// only): the system in sub-cell order into xsub (reduced x, y, z as float, the
+// list code slot | type << 15) with the sub-cell starts in ssub.  A counting
+// sort in shared memory; members of a sub-cell end in slot order, so the order
+// does not depend on the atomics.
+__global__ void __launch_bounds__(BLOCK_SORT) k_sort_sub(View v) {
+  extern __shared__ int ssm[];
+  const int r = blockIdx.x;
+  if (!v.st[r].rebuild) return;
+  const SysDesc &d = v.desc[r];
+  if (!d.box || d.msub < 5) return;
   const int n = d.n, m = d.msub, M3 = m * m * m;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  float4 *xs = reinterpret_cast<float4 *>(smem);
-  uint16_t *key = reinterpret_cast<uint16_t *>(xs + n);  // sub-cell of slot s
-  uint16_t *ord = key + n;                               // slot at sorted position (unordered in a sub-cell)
-  int *sst = reinterpret_cast<int *>(ord + n);           // [M3 + 1] sub-cell starts
-  int *fill = sst + M3 + 1;                              // [M3]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int *fill = ssm;                                             // [M3]
+  int *sst = fill + M3;                                        // [M3 + 1]
+  uint16_t *key = reinterpret_cast<uint16_t *>(sst + M3 + 1);  // sub-cell of slot s
+  uint16_t *ord = key + n;                                     // slot at sorted position (unordered in a sub-cell)
   const double4 *pp = v.pos_s + d.poff;
+  float4 *xs = v.xsub + d.poff;
   for (int k = threadIdx.x; k < M3; k += blockDim.x) fill[k] = 0;
   __syncthreads();
   for (int s = threadIdx.x; s < n; s += blockDim.x) {
@@ -1872,12 +1880,8 @@ __device__ void box_list_subcells(const View &v, const SysDesc &d, int r, int gp
     const double4 p = pp[s];
     xs[q0 + rank] = make_float4((float)p.x, (float)p.y, (float)p.z, __int_as_float(s | ((int)p.w << 15)));
   }
-  __syncthreads();
-  // bricks of 2 x 2 x d.bz sub-cells, one warp each (global warp gw of the
-  // system's G blocks takes bricks gw, gw + W, ...)
-  const int nbx = (m + 1) >> 1, nbz = (m + d.bz - 1) / d.bz, NB = nbx * nbx * nbz;
-  const int W = G * nw;
-  for (int B = gp * nw + warp; B < NB; B += W) box_list_brick(v, d, r, xs, sst, B, lane);
+  int *gst = v.ssub + d.soff;
+  for (int k = threadIdx.x; k <= M3; k += blockDim.x) gst[k] = sst[k];
 }
 
 // lists of a whole box, each tile shared by LIST_SPLIT blocks so that a system
@@ -1898,7 +1902,12 @@ __global__ void __launch_bounds__(BLOCK_X) k_build_list_box(View v) {
   const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int ca = b * d.cpb, cb = min(nce, ca + d.cpb);
   if (d.msub >= 5) {
-    box_list_subcells(v, d, r, b * LIST_SPLIT + part, d.ntile_b * LIST_SPLIT, reinterpret_cast<unsigned char *>(xstg));
+    // bricks of 2 x 2 x d.bz sub-cells, one warp each: warp gw of the system's
+    // G blocks takes bricks gw, gw + W, ... of the sorted system
+    const int m = d.msub, nbx = (m + 1) >> 1, nbz = (m + d.bz - 1) / d.bz, NB = nbx * nbx * nbz;
+    const int W = d.ntile_b * LIST_SPLIT * nw;
+    for (int B = (b * LIST_SPLIT + part) * nw + (threadIdx.x >> 5); B < NB; B += W)
+      box_list_brick(v, d, r, v.xsub + d.poff, v.ssub + d.soff, B, lane);
   } else {
     const int W = LIST_SPLIT * nw, gw = part * nw + (threadIdx.x >> 5);
     box_stage_list(v, d, xstg, cst, pre4);
