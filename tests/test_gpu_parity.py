@@ -210,3 +210,35 @@ def test_reused_step_graph_matches_eager(cuda_lib, g1000):
     for u, w in zip(b.get_state(), c.get_state()):
         assert np.array_equal(u, w)
     assert b.thermo()["rebuilds"] == c.thermo()["rebuilds"]
+
+
+@pytest.mark.parametrize("n,rho", [(300, 1.2), (600, 1.2), (1500, 1.2), (2500, 1.2), (3400, 1.2), (380, 0.9),
+                                   (1800, 0.8)])
+def test_whole_box_list_paths(cuda_lib, n, rho):
+    """Whole-box systems of every list geometry against the oracle: 2 cells per
+    side with fewer than 5 list sub-cells (minimum-image pass, n=300), 5
+    sub-cells per side where a brick's neighbourhood is wider than the box
+    (n=600; at rho=0.9, n=380, on all three axes), 3 and 4 cells per side with
+    7 to 9 sub-cells, bricks of depth 1 (rho=1.2) and 2 (rho=0.8, n=1800).
+    FP64 forces, pe and virial <= 1e-12 (both list cuts); FP32 pair forces
+    <= 1e-5."""
+    from activechi4_b200 import Engine, default_params, lattice_state
+    from oracle import Oracle
+    st = lattice_state(n, 1.0, seed=100 + n, density=rho)
+    o = Oracle.from_state(st, 1.0, 2.0, p_eta=np.array([0.1, 0.2, 0.3]))
+    o.run(40)  # melt the lattice a little on the CPU
+    x, xu, p, _ = o.get_state()
+    st.x, st.xu, st.p = x, xu, p
+    for list_mode in (0, 1):
+        Fo, pe, vir, _ = Oracle.from_state(st, 1.0, 2.0, list_mode=list_mode).forces()
+        for prec, tol in ((0, 1e-12), (1, 1e-5)):
+            e = Engine(default_params(n, T=1.0, f0=2.0, shuffle=0, list_mode=list_mode, precision=prec,
+                                      density=rho))
+            e.set_state(0, st)
+            e.compute_forces()
+            assert e.thermo()["overflow"] == 0
+            err = force_err(e.get_state()[3], Fo)
+            assert err <= tol, (n, list_mode, prec, err)
+            th = e.thermo()
+            assert rel(th["pe"], pe) <= tol and rel(th["virial"], vir) <= tol, (n, list_mode, prec)
+            e.close()
