@@ -1,8 +1,9 @@
-"""The oracle: CPU checkers for the CUDA timestep.  TEST INFRASTRUCTURE ONLY.
+"""The oracle: CPU restatements to check the CUDA timestep against.  TEST
+INFRASTRUCTURE ONLY.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
-``bench.py`` may import this package, and only as the checker (or the timed
-CPU baseline), never as the thing measured or shipped.
+``bench.py`` may import this package, and only to check results against (or as
+the timed CPU baseline), never as the thing measured or shipped.
 
 * ``Oracle``    — the project's own C restatement of the reference timestep
                   (``acg_oracle.c``), built to ``oracle/_build/libacg_oracle.so``.

@@ -1,7 +1,7 @@
 /*
  * acg_oracle — CPU restatement of the reference's MD timestep.
- * TEST INFRASTRUCTURE ONLY (see acg_oracle.h): the checker for the CUDA path,
- * never part of it.
+ * TEST INFRASTRUCTURE ONLY (see acg_oracle.h): the CUDA path is checked
+ * against it; never part of it.
  *
  * Each routine cites the reference lines it restates.  Loop orders, the
  * order of floating-point operations and the neighbour-list construction

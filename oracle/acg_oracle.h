@@ -1,7 +1,8 @@
 /*
  * acg_oracle — CPU restatement of the reference's MD timestep.
  * TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
- * bench.py's CPU-baseline leg as the checker; never linked into the product.
+ * bench.py's CPU-baseline leg, to check results against; never linked into
+ * the product.
  *
  * One FP64 system at a time, single process, following the reference's
  * operation order so that, for boxes with at least 3 cells per dimension, the

@@ -1,5 +1,5 @@
 """numpy restatement of the reference's trajectory analysis.  TEST
-INFRASTRUCTURE ONLY: the checker for the device's in-place observables.
+INFRASTRUCTURE ONLY: the device's in-place observables are checked against it.
 
 * log_pairs — the (origin, later step, time bin) pairs that Analysis/overlap.c
   and Analysis/msd_pos.c visit: origins every run/num_origins steps

@@ -1,5 +1,5 @@
 /*
- * Reference harness — TEST INFRASTRUCTURE ONLY (the checker, never the product).
+ * Reference harness — TEST INFRASTRUCTURE ONLY (results are checked against it; never the product).
  *
  * This file is compiled together with the reference MD engine's own sources
  * (MDcode/*.c, built in place by oracle/Makefile with a single-rank MPI shim
