@@ -36,6 +36,7 @@ constexpr int BLOCK_X = 256;      // threads of the whole-box kernels
 constexpr int BOX_CELLS = 8;      // most cells per whole-box block
 constexpr int LIST_SPLIT = 4;     // blocks sharing a whole-box tile in the list build
 constexpr int BLOCK_SORT = 512;    // threads of the per-system sub-cell sort
+constexpr int BLOCK_COMPACT = 1024; // threads of the rebuild-list compaction (one block)
 constexpr int MAX_BOX_NC = 4;     // whole-box mode for 2..4 cells per side
 constexpr int MAX_BOX_CELLS = MAX_BOX_NC * MAX_BOX_NC * MAX_BOX_NC;
 constexpr int MAX_BOX_N = 8192;   // whole-box staging limit (FP64: 192 KB of shared memory)
@@ -127,6 +128,7 @@ struct View {
   int *cell_tmp, *perm_u, *perm;
   float4 *xsub;     // whole-box systems with list sub-cells: the system in sub-cell order {x, y, z, list code}
   int *ssub;        // their sub-cell starts [msub^3 + 1] per system
+  int *rbs;         // this step's rebuilding systems with list sub-cells: count, bricks, then (system, first brick)
   int *ccount_b, *cfill, *cstart, *ccount;
   const int2 *tiles_a, *tiles_b, *tiles_l, *tiles_c, *tiles_g, *tiles_x;
   int *gstart;      // per group: first centre particle (prefix over the system's groups)

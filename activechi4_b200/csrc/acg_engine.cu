@@ -193,6 +193,7 @@ int plan(const acg_params *params, int nsys, Layout &lay, int nsm) {
   add(24 * S);                            // stage_f
   add(16 * S);                            // xsub
   add(4 * ((size_t)lay.nsub + 1));        // ssub
+  add(4 * (2 * (size_t)nsys + 2));        // rbs
   lay.bytes = b;
   return ACG_OK;
 }
@@ -418,6 +419,8 @@ int launch_rebuild(acg_engine *e) {
   k_cells_order<<<e->ntiles_c, 32 * CELLS_PER_TILE, 0, s>>>(v);
   k_permute<<<e->ntiles_a, BLOCK_R, 0, s>>>(v);
   if (e->lay.box_m3max) k_sort_sub<<<e->lay.nsys, BLOCK_SORT, sort_sub_smem(e->lay.box_nmax, e->lay.box_m3max), s>>>(v);
+  // the list build reads the compacted rebuild list whenever it runs
+  if (e->ntiles_x) k_rebuild_compact<<<1, BLOCK_COMPACT, 0, s>>>(v);
   if (e->ntiles_g) k_build_list_groups<<<e->ntiles_g, BLOCK_G, list_smem(v.gcap), s>>>(v);
   if (e->ntiles_x) k_build_list_box<<<e->ntiles_x * LIST_SPLIT, BLOCK_X, box_list_smem(e->lay.box_cell_nmax), s>>>(v);
   if (e->ntiles_l) k_build_list<<<e->ntiles_l, BLOCK_L, 0, s>>>(v);
@@ -524,6 +527,7 @@ int add_steps(acg_engine *e, cudaGraph_t g, int K, cudaGraphNode_t *prev_io) {
               {(void *)k_permute, e->ntiles_a, BLOCK_R, 0},
               {(void *)k_sort_sub, e->lay.box_m3max ? e->lay.nsys : 0, BLOCK_SORT,
                sort_sub_smem(e->lay.box_nmax, e->lay.box_m3max)},
+              {(void *)k_rebuild_compact, e->ntiles_x ? 1 : 0, BLOCK_COMPACT, 0},
               {(void *)k_build_list_groups, e->ntiles_g, BLOCK_G, list_smem(v.gcap)},
               {(void *)k_build_list_box, e->ntiles_x * LIST_SPLIT, BLOCK_X, box_list_smem(e->lay.box_cell_nmax)},
               {(void *)k_build_list, e->ntiles_l, BLOCK_L, 0}};
@@ -800,6 +804,7 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   v.stage_f = (double *)take(24 * S);
   v.xsub = (float4 *)take(16 * S);
   v.ssub = (int *)take(4 * ((size_t)L.nsub + 1));
+  v.rbs = (int *)take(4 * (2 * (size_t)nsys + 2));
   v.tiles_a = ta;
   v.tiles_b = e->d_tiles_b;
   v.tiles_l = tl;

@@ -1884,45 +1884,121 @@ __global__ void __launch_bounds__(BLOCK_SORT) k_sort_sub(View v) {
   for (int k = threadIdx.x; k <= M3; k += blockDim.x) gst[k] = sst[k];
 }
 
-// lists of a whole box, each tile shared by LIST_SPLIT blocks so that a system
-// that rebuilds while others do not still spreads over many SMs: with list
-// sub-cells, the system's centre sub-cells are split over its tiles' blocks;
-// otherwise the work items (cell, 8 particles) of the tile go round the
-// LIST_SPLIT x 8 warps.  Every block stages the system once.
+// list bricks of a whole-box system with list sub-cells
+__device__ __forceinline__ int bricks_of(const SysDesc &d) {
+  const int nbx = (d.msub + 1) >> 1;
+  return nbx * nbx * ((d.msub + d.bz - 1) / d.bz);
+}
+
+// one block: the whole-box systems with list sub-cells that rebuild this step,
+// in system order, with the running count of their bricks, so the list build
+// can spread all their bricks evenly over its warps: rbs[0] systems, rbs[1]
+// bricks, then (system, first brick) pairs
+__global__ void __launch_bounds__(BLOCK_COMPACT) k_rebuild_compact(View v) {
+  __shared__ int wk[32], wb[32];
+  __shared__ int base_k, base_b;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (threadIdx.x == 0) base_k = base_b = 0;
+  __syncthreads();
+  for (int r0 = 0; r0 < v.nsys; r0 += blockDim.x) {
+    const int r = r0 + threadIdx.x;
+    int f = 0, nb = 0;
+    if (r < v.nsys) {
+      const SysDesc &d = v.desc[r];
+      if (v.st[r].rebuild && d.box && d.msub >= 5) {
+        f = 1;
+        nb = bricks_of(d);
+      }
+    }
+    // block-wide exclusive scans of the flags and brick counts
+    int kf = f, kb = nb;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, kf, o), z = __shfl_up_sync(0xffffffffu, kb, o);
+      if (lane >= o) {
+        kf += y;
+        kb += z;
+      }
+    }
+    if (lane == 31) {
+      wk[warp] = kf;
+      wb[warp] = kb;
+    }
+    __syncthreads();
+    int bk = base_k, bb = base_b;
+    for (int w = 0; w < warp; w++) {
+      bk += wk[w];
+      bb += wb[w];
+    }
+    if (f) {
+      const int k = bk + kf - 1;
+      v.rbs[2 + 2 * k] = r;
+      v.rbs[3 + 2 * k] = bb + kb - nb;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int w = 0; w < nw; w++) {
+        base_k += wk[w];
+        base_b += wb[w];
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    v.rbs[0] = base_k;
+    v.rbs[1] = base_b;
+  }
+}
+
+// lists of whole boxes, each tile shared by LIST_SPLIT blocks: the bricks of
+// all systems with list sub-cells that rebuild go round all warps of the grid
+// (k_rebuild_compact lists them), so the few systems that rebuild in a step
+// spread evenly over the SMs; a system without list sub-cells has the work
+// items (cell, 8 particles) of each tile go round the tile's LIST_SPLIT x 8
+// warps, each block staging the system once.
 __global__ void __launch_bounds__(BLOCK_X) k_build_list_box(View v) {
   extern __shared__ float4 xstg[];
   __shared__ int cst[MAX_BOX_CELLS + 1], pre4[MAX_BOX_CELLS + 1];
   const int2 tile = v.tiles_x[blockIdx.x / LIST_SPLIT];
   const int part = blockIdx.x % LIST_SPLIT;
   const int r = tile.x, b = tile.y;
-  if (!v.st[r].rebuild) return;
   const SysDesc &d = v.desc[r];
-  const int nce = d.ncell;
-  box_cells(v, d, cst, pre4);
-  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  const int ca = b * d.cpb, cb = min(nce, ca + d.cpb);
-  if (d.msub >= 5) {
-    // bricks of 2 x 2 x d.bz sub-cells, one warp each: warp gw of the system's
-    // G blocks takes bricks gw, gw + W, ... of the sorted system
-    const int m = d.msub, nbx = (m + 1) >> 1, nbz = (m + d.bz - 1) / d.bz, NB = nbx * nbx * nbz;
-    const int W = d.ntile_b * LIST_SPLIT * nw;
-    for (int B = (b * LIST_SPLIT + part) * nw + (threadIdx.x >> 5); B < NB; B += W)
-      box_list_brick(v, d, r, v.xsub + d.poff, v.ssub + d.soff, B, lane);
-  } else {
-    const int W = LIST_SPLIT * nw, gw = part * nw + (threadIdx.x >> 5);
-    box_stage_list(v, d, xstg, cst, pre4);
-    __syncthreads();
-    int item = 0;
-    for (int c = ca; c < cb; c++) {
-      const int groups = (cst[c + 1] - cst[c] + 7) >> 3;
-      // warp gw takes the cell's groups g with (item + g) % W == gw
-      for (int g = (gw - item % W + W) % W; g < groups; g += W)
-        box_list_group(v, d, r, xstg, cst, pre4, c, 8 * g, lane);
-      item += groups;
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5, warp = threadIdx.x >> 5;
+  if (v.st[r].rebuild) {
+    // the tile's own work: lists of a system without list sub-cells, and the
+    // copy-back of the tile's slots
+    const int nce = d.ncell;
+    box_cells(v, d, cst, pre4);
+    const int ca = b * d.cpb, cb = min(nce, ca + d.cpb);
+    if (d.msub < 5) {
+      const int W = LIST_SPLIT * nw, gw = part * nw + warp;
+      box_stage_list(v, d, xstg, cst, pre4);
+      __syncthreads();
+      int item = 0;
+      for (int c = ca; c < cb; c++) {
+        const int groups = (cst[c + 1] - cst[c] + 7) >> 3;
+        // warp gw takes the cell's groups g with (item + g) % W == gw
+        for (int g = (gw - item % W + W) % W; g < groups; g += W)
+          box_list_group(v, d, r, xstg, cst, pre4, c, 8 * g, lane);
+        item += groups;
+      }
     }
+    const int stride = LIST_SPLIT * blockDim.x;
+    for (int sl = cst[ca] + part * blockDim.x + threadIdx.x; sl < cst[cb]; sl += stride) copy_back(v, d.poff + sl);
   }
-  const int stride = LIST_SPLIT * blockDim.x;
-  for (int sl = cst[ca] + part * blockDim.x + threadIdx.x; sl < cst[cb]; sl += stride) copy_back(v, d.poff + sl);
+  // the bricks of all rebuilding systems with list sub-cells, spread over the
+  // warps of the whole grid: global warp w takes bricks w, w + W, ...
+  const int K = v.rbs[0], T = v.rbs[1], Wg = gridDim.x * nw;
+  for (int it = blockIdx.x * nw + warp; it < T; it += Wg) {
+    int lo = 0, hi = K - 1;  // the last system whose first brick is <= it
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (v.rbs[3 + 2 * mid] <= it) lo = mid;
+      else hi = mid - 1;
+    }
+    const int rs = v.rbs[2 + 2 * lo];
+    const SysDesc &ds = v.desc[rs];
+    box_list_brick(v, ds, rs, v.xsub + ds.poff, v.ssub + ds.soff, it - v.rbs[3 + 2 * lo], lane);
+  }
 }
 
 // the system's current positions staged for the pair loop: FP32 as three
