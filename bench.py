@@ -55,7 +55,7 @@ def parse():
 
 # ---------------------------------------------------------------------------
 # CPU side: the reference (or the oracle restatement) on host cores
-def _cpu_worker(n, seed, seconds, max_steps, kind, barrier, q):
+def _cpu_worker(n, seed, seconds, max_steps, kind, barrier, q, warm=3):
     import numpy as np
 
     from activechi4_b200.init import lattice_state
@@ -71,23 +71,23 @@ def _cpu_worker(n, seed, seconds, max_steps, kind, barrier, q):
         sysm = Oracle.from_state(st, 0.45, 1.0, p_eta=p_eta)
         sysm.seed_rng(seed + 1)
     t0 = time.perf_counter()
-    sysm.run(2, start=0, shuffle=True)  # warm-up and per-step estimate
-    t1 = (time.perf_counter() - t0) / 2
+    sysm.run(warm, start=0, shuffle=True)  # warm-up and per-step estimate
+    t1 = (time.perf_counter() - t0) / warm
     steps = int(max(3, min(max_steps, seconds / max(t1, 1e-9))))
     if barrier is not None:
         barrier.wait()
     t0 = time.perf_counter()
-    sysm.run(steps, start=2, shuffle=True)
+    sysm.run(steps, start=warm, shuffle=True)
     q.put((steps, time.perf_counter() - t0))
 
 
-def cpu_run(n, nproc, seconds, max_steps):
+def cpu_run(n, nproc, seconds, max_steps, warm=3):
     from oracle import reference_available
     kind = "reference" if reference_available(n) else "port"
     ctx = mp.get_context("spawn")  # never fork a process that holds a CUDA context
     q = ctx.Queue()
     bar = ctx.Barrier(nproc) if nproc > 1 else None
-    procs = [ctx.Process(target=_cpu_worker, args=(n, 100 + i, seconds, max_steps, kind, bar, q))
+    procs = [ctx.Process(target=_cpu_worker, args=(n, 100 + i, seconds, max_steps, kind, bar, q, warm))
              for i in range(nproc)]
     for p in procs:
         p.start()
@@ -371,7 +371,7 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        kind, cval, csteps, cwall = cpu_run(n, 1, args.cpu_seconds, 10 ** 6)
+        kind, cval, csteps, cwall = cpu_run(n, 1, args.cpu_seconds, 10 ** 6, 3)
         cpu = {"value": cval, "unit": "particle-steps/s", "cores": 1, "kind": kind,
                "sample": f"{csteps[0]} NVT steps of one N={n} system from a T=0.45 lattice start, "
                          f"single rank, {cwall:.1f} s"}
@@ -422,11 +422,13 @@ def run_reference(args):
         return
     n = args.n
     cores = host_cores()
-    kind, value, steps, wall = cpu_run(n, cores, args.cpu_seconds, max(3, args.steps))
+    # the CPU steps are a bounded sample: at least 3 warm-up steps, at most 5
+    warm = max(3, min(args.warmup, 5))
+    kind, value, steps, wall = cpu_run(n, cores, args.cpu_seconds, max(3, args.steps), warm)
     line = {
         "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "impl": "reference",
         "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": int(min(steps)),
-        "warmup": 2, "ms_per_step": wall * 1e3 / max(1, min(steps)), "higher_is_better": True,
+        "warmup": warm, "ms_per_step": wall * 1e3 / max(1, min(steps)), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic: seeded random lattice at T=0.45",
         "config": {"workload": f"plain KA active glass, N={n} one system per process, rho=1.2, T=0.45, "
