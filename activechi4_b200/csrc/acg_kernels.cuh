@@ -1180,17 +1180,18 @@ __device__ __forceinline__ void pair_f32(PairAccF &a, float dx, float dy, float 
   const float is2 = tj ? P.is2[1] : P.is2[0];
   const float dr2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
   const float rs2 = dr2 * is2;
-  if (rs2 < (float)KA_RC2) {
-    const float e4 = tj ? P.e4[1] : P.e4[0], ge = tj ? P.ge[1] : P.ge[0];
-    const float s2 = rcp_approx(rs2);
-    const float s6 = s2 * s2 * s2;
-    a.pe = fmaf(e4, fmaf(s6, s6, -s6) + fmaf((float)KA_C2, rs2, (float)KA_C0), a.pe);
-    const float g = ge * fmaf(s6 * fmaf(6.0f, s6, -3.0f), s2, -(float)KA_C2);
-    a.fx = fmaf(g, dx, a.fx);
-    a.fy = fmaf(g, dy, a.fy);
-    a.fz = fmaf(g, dz, a.fz);
-    a.vir = fmaf(g, dr2, a.vir);
-  }
+  // evaluated for every entry and masked (no divergent branch): beyond the cut
+  // the factors are zero and each sum gains exactly nothing
+  const bool in = rs2 < (float)KA_RC2;
+  const float e4 = in ? (tj ? P.e4[1] : P.e4[0]) : 0.0f, ge = in ? (tj ? P.ge[1] : P.ge[0]) : 0.0f;
+  const float s2 = rcp_approx(rs2);
+  const float s6 = s2 * s2 * s2;
+  a.pe = fmaf(e4, fmaf(s6, s6, -s6) + fmaf((float)KA_C2, rs2, (float)KA_C0), a.pe);
+  const float g = ge * fmaf(s6 * fmaf(6.0f, s6, -3.0f), s2, -(float)KA_C2);
+  a.fx = fmaf(g, dx, a.fx);
+  a.fy = fmaf(g, dy, a.fy);
+  a.fz = fmaf(g, dz, a.fz);
+  a.vir = fmaf(g, dr2, a.vir);
 }
 
 // pair term on a separation already in the minimum image, absolute units
