@@ -35,7 +35,7 @@ constexpr int MAX_UNION = 64;     // 4 x 4 x 4 union cells of a 2 x 2 x 2 group
 constexpr int BLOCK_X = 256;      // threads of the whole-box kernels
 constexpr int BOX_CELLS = 8;      // most cells per whole-box block
 constexpr int LIST_SPLIT = 4;     // blocks sharing a whole-box tile in the list build
-constexpr int BLOCK_SORT = 512;    // threads of the per-system sub-cell sort
+constexpr int BLOCK_SORT = 1024;   // threads of the per-system sub-cell sort
 constexpr int BLOCK_COMPACT = 1024; // threads of the rebuild-list compaction (one block)
 constexpr int MAX_BOX_NC = 4;     // whole-box mode for 2..4 cells per side
 constexpr int MAX_BOX_CELLS = MAX_BOX_NC * MAX_BOX_NC * MAX_BOX_NC;
