@@ -27,7 +27,7 @@ class acg_params(C.Structure):
         ("T", C.c_double), ("f0", C.c_double), ("tau_p_steps", C.c_int), ("dt", C.c_double),
         ("skin", C.c_double), ("rebuild_factor", C.c_double), ("list_mode", C.c_int),
         ("thermostat", C.c_int), ("shuffle", C.c_int), ("precision", C.c_int),
-        ("nb_capacity", C.c_int), ("seed", C.c_uint64),
+        ("nb_capacity", C.c_int), ("seed", C.c_uint64), ("drift_every", C.c_int),
     ]
 
 
@@ -67,6 +67,12 @@ _SIGS = {
     "acg_set_directions": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "acg_get_directions": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "acg_shuffle_directions": (C.c_int, [C.c_void_p, C.c_int]),
+    "acg_seed_shuffle": (C.c_int, [C.c_void_p, C.c_int, C.c_uint64]),
+    "acg_fix_drift": (C.c_int, [C.c_void_p, C.c_int]),
+    "acg_adjust_temperature": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.POINTER(C.c_double)]),
+    "acg_start_ramp": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_int64)]),
+    "acg_extend_ramp": (C.c_int, [C.c_void_p, C.c_int, C.c_int64]),
+    "acg_set_lattice": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "acg_set_nhc": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "acg_set_temperature": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
     "acg_rebuild": (C.c_int, [C.c_void_p]),

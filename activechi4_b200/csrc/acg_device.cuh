@@ -41,6 +41,10 @@ constexpr int MAX_BOX_NC = 4;     // whole-box mode for 2..4 cells per side
 constexpr int MAX_BOX_CELLS = MAX_BOX_NC * MAX_BOX_NC * MAX_BOX_NC;
 constexpr int MAX_BOX_N = 8192;   // whole-box staging limit (FP64: 192 KB of shared memory)
 constexpr int MAX_SUB3 = 1000;    // list sub-cells of a whole box (side >= 1.45 and L < 15: <= 10^3)
+constexpr int MT_N = 624;         // MT19937 state words
+constexpr int MT_WORDS = 625;     // one stored state: 624 words + the next word's index
+constexpr int BLOCK_SHUF = 256;   // threads of the reference-order direction shuffle
+constexpr int SHUF_SMEM_NACT = 32768;  // directions staged in shared memory up to this many
 
 // A cell group: up to 2 x 2 x 2 cells (clipped at the box edge) and the union
 // of their neighbour cells, up to 4 x 4 x 4, in which union cell (ux,uy,uz)
@@ -73,6 +77,7 @@ struct SysDesc {
   int shuffle, list_mode, precision, goff;  // goff: offset of the system's groups
   int tile0_a, ntile_a, box, xoff;            // kick/drift tiles; box: whole-box kernels (2..4 cells per side), xoff: first box tile
   int cpb, msub, bz, soff;                    // cpb: cells per whole-box block; msub: list sub-cells per side, bz: their list bricks' depth, soff: first sub-cell start
+  int drift_every, pad0, pad1, pad2;          // drift_every: remove the mean momentum after every such step (0: never)
   double L, invL, inv_cell;  // inv_cell: cells per unit reduced length (InvCellSize)
   double T, f0, dt, half_dt, skin2, rebuild_factor, dof;
   double q[NHC_M];
@@ -98,6 +103,15 @@ struct SysState {
   int overflow;
   int obs_lo, obs_hi, obs_cur;  // observable events due this step, next event
   unsigned int counter_o;       // last-block counter of the observable kernel
+  int shuf;                  // this step re-randomises the directions (reference order, MT19937)
+  int mt_cur;                // which of the two stored MT19937 states is current
+  int drift;                 // this step ends with the mean momentum removed (fixDrift)
+  unsigned int counter_d;    // last-block counter of the drift kernels
+  double drift_m[3];         // mean momentum of the last drift removal
+  double ramp_T, ramp_dT;    // temperature ramp: this step's target and its change per step
+  double ramp_end;           // the ramp's final temperature (target of the padding steps)
+  long long ramp_left;       // ramp steps still to run (NVE with a velocity rescale before each)
+  long long ramp_real;       // of these, steps of the ramp itself; the rest hold ramp_end
 };
 
 // In-place observables of one system (set by acg_obs_configure): events of the
@@ -129,6 +143,7 @@ struct View {
   float4 *xsub;     // whole-box systems with list sub-cells: the system in sub-cell order {x, y, z, list code}
   int *ssub;        // their sub-cell starts [msub^3 + 1] per system
   int *rbs;         // this step's rebuilding systems with list sub-cells: count, bricks, then (system, first brick)
+  unsigned int *mt; // [nsys][2][MT_WORDS]: two stored MT19937 states per system (current, next)
   int *ccount_b, *cfill, *cstart, *ccount;
   const int2 *tiles_a, *tiles_b, *tiles_l, *tiles_c, *tiles_g, *tiles_x;
   int *gstart;      // per group: first centre particle (prefix over the system's groups)
@@ -216,6 +231,21 @@ __device__ inline double nhc_half(double *eta, double *p_eta, const double *q, d
   double s2k = (s * s) * ksum;
   nhc_u4(p_eta, q, T, dof, t4, 0, NHC_M - 1, s2k);
   return s;
+}
+
+// MT19937 (Matsumoto & Nishimura 1998): seeding by their 2002 initialisation
+// (GSL's gsl_rng_set for mt19937, seed 0 taken as 4357), tempering of one word
+__host__ __device__ inline void mt_seed(unsigned int *mt, unsigned long long seed) {
+  if (seed == 0) seed = 4357;
+  mt[0] = (unsigned int)(seed & 0xffffffffull);
+  for (int i = 1; i < MT_N; i++) mt[i] = 1812433253u * (mt[i - 1] ^ (mt[i - 1] >> 30)) + (unsigned int)i;
+  mt[MT_N] = MT_N;  // next word index: the first draw twists
+}
+__device__ __forceinline__ unsigned int mt_temper(unsigned int y) {
+  y ^= y >> 11;
+  y ^= (y << 7) & 0x9d2c5680u;
+  y ^= (y << 15) & 0xefc60000u;
+  return y ^ (y >> 18);
 }
 
 // keyed bijection of 32-bit integers (4-round Feistel network): distinct

@@ -37,6 +37,7 @@ constexpr int GRAPH_STEPS = 32;
 
 struct Layout {
   int nsys = 0, nslots = 0, ncells = 0, nact = 0, maxnb = 0, ngroups = 0, nboxtiles = 0, box_nmax = 0;
+  int nact_max = 0;  // most active particles of one system
   int box_m3max = 0;  // most list sub-cells of a whole-box system (0: none uses them)
   int box_cell_nmax = 0;  // most particles of a whole-box system listed from its cells
   int nsub = 0;           // sub-cell starts of all whole-box systems with list sub-cells
@@ -80,14 +81,17 @@ int resolve(const acg_params &p, SysDesc &d) {
   }
   d.tau_p = p.tau_p_steps;
   d.thermostat = p.thermostat ? 1 : 0;
-  d.shuffle = p.shuffle ? 1 : 0;
+  d.shuffle = p.shuffle;
+  d.drift_every = p.drift_every;
   d.list_mode = p.list_mode;
   d.precision = p.precision;
   d.seed = p.seed;
   if (p.dt <= 0 || p.skin <= 0 || p.rebuild_factor <= 0)
     return fail(ACG_ERR_INVALID, "dt, skin and rebuild_factor must be positive");
   if (p.thermostat && !(p.T > 0)) return fail(ACG_ERR_INVALID, "thermostat needs T > 0");
+  if (p.shuffle < 0 || p.shuffle > 2) return fail(ACG_ERR_INVALID, "shuffle must be 0, 1 or 2");
   if (p.shuffle && p.tau_p_steps <= 0) return fail(ACG_ERR_INVALID, "shuffle needs tau_p_steps > 0");
+  if (p.drift_every < 0) return fail(ACG_ERR_INVALID, "drift_every must be >= 0");
   return ACG_OK;
 }
 
@@ -137,6 +141,7 @@ int plan(const acg_params *params, int nsys, Layout &lay, int nsm) {
     lay.nslots += (int)align_up((size_t)d.n, 32);
     lay.ncells += d.ncell;
     lay.nact += d.nact;
+    lay.nact_max = std::max(lay.nact_max, d.nact);
     dens_max = std::max(dens_max, (double)d.n / (d.L * d.L * d.L));
   }
   // whole-box partition: about two blocks per SM over all whole-box cells,
@@ -194,6 +199,7 @@ int plan(const acg_params *params, int nsys, Layout &lay, int nsm) {
   add(16 * S);                            // xsub
   add(4 * ((size_t)lay.nsub + 1));        // ssub
   add(4 * (2 * (size_t)nsys + 2));        // rbs
+  add(4 * 2 * (size_t)MT_WORDS * nsys);   // mt
   lay.bytes = b;
   return ACG_OK;
 }
@@ -205,13 +211,6 @@ namespace acg {
 int set_last_error(int code, const std::string &msg) { return fail(code, msg); }
 }  // namespace acg
 
-// whole-step kernel (one block per system) for engines whose systems are all
-// whole-box; off by default: one block per system leaves a lone small system
-// on one SM and balances a batch of uneven sizes poorly
-#ifndef ACG_FUSED_STEPS
-#define ACG_FUSED_STEPS 0
-#endif
-
 struct acg_engine {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -220,7 +219,6 @@ struct acg_engine {
   View v{};
   SysDesc *d_desc = nullptr;
   int tpp = 4, block = 128, gtpp = 2, btpp = 2;  // btpp: whole-box kernels
-  bool fused = false;  // every system whole-box: one k_steps_box launch per step
   int ntiles_a = 0, ntiles_b = 0, ntiles_l = 0, ntiles_c = 0, ntiles_g = 0, ntiles_x = 0;
   int2 *d_tiles_b = nullptr;
   std::vector<int> dirty;  // systems whose forces/lists must be recomputed
@@ -270,22 +268,14 @@ GroupFn box_fn(int gtpp, int prec) {
 }
 // whole-box staging: int4 fixed point (FP32) or three doubles (FP64) per particle
 size_t box_smem(int nmax, int prec) { return (size_t)nmax * 3 * (prec ? sizeof(int) : sizeof(double)); }
-// whole-box list build: the staged system padded per cell (cell path, also the
-// fused kernel's); the sub-cell path reads the sorted system from memory.  The
-// sub-cell sort: two 16-bit arrays of n and the sub-cell starts and counters.
+// whole-box list build: the staged system padded per cell (cell path); the
+// sub-cell path reads the sorted system from memory.  The sub-cell sort: two
+// 16-bit arrays of n and the sub-cell starts and counters.
 size_t box_list_smem_cells(int nmax) { return ((size_t)nmax + 3 * MAX_BOX_CELLS) * sizeof(float4); }
 size_t box_list_smem(int cell_nmax) { return cell_nmax > 0 ? box_list_smem_cells(cell_nmax) : 0; }
+// reference-order shuffle: one system's directions staged as bytes
+size_t shuffle_smem(const Layout &lay) { return align_up((size_t)std::max(1, std::min(lay.nact_max, SHUF_SMEM_NACT)), 16); }
 size_t sort_sub_smem(int nmax, int m3max) { return (size_t)nmax * 2 * sizeof(uint16_t) + (2 * (size_t)m3max + 1) * sizeof(int); }
-using StepFn = void (*)(View, int);
-StepFn steps_fn(int gtpp, int prec) {
-  switch (gtpp) {
-    case 1: return prec ? (StepFn)k_steps_box<1, 1> : (StepFn)k_steps_box<1, 0>;
-    case 2: return prec ? (StepFn)k_steps_box<2, 1> : (StepFn)k_steps_box<2, 0>;
-    case 4: return prec ? (StepFn)k_steps_box<4, 1> : (StepFn)k_steps_box<4, 0>;
-  }
-  return nullptr;
-}
-size_t steps_smem(int nmax, int prec) { return std::max(box_list_smem_cells(nmax), box_smem(nmax, prec)); }
 
 ForceFn force_fn(int tpp, int prec) {
 #define F(T)                                                                     \
@@ -440,18 +430,15 @@ int launch_force(acg_engine *e, int mode) {
 }
 
 int launch_step_eager(acg_engine *e) {
-  if (e->fused) {
-    const int prec = e->lay.desc[0].precision;
-    steps_fn(e->btpp, prec)<<<e->lay.nsys, BLOCK_F, steps_smem(e->lay.box_nmax, prec), e->stream>>>(e->v, 1);
-    CK(cudaGetLastError());
-    return ACG_OK;
-  }
-  k_kick_drift<<<e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, 0, e->stream>>>(e->v, 0, 0, 0);
+  k_kick_drift<<<e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, 0, e->stream>>>(e->v, 0, 0, 0, 0);
+  k_shuffle_ref<<<3 * e->lay.nsys, BLOCK_SHUF, shuffle_smem(e->lay), e->stream>>>(e->v, -1);
   CK(cudaGetLastError());
   int rc = launch_rebuild(e);
   if (rc) return rc;
   rc = launch_force(e, 0);
   if (rc) return rc;
+  k_drift_sum<<<e->ntiles_a, BLOCK_A, 0, e->stream>>>(e->v);
+  k_drift_apply<<<e->ntiles_a, BLOCK_A, 0, e->stream>>>(e->v);
   k_observe<<<e->ntiles_a, BLOCK_A, 0, e->stream>>>(e->v);
   CK(cudaGetLastError());
   return ACG_OK;
@@ -500,11 +487,15 @@ int add_steps(acg_engine *e, cudaGraph_t g, int K, cudaGraphNode_t *prev_io) {
   GroupFn xf = box_fn(e->btpp, prec);
   int mode0 = 0, use_cond = 1, tbase = e->ntiles_g + e->ntiles_x;
   for (int s = 0; s < K; s++) {
-    cudaGraphConditionalHandle h, ho;
+    // per step: kick/drift, then two device-decided branches side by side (the
+    // list rebuild; the reference-order direction shuffle), the force kernels,
+    // and one device-decided branch after them (drift removal, observables)
+    cudaGraphConditionalHandle h, ho, hs;
     CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
     CK(cudaGraphConditionalHandleCreate(&ho, g, 0, cudaGraphCondAssignDefault));
-    cudaGraphNode_t na, nc, nb;
-    void *aa[] = {&v, &use_cond, &h, &ho};
+    CK(cudaGraphConditionalHandleCreate(&hs, g, 0, cudaGraphCondAssignDefault));
+    cudaGraphNode_t na, nc, ns, nb;
+    void *aa[] = {&v, &use_cond, &h, &ho, &hs};
     int rc = add_kernel(g, prev ? &prev : nullptr, prev ? 1 : 0, &na, (void *)k_kick_drift,
                         e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, aa);
     if (rc) return rc;
@@ -539,34 +530,63 @@ int add_steps(acg_engine *e, cudaGraph_t g, int K, cudaGraphNode_t *prev_io) {
       if (rc) return rc;
       bp = nn;
     }
-    cudaGraphNode_t last = nc;
+    cudaGraphNodeParams sp = {};
+    sp.type = cudaGraphNodeTypeConditional;
+    sp.conditional.handle = hs;
+    sp.conditional.type = cudaGraphCondTypeIf;
+    sp.conditional.size = 1;
+    CK(cudaGraphAddNode(&ns, g, &na, 1, &sp));
+    {
+      cudaGraphNode_t nk;
+      int all = -1;
+      void *sa[] = {&v, &all};
+      rc = add_kernel(sp.conditional.phGraph_out[0], nullptr, 0, &nk, (void *)k_shuffle_ref, 3 * e->lay.nsys,
+                      BLOCK_SHUF, sa, shuffle_smem(e->lay));
+      if (rc) return rc;
+    }
+    cudaGraphNode_t pre[2] = {nc, ns};
+    const cudaGraphNode_t *dep = pre;
+    size_t ndep = 2;
+    cudaGraphNode_t last = nullptr;
     if (e->ntiles_g) {
       void *ga[] = {&v, &mode0};
-      rc = add_kernel(g, &last, 1, &nb, (void *)gf, e->ntiles_g, BLOCK_G, ga, group_smem(v.gcap));
+      rc = add_kernel(g, dep, ndep, &nb, (void *)gf, e->ntiles_g, BLOCK_G, ga, group_smem(v.gcap));
       if (rc) return rc;
       last = nb;
+      dep = &last;
+      ndep = 1;
     }
     if (e->ntiles_x) {
       void *xa[] = {&v, &mode0};
-      rc = add_kernel(g, &last, 1, &nb, (void *)xf, e->ntiles_x, BLOCK_X, xa, box_smem(e->lay.box_nmax, prec));
+      rc = add_kernel(g, dep, ndep, &nb, (void *)xf, e->ntiles_x, BLOCK_X, xa, box_smem(e->lay.box_nmax, prec));
       if (rc) return rc;
       last = nb;
+      dep = &last;
+      ndep = 1;
     }
     if (e->ntiles_b) {
       void *ba[] = {&v, &mode0, &tbase};
-      rc = add_kernel(g, &last, 1, &nb, (void *)ff, e->ntiles_b, e->block, ba);
+      rc = add_kernel(g, dep, ndep, &nb, (void *)ff, e->ntiles_b, e->block, ba);
       if (rc) return rc;
       last = nb;
+      dep = &last;
+      ndep = 1;
     }
-    // observables at the scheduled steps (device-decided, like the rebuild)
+    // after the step: drift removal and observables at the scheduled steps
+    // (device-decided, like the rebuild)
     cudaGraphNodeParams op = {};
     op.type = cudaGraphNodeTypeConditional;
     op.conditional.handle = ho;
     op.conditional.type = cudaGraphCondTypeIf;
     op.conditional.size = 1;
-    cudaGraphNode_t no, nk;
-    CK(cudaGraphAddNode(&no, g, &last, 1, &op));
-    rc = add_kernel(op.conditional.phGraph_out[0], nullptr, 0, &nk, (void *)k_observe, e->ntiles_a, BLOCK_A, va);
+    cudaGraphNode_t no, nk0, nk1, nk2;
+    CK(cudaGraphAddNode(&no, g, dep, ndep, &op));
+    cudaGraph_t ob = op.conditional.phGraph_out[0];
+    rc = add_kernel(ob, nullptr, 0, &nk0, (void *)k_drift_sum, e->ntiles_a, BLOCK_A, va);
+    if (rc) return rc;
+    rc = add_kernel(ob, &nk0, 1, &nk1, (void *)k_drift_apply, e->ntiles_a, BLOCK_A, va);
+    if (rc) return rc;
+    rc = add_kernel(ob, &nk1, 1, &nk2, (void *)k_observe, e->ntiles_a, BLOCK_A, va);
     if (rc) return rc;
     prev = no;
   }
@@ -577,27 +597,6 @@ int add_steps(acg_engine *e, cudaGraph_t g, int K, cudaGraphNode_t *prev_io) {
 int build_graph(acg_engine *e, int K, cudaGraph_t *gout, cudaGraphExec_t *xout) {
   cudaGraph_t g;
   CK(cudaGraphCreate(&g, 0));
-  View v = e->v;
-  const int prec = e->lay.desc[0].precision;
-  if (e->fused) {
-    // one whole-step launch per step, all systems of the batch
-    StepFn sf = steps_fn(e->btpp, prec);
-    cudaGraphNode_t prev = nullptr;
-    int one = 1;
-    for (int s = 0; s < K; s++) {
-      void *a[] = {&v, &one};
-      cudaGraphNode_t nn;
-      int rc = add_kernel(g, prev ? &prev : nullptr, prev ? 1 : 0, &nn, (void *)sf, e->lay.nsys, BLOCK_F, a,
-                          steps_smem(e->lay.box_nmax, prec));
-      if (rc) return rc;
-      prev = nn;
-    }
-    cudaGraphExec_t x;
-    CK(cudaGraphInstantiate(&x, g, 0));
-    *gout = g;
-    *xout = x;
-    return ACG_OK;
-  }
   cudaGraphNode_t prev = nullptr;
   int rc = add_steps(e, g, K, &prev);
   if (rc) return rc;
@@ -708,6 +707,7 @@ int acg_params_default(acg_params *p, int n) {
   p->shuffle = 1;
   p->precision = ACG_PREC_FP64;
   p->seed = 12345;
+  p->drift_every = 100000;  // fixDrift cadence of run() (MDcode/main.c:261)
   return ACG_OK;
 }
 
@@ -805,6 +805,7 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   v.xsub = (float4 *)take(16 * S);
   v.ssub = (int *)take(4 * ((size_t)L.nsub + 1));
   v.rbs = (int *)take(4 * (2 * (size_t)nsys + 2));
+  v.mt = (unsigned int *)take(4 * 2 * (size_t)MT_WORDS * nsys);
   v.tiles_a = ta;
   v.tiles_b = e->d_tiles_b;
   v.tiles_l = tl;
@@ -886,14 +887,10 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
       for (int pr : {0, 1}) attr_ok = attr_ok && raise_smem((const void *)box_fn(gt, pr), box_smem(L.box_nmax, pr));
     attr_ok = attr_ok && raise_smem((const void *)k_build_list_box, box_list_smem(L.box_cell_nmax));
     attr_ok = attr_ok && raise_smem((const void *)k_sort_sub, sort_sub_smem(L.box_nmax, L.box_m3max));
-    for (int gt : {1, 2, 4})
-      for (int pr : {0, 1}) attr_ok = attr_ok && raise_smem((const void *)steps_fn(gt, pr), steps_smem(L.box_nmax, pr));
   }
   // threads per particle of the whole-box kernels: fixed (not derived from the
   // batch), so an FP64 system sums its pairs in the same order alone and batched
   e->btpp = 2;
-  e->fused = ACG_FUSED_STEPS != 0;
-  for (int r = 0; r < nsys; r++) e->fused = e->fused && L.desc[r].box;
   if (!attr_ok) {
     acg_destroy(e);
     return fail(ACG_ERR_CUDA, "cudaFuncSetAttribute (group kernels' shared memory) failed");
@@ -925,6 +922,15 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   if (cudaMemcpyAsync(v.st, st.data(), sizeof(SysState) * nsys, cudaMemcpyHostToDevice, e->stream) !=
       cudaSuccess)
     return cleanup_fail(fail(ACG_ERR_CUDA, "state upload failed"));
+  {
+    // each system's direction-shuffle stream (state buffer 0 current)
+    std::vector<unsigned int> mt(2 * (size_t)MT_WORDS * nsys, 0u);
+    for (int r = 0; r < nsys; r++) mt_seed(mt.data() + 2 * (size_t)MT_WORDS * r, L.desc[r].seed);
+    if (cudaMemcpyAsync(v.mt, mt.data(), mt.size() * sizeof(unsigned int), cudaMemcpyHostToDevice, e->stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(e->stream) != cudaSuccess)
+      return cleanup_fail(fail(ACG_ERR_CUDA, "shuffle stream upload failed"));
+  }
   rc = build_tiles_b(e);
   if (rc) return cleanup_fail(rc);
   e->dirty.assign(nsys, 1);
@@ -1020,8 +1026,10 @@ int acg_set_state(acg_engine *e, int sys, const double *x, const double *xu, con
   k_load<<<std::max(1, std::min((int)((n + 255) / 256), 1024)), 256, 0, e->stream>>>(e->v, sys);
   CK(cudaGetLastError());
   double one = 1.0;
+  long long zero_ll = 0;
   CK(cudaMemcpyAsync(&e->v.st[sys].s1, &one, sizeof(double), cudaMemcpyHostToDevice, e->stream));
   CK(cudaMemcpyAsync(&e->v.st[sys].s2, &one, sizeof(double), cudaMemcpyHostToDevice, e->stream));
+  CK(cudaMemcpyAsync(&e->v.st[sys].ramp_left, &zero_ll, sizeof(long long), cudaMemcpyHostToDevice, e->stream));
   CK(cudaStreamSynchronize(e->stream));  // host buffers may be freed on return
   e->dirty[sys] = 1;
   e->any_dirty = true;
@@ -1089,8 +1097,140 @@ int acg_shuffle_directions(acg_engine *e, int sys) {
   if (rc) return rc;
   if (e->lay.desc[sys].nact == 0) return ACG_OK;
   CK(cudaSetDevice(e->device));
-  k_shuffle_now<<<3, 256, 0, e->stream>>>(e->v, sys);
+  if (e->lay.desc[sys].shuffle == 2) {
+    k_shuffle_now<<<3, 256, 0, e->stream>>>(e->v, sys);
+  } else {
+    k_shuffle_ref<<<3, BLOCK_SHUF, shuffle_smem(e->lay), e->stream>>>(e->v, sys);
+    k_mt_flip<<<1, 32, 0, e->stream>>>(e->v, sys);
+  }
   CK(cudaGetLastError());
+  return ACG_OK;
+}
+
+int acg_seed_shuffle(acg_engine *e, int sys, uint64_t seed) {
+  int rc = check_sys(e, sys);
+  if (rc) return rc;
+  CK(cudaSetDevice(e->device));
+  SysState st;
+  CK(cudaMemcpyAsync(&st, e->v.st + sys, sizeof(st), cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  std::vector<unsigned int> mt(MT_WORDS);
+  mt_seed(mt.data(), seed);
+  CK(cudaMemcpyAsync(e->v.mt + ((size_t)2 * sys + st.mt_cur) * MT_WORDS, mt.data(), MT_WORDS * sizeof(unsigned int),
+                     cudaMemcpyHostToDevice, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  return ACG_OK;
+}
+
+int acg_fix_drift(acg_engine *e, int sys) {
+  int rc = check_sys(e, sys);
+  if (rc) return rc;
+  CK(cudaSetDevice(e->device));
+  rc = prime(e);
+  if (rc) return rc;
+  k_flag_drift<<<1, 32, 0, e->stream>>>(e->v, sys);
+  k_drift_sum<<<e->ntiles_a, BLOCK_A, 0, e->stream>>>(e->v);
+  k_drift_apply<<<e->ntiles_a, BLOCK_A, 0, e->stream>>>(e->v);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(e->stream));
+  return ACG_OK;
+}
+
+int acg_adjust_temperature(acg_engine *e, int sys, double T, double *inst_T) {
+  int rc = check_sys(e, sys);
+  if (rc) return rc;
+  if (!(T > 0) || !std::isfinite(T)) return fail(ACG_ERR_INVALID, "T must be positive");
+  CK(cudaSetDevice(e->device));
+  rc = prime(e);
+  if (rc) return rc;
+  k_rescale<<<1, 1024, 0, e->stream>>>(e->v, sys, T);
+  CK(cudaGetLastError());
+  double ke = 0;
+  CK(cudaMemcpyAsync(&ke, &e->v.st[sys].ke_end, sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  if (inst_T) *inst_T = 2.0 * ke / e->lay.desc[sys].dof;
+  return ACG_OK;
+}
+
+int acg_start_ramp(acg_engine *e, int sys, double T_start, double T_end, double rate, int64_t *steps) {
+  int rc = check_sys(e, sys);
+  if (rc) return rc;
+  if (!(T_start > 0) || !(T_end > 0) || !(rate > 0) || !std::isfinite(T_start) || !std::isfinite(T_end))
+    return fail(ACG_ERR_INVALID, "ramp temperatures and rate must be positive");
+  const SysDesc &d = e->lay.desc[sys];
+  double T0 = 0;
+  rc = acg_adjust_temperature(e, sys, T_start, &T0);
+  if (rc) return rc;
+  // the reference's loop: while (T < final) { rescale to T; step; T += dt*rate }
+  // (heating, MDcode/initialise.c:179-186) or while (T > final) ... T -= dt*rate
+  // (cooling, :191-197), T starting at the temperature reached by the rescale
+  const double dT = d.dt * rate;
+  const bool heat = T_end > T_start;
+  long long K = 0;
+  for (double T = T0; heat ? T < T_end : T > T_end; T = heat ? T + dT : T - dT) {
+    if (++K > 100000000LL) return fail(ACG_ERR_INVALID, "ramp longer than 1e8 steps");
+  }
+  CK(cudaSetDevice(e->device));
+  // the ramps rebuild the lists at their start (update_cell_list,
+  // MDcode/initialise.c:174,192); the positions, hence the forces, stay
+  k_flag_rebuild_one<<<1, 256, 0, e->stream>>>(e->v, sys);
+  CK(cudaGetLastError());
+  rc = launch_rebuild(e);
+  if (rc) return rc;
+  k_ramp_begin<<<1, 32, 0, e->stream>>>(e->v, sys, T0, heat ? dT : -dT, T_end, K);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(e->stream));
+  if (steps) *steps = K;
+  return ACG_OK;
+}
+
+int acg_extend_ramp(acg_engine *e, int sys, int64_t total_steps) {
+  int rc = check_sys(e, sys);
+  if (rc) return rc;
+  CK(cudaSetDevice(e->device));
+  k_ramp_extend<<<1, 32, 0, e->stream>>>(e->v, sys, (long long)total_steps);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(e->stream));
+  return ACG_OK;
+}
+
+int acg_set_lattice(acg_engine *e, int sys, const int *site, const int *type, const double *p, const int *act_tag) {
+  int rc = check_sys(e, sys);
+  if (rc) return rc;
+  if (!site || !type || !p || !act_tag) return fail(ACG_ERR_INVALID, "site, type, p and act_tag are required");
+  const SysDesc &d = e->lay.desc[sys];
+  const size_t n = d.n;
+  int troot = 1;
+  while ((long long)troot * troot * troot < (long long)n) troot++;  // MDcode/initialise.c:35-37
+  const long long nsite = (long long)troot * troot * troot;
+  std::vector<char> used((size_t)nsite, 0);
+  for (size_t i = 0; i < n; i++) {
+    if (site[i] < 0 || site[i] >= nsite || used[site[i]])
+      return fail(ACG_ERR_INVALID, "site must hold distinct grid sites in [0, troot^3)");
+    used[site[i]] = 1;
+    if (type[i] != 0 && type[i] != 1) return fail(ACG_ERR_INVALID, "type must be 0 or 1");
+    if (act_tag[i] < -1 || act_tag[i] >= d.nact) return fail(ACG_ERR_INVALID, "act_tag out of range");
+  }
+  CK(cudaSetDevice(e->device));
+  double *sd = e->v.stage_d + 9 * (size_t)d.poff;
+  int *si = e->v.stage_i + 2 * (size_t)d.poff;
+  CK(cudaMemcpyAsync(sd + 6 * n, p, 24 * n, cudaMemcpyHostToDevice, e->stream));
+  CK(cudaMemcpyAsync(si, type, 4 * n, cudaMemcpyHostToDevice, e->stream));
+  CK(cudaMemcpyAsync(si + n, site, 4 * n, cudaMemcpyHostToDevice, e->stream));
+  const int grid = std::max(1, std::min((int)((n + 255) / 256), 1024));
+  k_lattice<<<grid, 256, 0, e->stream>>>(e->v, sys, troot);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(si + n, act_tag, 4 * n, cudaMemcpyHostToDevice, e->stream));
+  k_load<<<grid, 256, 0, e->stream>>>(e->v, sys);
+  CK(cudaGetLastError());
+  double one = 1.0;
+  long long zero_ll = 0;
+  CK(cudaMemcpyAsync(&e->v.st[sys].s1, &one, sizeof(double), cudaMemcpyHostToDevice, e->stream));
+  CK(cudaMemcpyAsync(&e->v.st[sys].s2, &one, sizeof(double), cudaMemcpyHostToDevice, e->stream));
+  CK(cudaMemcpyAsync(&e->v.st[sys].ramp_left, &zero_ll, sizeof(long long), cudaMemcpyHostToDevice, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  e->dirty[sys] = 1;
+  e->any_dirty = true;
   return ACG_OK;
 }
 
@@ -1163,7 +1303,7 @@ int acg_step(acg_engine *e, int nsteps) {
   CK(cudaSetDevice(e->device));
   int rc = prime(e);
   if (rc) return rc;
-  if (!e->fused && !e->no_while) {
+  if (!e->no_while) {
     // device loop: one launch for the GRAPH_STEPS-step blocks, one for the rest
     const long long q = nsteps / GRAPH_STEPS, r = nsteps % GRAPH_STEPS;
     const int need[3] = {q > 0 && e->wturn == 0, q > 0 && e->wturn == 1, r > 0};
@@ -1209,7 +1349,7 @@ int acg_prepare(acg_engine *e) {
   CK(cudaSetDevice(e->device));
   int rc = prime(e);
   if (rc) return rc;
-  if (e->fused || e->no_while) return ACG_OK;
+  if (e->no_while) return ACG_OK;
   for (int k = 0; k < 3 && !e->no_while; k++)
     if (!e->wexec[k] &&
         build_while_graph(e, k < 2 ? GRAPH_STEPS : 1, e->counts + k, &e->wgraph[k], &e->wexec[k]) != ACG_OK)
@@ -1355,7 +1495,7 @@ int acg_time_stage(acg_engine *e, int stage, int reps, double *ms) {
   CK(cudaEventRecord(a, e->stream));
   for (int i = 0; i < reps; i++) {
     if (stage == 0) {
-      k_kick_drift<<<e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, 0, e->stream>>>(e->v, 0, 0, 0);
+      k_kick_drift<<<e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, 0, e->stream>>>(e->v, 0, 0, 0, 0);
     } else if (stage == 1) {
       rc = launch_force(e, 2);
     } else {
@@ -1544,11 +1684,11 @@ int acg_bench_steps(acg_engine *e, int nchunks, size_t flush_bytes, double *ms, 
   // rebuild kernels with a non-empty grid (the node list of build_graph)
   long long steps_with_rebuild = 0;
   for (int r = 0; r < e->lay.nsys; r++) steps_with_rebuild = std::max(steps_with_rebuild, rb1[r] - rb0[r]);
-  const long long per_step = e->fused ? 1 : 1 + (e->ntiles_g > 0) + (e->ntiles_x > 0) + (e->ntiles_b > 0);
+  const long long per_step = 1 + (e->ntiles_g > 0) + (e->ntiles_x > 0) + (e->ntiles_b > 0);
   const long long per_rebuild = 3 * (e->ntiles_a > 0) + (e->lay.nsys > 0) + (e->ntiles_c > 0) +
                                 (e->ntiles_g > 0) + (e->ntiles_x > 0) + (e->ntiles_l > 0);
   *ms = tot;
-  if (launches) *launches = per_step * GRAPH_STEPS * nchunks + (e->fused ? 0 : per_rebuild * steps_with_rebuild);
+  if (launches) *launches = per_step * GRAPH_STEPS * nchunks + per_rebuild * steps_with_rebuild;
   return ACG_OK;
 }
 

@@ -116,6 +116,122 @@ __device__ void shuffle_component(const View &v, int r, int comp, long long step
 }
 
 // ---------------------------------------------------------------------------
+// ShuffleActDirec (MDcode/active.c:45-85) in the reference's own order: for
+// each component in turn (x, y, z) and i = 0 .. Nact-1, swap k[i] with k[j],
+// j = (int)(Nact * u), u = the next MT19937 word / 2^32 (gsl_ran_flat(0, 1)
+// through uniform(), MDcode/initialise.c:19-21).  All three components draw
+// from one stream, so with the same seed the directions equal the reference
+// program's bit for bit.
+//
+// One block per (system, component): every block regenerates the stream from
+// the stored state (twisting 624 words per round in four dependency phases)
+// and its one thread 0 applies the swaps of its component's draws to the
+// component staged in shared memory; the swaps depend on one another and
+// stay sequential.  The z block stores the state after all 3 Nact draws into
+// the other buffer; the step's last force block makes it current.
+
+// one twist of the 624-word state by all threads of the block: word i needs
+// words i+1 (old) and i+397 (wrapping to i-227, already new for i >= 227),
+// so [0,227), [227,454), [454,623) and 623 are computed one after another
+__device__ __forceinline__ void mt_twist(unsigned int *mt) {
+  const int lo[4] = {0, 227, 454, 623}, hi[4] = {227, 454, 623, 624};
+#pragma unroll
+  for (int ph = 0; ph < 4; ph++) {
+    const int i = lo[ph] + (int)threadIdx.x;
+    unsigned int w = 0;
+    const bool act = i < hi[ph];
+    if (act) {
+      const unsigned int y = (mt[i] & 0x80000000u) | (mt[i + 1 < MT_N ? i + 1 : 0] & 0x7fffffffu);
+      w = mt[i + 397 < MT_N ? i + 397 : i + 397 - MT_N] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+    }
+    __syncthreads();
+    if (act) mt[i] = w;
+    __syncthreads();
+  }
+}
+
+// one component of one system (blockDim.x == BLOCK_SHUF); state read from
+// mt_in, the final state (after 3 nact draws) written to mt_out by comp 2
+__device__ void shuffle_ref_component(const View &v, int r, int comp, const unsigned int *mt_in,
+                                      unsigned int *mt_out) {
+  __shared__ unsigned int s_mt[MT_N];
+  __shared__ int s_j[MT_N];
+  extern __shared__ signed char s_k[];
+  const SysDesc &d = v.desc[r];
+  const int nact = d.nact;
+  char4 *kd = v.kdir + d.aoff;
+  signed char *kg = reinterpret_cast<signed char *>(kd) + comp;  // component bytes, stride 4
+  const bool staged = nact <= SHUF_SMEM_NACT;
+  for (int a = threadIdx.x; a < MT_N; a += blockDim.x) s_mt[a] = mt_in[a];
+  if (staged)
+    for (int a = threadIdx.x; a < nact; a += blockDim.x) s_k[a] = kg[4 * (size_t)a];
+  int idx = (int)mt_in[MT_N];
+  __syncthreads();
+  const long long beg = (long long)comp * nact, end = beg + nact;
+  long long pos = 0;  // draws taken so far
+  const double fn = (double)nact;
+  while (pos < end) {
+    if (idx >= MT_N) {
+      mt_twist(s_mt);
+      idx = 0;
+    }
+    const long long take = min((long long)(MT_N - idx), end - pos);
+    const long long lo = max(pos, beg), hi = pos + take;
+    if (lo < hi) {
+      const int w0 = idx + (int)(lo - pos), cnt = (int)(hi - lo);
+      for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+        // (double)Nact * uniform(0,1); the word / 2^32 is exact
+        const double u = (double)mt_temper(s_mt[w0 + t]) * (1.0 / 4294967296.0);
+        s_j[t] = (int)__dmul_rn(fn, u);
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        int i = (int)(lo - beg);
+        if (staged) {
+          for (int t = 0; t < cnt; t++, i++) {
+            const int j = s_j[t];
+            const signed char a = s_k[i];
+            s_k[i] = s_k[j];
+            s_k[j] = a;
+          }
+        } else {
+          for (int t = 0; t < cnt; t++, i++) {
+            const size_t ii = 4 * (size_t)i, jj = 4 * (size_t)s_j[t];
+            const signed char a = kg[ii];
+            kg[ii] = kg[jj];
+            kg[jj] = a;
+          }
+        }
+      }
+      __syncthreads();
+    }
+    pos += take;
+    idx += (int)take;
+  }
+  if (staged)
+    for (int a = threadIdx.x; a < nact; a += blockDim.x) kg[4 * (size_t)a] = s_k[a];
+  if (comp == 2) {
+    for (int a = threadIdx.x; a < MT_N; a += blockDim.x) mt_out[a] = s_mt[a];
+    if (threadIdx.x == 0) mt_out[MT_N] = (unsigned int)idx;
+  }
+}
+
+// blocks 3 r + c: component c of system r (only >= 0: system `only`, blocks 0..2)
+__global__ void __launch_bounds__(BLOCK_SHUF) k_shuffle_ref(View v, int only) {
+  const int r = only >= 0 ? only : (int)blockIdx.x / 3, comp = (int)blockIdx.x % 3;
+  const SysDesc &d = v.desc[r];
+  const SysState &st = v.st[r];
+  if (d.nact == 0 || (only < 0 && !st.shuf)) return;
+  unsigned int *mt = v.mt + (size_t)r * 2 * MT_WORDS;
+  shuffle_ref_component(v, r, comp, mt + (size_t)st.mt_cur * MT_WORDS, mt + (size_t)(st.mt_cur ^ 1) * MT_WORDS);
+}
+
+// the stored state after a shuffle outside the step becomes current
+__global__ void k_mt_flip(View v, int r) {
+  if (threadIdx.x == 0 && v.desc[r].nact > 0) v.st[r].mt_cur ^= 1;
+}
+
+// ---------------------------------------------------------------------------
 // U3 U2 (pending thermostat scales and the half kick) and U1 for one
 // particle, in the reference's order of roundings; returns |x_u - x_old|^2
 // (reduced units) for the rebuild test
@@ -173,9 +289,19 @@ __device__ __forceinline__ int obs_due(const ObsDesc &o, SysState &st) {
 }
 
 // ---------------------------------------------------------------------------
-// stage 1: kick + drift (+ shuffle blocks) + rebuild decision
+// per-step events of one system decided before its forces: the direction
+// shuffle every tau_p steps (MDcode/main.c:245-247) and the mean-momentum
+// removal after every drift_every-th step (MDcode/main.c:261); neither runs
+// during a temperature ramp (the reference's ramps, MDcode/initialise.c:166-201,
+// only step)
+__device__ __forceinline__ bool shuffle_due(const SysDesc &d, const SysState &st, int mode) {
+  return d.shuffle == mode && d.nact > 0 && d.tau_p > 0 && st.ramp_left == 0 && (st.step % d.tau_p) == 0;
+}
+
+// stage 1: kick + drift (+ uniform-shuffle blocks) + rebuild decision
 __global__ void __launch_bounds__(BLOCK_A) k_kick_drift(View v, int use_cond, cudaGraphConditionalHandle h,
-                                                        cudaGraphConditionalHandle h_obs) {
+                                                        cudaGraphConditionalHandle h_obs,
+                                                        cudaGraphConditionalHandle h_shuf) {
   __shared__ double sm[BLOCK_A / 32];
   __shared__ int s_last;
   const int b = blockIdx.x;
@@ -200,10 +326,7 @@ __global__ void __launch_bounds__(BLOCK_A) k_kick_drift(View v, int use_cond, cu
   } else {
     int q = b - v.ntiles_a;
     int rs = q / 3, comp = q % 3;
-    const SysDesc &d = v.desc[rs];
-    long long step = v.st[rs].step;
-    if (d.shuffle && d.nact > 0 && d.tau_p > 0 && (step % d.tau_p) == 0)
-      shuffle_component(v, rs, comp, step);
+    if (shuffle_due(v.desc[rs], v.st[rs], 2)) shuffle_component(v, rs, comp, v.st[rs].step);
   }
   // the last block to finish takes the per-system rebuild decisions
   __threadfence();
@@ -212,21 +335,33 @@ __global__ void __launch_bounds__(BLOCK_A) k_kick_drift(View v, int use_cond, cu
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-  int any = 0;
+  int any = 0, any_post = 0, any_shuf = 0;
   for (int s = threadIdx.x; s < v.nsys; s += blockDim.x) {
-    unsigned long long bits = atomicExch(&v.st[s].maxd_bits, 0ull);
-    any |= rebuild_decision(v.desc[s], v.st[s], __longlong_as_double((long long)bits));
+    const SysDesc &d = v.desc[s];
+    SysState &st = v.st[s];
+    unsigned long long bits = atomicExch(&st.maxd_bits, 0ull);
+    any |= rebuild_decision(d, st, __longlong_as_double((long long)bits));
+    st.shuf = shuffle_due(d, st, 1);
+    any_shuf |= st.shuf;
+    st.drift = d.drift_every > 0 && st.ramp_left == 0 && (st.step % d.drift_every) == 0;
+    // observable events due at the end of this step (none during a ramp)
+    int ob = 0;
+    if (st.ramp_left == 0) {
+      ob = obs_due(v.obs[s], st);
+    } else {
+      st.obs_lo = st.obs_hi = 0;
+    }
+    any_post |= ob | st.drift;
   }
-  // observable events due at the end of this step
-  int any_obs = 0;
-  for (int s = threadIdx.x; s < v.nsys; s += blockDim.x) any_obs |= obs_due(v.obs[s], v.st[s]);
   any = __syncthreads_or(any);
-  any_obs = __syncthreads_or(any_obs);
+  any_post = __syncthreads_or(any_post);
+  any_shuf = __syncthreads_or(any_shuf);
   if (threadIdx.x == 0) {
     *v.counter_a = 0;
     if (use_cond) {
       cudaGraphSetConditional(h, any ? 1u : 0u);
-      cudaGraphSetConditional(h_obs, any_obs ? 1u : 0u);
+      cudaGraphSetConditional(h_obs, any_post ? 1u : 0u);
+      cudaGraphSetConditional(h_shuf, any_shuf ? 1u : 0u);
     }
   }
 }
@@ -350,6 +485,11 @@ __global__ void k_flag_rebuild(View v, int all) {
     SysState &st = v.st[s];
     st.rebuild = all ? 1 : st.prime;
   }
+}
+
+// host request: rebuild system r only (at its current positions)
+__global__ void k_flag_rebuild_one(View v, int r) {
+  for (int s = threadIdx.x; s < v.nsys; s += blockDim.x) v.st[s].rebuild = s == r;
 }
 
 // ---------------------------------------------------------------------------
@@ -666,6 +806,32 @@ __device__ void finalize_system(const View &v, int r, int mode) {
 // thermostat and scalars of one system from its sums (one thread): pe and
 // virial halved (every pair is counted from both sides), then for a step the
 // chain's second half on the new KE and its first half of the next step
+// the velocity scale of the next step's first half from sum p^2 = kb of the
+// velocities at the step boundary: the thermostat chain's U4 U3 U4
+// (MDcode/time_evolve.c:499-501), a ramp step's rescale to the ramp target
+// (adjustInitialTemp, MDcode/initialise.c:141-151, with inst_T of
+// calculate_temp, :153-164), or none (NVE)
+__device__ void next_first_half(const SysDesc &d, SysState &st, double kb) {
+  if (st.ramp_left > 0) {
+    const double inst = 2.0 * (kb * 0.5) / d.dof;
+    st.s1 = sqrt(st.ramp_T / inst);
+  } else if (d.thermostat) {
+    double eta[NHC_M], pet[NHC_M];
+    for (int k = 0; k < NHC_M; k++) {
+      eta[k] = st.eta_end[k];
+      pet[k] = st.p_eta_end[k];
+    }
+    double s1 = nhc_half(eta, pet, d.q, d.T, d.dof, d.dt, kb);
+    for (int k = 0; k < NHC_M; k++) {
+      st.eta_cur[k] = eta[k];
+      st.p_eta_cur[k] = pet[k];
+    }
+    st.s1 = s1;
+  } else {
+    st.s1 = 1.0;
+  }
+}
+
 __device__ void finalize_sums(const SysDesc &d, SysState &st, int mode, double pe, double vir, double ke, double va) {
   st.pe = 0.5 * pe;
   st.virial = (0.5 * vir) / 3.0;
@@ -675,10 +841,19 @@ __device__ void finalize_sums(const SysDesc &d, SysState &st, int mode, double p
     st.counter_b = 0;
     return;
   }
-  double eta[NHC_M], pet[NHC_M];
   double kb;
-  if (mode == 0) {
+  if (mode == 0 && st.ramp_left > 0) {
+    // a ramp step (advance_time_NVEFrog inside coldstart / breakxal): NVE, the
+    // step counter and its schedules stay where they are; the next ramp step
+    // rescales to the next target (T +- time_step * rate)
+    st.s2 = 1.0;
+    kb = ke;
+    st.ramp_left -= 1;
+    st.ramp_real -= 1;
+    if (st.ramp_left > 0) st.ramp_T = st.ramp_real > 0 ? __dadd_rn(st.ramp_T, st.ramp_dT) : st.ramp_end;
+  } else if (mode == 0) {
     if (d.thermostat) {
+      double eta[NHC_M], pet[NHC_M];
       for (int k = 0; k < NHC_M; k++) {
         eta[k] = st.eta_cur[k];
         pet[k] = st.p_eta_cur[k];
@@ -695,29 +870,209 @@ __device__ void finalize_sums(const SysDesc &d, SysState &st, int mode, double p
       kb = ke;
     }
     st.step += 1;
+    if (st.shuf) {  // the shuffle's new MT19937 state becomes current
+      st.mt_cur ^= 1;
+      st.shuf = 0;
+    }
   } else {
     st.s2 = 1.0;  // velocities were materialised by the prime pass
     kb = ke;
   }
   st.ke_end = kb * 0.5;
-  if (d.thermostat) {
-    for (int k = 0; k < NHC_M; k++) {
-      eta[k] = st.eta_end[k];
-      pet[k] = st.p_eta_end[k];
-    }
-    double s1 = nhc_half(eta, pet, d.q, d.T, d.dof, d.dt, kb);
-    for (int k = 0; k < NHC_M; k++) {
-      st.eta_cur[k] = eta[k];
-      st.p_eta_cur[k] = pet[k];
-    }
-    st.s1 = s1;
-  } else {
-    st.s1 = 1.0;
-  }
+  next_first_half(d, st, kb);
   if (!(ke == ke) || ke > 1.0e300) st.status = 1;
   st.prime = 0;
   __threadfence();
   st.counter_b = 0;
+}
+
+// ---------------------------------------------------------------------------
+// fixDrift (MDcode/initialise.c:104-138) after the step, on the momenta at the
+// step boundary p = v * s2: P = sum p / N, p -= P; then the next step's first
+// half from the new sum p^2 (the reference's next U4 sums the corrected p).
+// Two passes over the flagged systems: the mean, then the removal.
+__global__ void __launch_bounds__(BLOCK_A) k_drift_sum(View v) {
+  __shared__ double sh[BLOCK_A / 32];
+  __shared__ int s_last;
+  const int2 t = v.tiles_a[blockIdx.x];
+  const int r = t.x;
+  SysState &st = v.st[r];
+  if (!st.drift) return;
+  const SysDesc &d = v.desc[r];
+  const int loc = t.y + threadIdx.x;
+  const double s2 = st.s2;
+  double px = 0.0, py = 0.0, pz = 0.0;
+  if (loc < d.n) {
+    const int i = d.poff + loc;
+    px = __dmul_rn(v.vx[i], s2);
+    py = __dmul_rn(v.vy[i], s2);
+    pz = __dmul_rn(v.vz[i], s2);
+  }
+  px = block_sum<BLOCK_A / 32>(px, sh);
+  py = block_sum<BLOCK_A / 32>(py, sh);
+  pz = block_sum<BLOCK_A / 32>(pz, sh);
+  double *part = v.part_o + (size_t)blockIdx.x * OBS_EMAX * OBS_NV;
+  if (threadIdx.x == 0) {
+    part[0] = px;
+    part[1] = py;
+    part[2] = pz;
+    __threadfence();
+    s_last = atomicAdd(&st.counter_d, 1u) == (unsigned)(d.ntile_a - 1);
+  }
+  __syncthreads();
+  if (!s_last || threadIdx.x != 0) return;
+  __threadfence();
+  double P[3] = {0.0, 0.0, 0.0};
+  for (int b = 0; b < d.ntile_a; b++) {
+    const double *pb = v.part_o + (size_t)(d.tile0_a + b) * OBS_EMAX * OBS_NV;
+    for (int k = 0; k < 3; k++) P[k] += __ldcg(pb + k);
+  }
+  for (int k = 0; k < 3; k++) st.drift_m[k] = P[k] / (double)d.n;
+  __threadfence();
+  st.counter_d = 0;
+}
+
+__global__ void __launch_bounds__(BLOCK_A) k_drift_apply(View v) {
+  __shared__ double sh[BLOCK_A / 32];
+  __shared__ int s_last;
+  const int2 t = v.tiles_a[blockIdx.x];
+  const int r = t.x;
+  SysState &st = v.st[r];
+  if (!st.drift) return;
+  const SysDesc &d = v.desc[r];
+  const int loc = t.y + threadIdx.x;
+  const double s2 = st.s2, mx = st.drift_m[0], my = st.drift_m[1], mz = st.drift_m[2];
+  double k2 = 0.0;
+  if (loc < d.n) {
+    const int i = d.poff + loc;
+    const double px = __dadd_rn(__dmul_rn(v.vx[i], s2), -mx);
+    const double py = __dadd_rn(__dmul_rn(v.vy[i], s2), -my);
+    const double pz = __dadd_rn(__dmul_rn(v.vz[i], s2), -mz);
+    v.vx[i] = px;
+    v.vy[i] = py;
+    v.vz[i] = pz;
+    k2 = px * px + py * py + pz * pz;
+  }
+  k2 = block_sum<BLOCK_A / 32>(k2, sh);
+  double *part = v.part_o + (size_t)blockIdx.x * OBS_EMAX * OBS_NV;
+  if (threadIdx.x == 0) {
+    part[3] = k2;
+    __threadfence();
+    s_last = atomicAdd(&st.counter_d, 1u) == (unsigned)(d.ntile_a - 1);
+  }
+  __syncthreads();
+  if (!s_last || threadIdx.x != 0) return;
+  __threadfence();
+  double kb = 0.0;
+  for (int b = 0; b < d.ntile_a; b++) kb += __ldcg(v.part_o + (size_t)(d.tile0_a + b) * OBS_EMAX * OBS_NV + 3);
+  st.s2 = 1.0;
+  st.ke_end = kb * 0.5;
+  next_first_half(d, st, kb);
+  st.drift = 0;
+  __threadfence();
+  st.counter_d = 0;
+}
+
+// host request: remove the mean momentum of system r now (with k_drift_sum and
+// k_drift_apply after it)
+__global__ void k_flag_drift(View v, int r) {
+  if (threadIdx.x == 0) v.st[r].drift = 1;
+}
+
+// adjustInitialTemp (MDcode/initialise.c:141-151) for system r, one block:
+// the momenta at the step boundary (v * s2) are scaled by sqrt(T / inst_T)
+// with inst_T from their sum p^2 (calculate_temp); the new sum sets ke_end and
+// the next step's first half.  Ramp (ramp_left > 0, set by k_ramp_begin after
+// this): the first ramp step's rescale.
+__global__ void __launch_bounds__(1024) k_rescale(View v, int r, double T) {
+  __shared__ double sh[32];
+  __shared__ double s_xi;
+  const SysDesc &d = v.desc[r];
+  SysState &st = v.st[r];
+  const double s2 = st.s2;
+  double k2 = 0.0;
+  for (int k = threadIdx.x; k < d.n; k += blockDim.x) {
+    const int i = d.poff + k;
+    const double px = __dmul_rn(v.vx[i], s2), py = __dmul_rn(v.vy[i], s2), pz = __dmul_rn(v.vz[i], s2);
+    v.vx[i] = px;
+    v.vy[i] = py;
+    v.vz[i] = pz;
+    k2 += px * px + py * py + pz * pz;
+  }
+  k2 = block_sum_dyn(k2, sh);
+  if (threadIdx.x == 0) {
+    const double inst = 2.0 * (k2 * 0.5) / d.dof;
+    s_xi = sqrt(T / inst);
+  }
+  __syncthreads();
+  const double xi = s_xi;
+  double k3 = 0.0;
+  for (int k = threadIdx.x; k < d.n; k += blockDim.x) {
+    const int i = d.poff + k;
+    const double px = __dmul_rn(v.vx[i], xi), py = __dmul_rn(v.vy[i], xi), pz = __dmul_rn(v.vz[i], xi);
+    v.vx[i] = px;
+    v.vy[i] = py;
+    v.vz[i] = pz;
+    k3 += px * px + py * py + pz * pz;
+  }
+  k3 = block_sum_dyn(k3, sh);
+  if (threadIdx.x == 0) {
+    st.s2 = 1.0;
+    st.ke_end = k3 * 0.5;
+    next_first_half(d, st, k3);
+  }
+}
+
+// arm a temperature ramp of K steps on system r starting at target T0 (the
+// momenta already rescaled to it by k_rescale), changing by dT per step
+__global__ void k_ramp_begin(View v, int r, double T0, double dT, double T_end, long long K) {
+  if (threadIdx.x != 0) return;
+  const SysDesc &d = v.desc[r];
+  SysState &st = v.st[r];
+  st.ramp_T = T0;
+  st.ramp_dT = dT;
+  st.ramp_end = T_end;
+  st.ramp_left = K;
+  st.ramp_real = K;
+  next_first_half(d, st, 2.0 * st.ke_end);
+}
+
+// lengthen system r's armed ramp to `total` steps; the steps after the ramp
+// itself rescale to its final temperature (lets systems whose ramps differ in
+// length finish together inside one engine)
+__global__ void k_ramp_extend(View v, int r, long long total) {
+  if (threadIdx.x != 0) return;
+  SysState &st = v.st[r];
+  if (st.ramp_left > 0 && total > st.ramp_left) {
+    if (st.ramp_real <= 0) st.ramp_T = st.ramp_end;
+    st.ramp_left = total;
+  }
+}
+
+// GetFccGrid (MDcode/initialise.c:34-101) placement of system r's particles on
+// the reference's near-cubic grid: particle k goes to grid site site[k] of
+// troot^3 sites (troot = the smallest integer with troot^3 >= N), with the
+// reference's arithmetic (the y and z coordinates use floating divisions);
+// types and momenta come from the host.  Reads the staged upload of
+// acg_set_lattice and writes the staged x = xu for k_load.
+__global__ void k_lattice(View v, int r, int troot) {
+  const SysDesc &d = v.desc[r];
+  double *s = v.stage_d + 9 * (size_t)d.poff;
+  const int *site = v.stage_i + 2 * (size_t)d.poff + (size_t)d.n;  // act tags follow at k_load time
+  const double dr = 1.0 / (double)troot;  // LENGTH / troot_n
+  const int t2 = troot * troot;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < d.n; k += gridDim.x * blockDim.x) {
+    const int i = site[k];
+    const double X = dr * (double)((i % t2) % troot);
+    const double Y = dr * (double)(i % t2) / (double)troot;
+    const double Z = dr * (double)(i / (double)t2);
+    s[3 * k] = X;
+    s[3 * k + 1] = Y;
+    s[3 * k + 2] = Z;
+    s[3 * (size_t)d.n + 3 * k] = X;
+    s[3 * (size_t)d.n + 3 * k + 1] = Y;
+    s[3 * (size_t)d.n + 3 * k + 2] = Z;
+  }
 }
 
 // stage 2: forces + second kick.  mode 0 = step; 1 = prime (forces at the
@@ -2150,194 +2505,6 @@ __global__ void __launch_bounds__(BLOCK_X) k_force_box(View v, int mode) {
 }
 
 // ---------------------------------------------------------------------------
-// Whole timesteps of whole-box systems, one block per system: kick/drift and
-// direction shuffle, rebuild decision, cell build and lists when due, pair
-// forces with the second kick, thermostat chain, observables, with block
-// barriers between the phases.  Blocks never wait on one another, so a batch
-// of replicas advances by one launch per step.  Every phase runs the same
-// per-particle arithmetic as the per-phase kernels (shared device functions);
-// only the order of the per-system sums differs (one block sum instead of
-// per-block partials).
-constexpr int BLOCK_F = 512;
-
-template <int TPP, int PREC>
-__global__ void __launch_bounds__(BLOCK_F) k_steps_box(View v, int nsteps) {
-  extern __shared__ __align__(16) unsigned char fsm[];
-  __shared__ int cst[MAX_BOX_CELLS + 1], pre4[MAX_BOX_CELLS + 1], cnt[MAX_BOX_CELLS], fill[MAX_BOX_CELLS];
-  __shared__ double wred[BLOCK_F / 32];
-  __shared__ double s_max;
-  __shared__ int s_rb, s_obs, s_lo, s_hi;
-  __shared__ long long s_step;
-  const int r = blockIdx.x;
-  const SysDesc &d = v.desc[r];
-  SysState &st = v.st[r];
-  const ObsDesc &o = v.obs[r];
-  const int n = d.n, nce = d.ncell, poff = d.poff;
-  const int lane32 = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = BLOCK_F / 32;
-  for (int s = 0; s < nsteps; s++) {
-    if (threadIdx.x == 0) s_step = st.step;
-    __syncthreads();
-    const long long step = s_step;
-    // U3 U2 U1 and the block max of the displacement since the last rebuild
-    {
-      // written by thread 0 in the previous step's thermostat update
-      const double s1 = *reinterpret_cast<volatile const double *>(&st.s1);
-      const double s2 = *reinterpret_cast<volatile const double *>(&st.s2);
-      double m = 0.0;
-      for (int k = threadIdx.x; k < n; k += BLOCK_F) m = fmax(m, kick_drift_one(v, d, poff + k, s1, s2));
-      for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, off));
-      if (lane32 == 0) wred[warp] = m;
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        double mm = wred[0];
-        for (int w = 1; w < nwarp; w++) mm = fmax(mm, wred[w]);
-        s_max = mm;
-      }
-    }
-    // direction shuffle at the persistence steps (MDcode/main.c:245)
-    if (d.shuffle && d.nact > 0 && d.tau_p > 0 && (step % d.tau_p) == 0)
-      for (int comp = 0; comp < 3; comp++) {
-        shuffle_component(v, r, comp, step);
-        __syncthreads();
-      }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      s_rb = rebuild_decision(d, st, s_max);
-      s_obs = obs_due(o, st);
-      s_lo = st.obs_lo;
-      s_hi = st.obs_hi;
-      if (s_rb) st.overflow = 0;
-    }
-    __syncthreads();
-    if (s_rb) {
-      // cells: count, scan, scatter, order by particle index, permute
-      for (int c = threadIdx.x; c < nce; c += BLOCK_F) {
-        cnt[c] = 0;
-        fill[c] = 0;
-      }
-      __syncthreads();
-      for (int k = threadIdx.x; k < n; k += BLOCK_F) {
-        const int i = poff + k;
-        const double4 p = v.pos[i];
-        const int c = cell_coord(p.x, d.inv_cell, d.nc) + cell_coord(p.y, d.inv_cell, d.nc) * d.nc +
-                      cell_coord(p.z, d.inv_cell, d.nc) * d.nc * d.nc;
-        v.cell_tmp[i] = c;
-        atomicAdd(&cnt[c], 1);
-      }
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        int run = 0, run4 = 0;
-        for (int c = 0; c < nce; c++) {
-          cst[c] = run;
-          pre4[c] = run4;
-          run += cnt[c];
-          run4 += (cnt[c] + 3) & ~3;
-        }
-        cst[nce] = run;
-        pre4[nce] = run4;
-      }
-      __syncthreads();
-      for (int c = threadIdx.x; c < nce; c += BLOCK_F) {
-        v.cstart[d.coff + c] = cst[c];
-        v.ccount[d.coff + c] = cnt[c];
-      }
-      for (int k = threadIdx.x; k < n; k += BLOCK_F) {
-        const int i = poff + k;
-        const int c = v.cell_tmp[i];
-        v.perm_u[poff + cst[c] + atomicAdd(&fill[c], 1)] = i;
-      }
-      __syncthreads();
-      for (int c = warp; c < nce; c += nwarp) {
-        const int m = cnt[c], base = poff + cst[c];
-        for (int a0 = 0; a0 < m; a0 += 32) {
-          const int a = a0 + lane32;
-          int sa = -1, ida = 0x7fffffff;
-          if (a < m) {
-            sa = v.perm_u[base + a];
-            ida = v.id[sa];
-          }
-          int rank = 0;
-          for (int b0 = 0; b0 < m; b0 += 32) {
-            const int b = b0 + lane32;
-            const int idb = b < m ? v.id[v.perm_u[base + b]] : 0x7fffffff;
-#pragma unroll 8
-            for (int q = 0; q < 32; q++) rank += __shfl_sync(0xffffffffu, idb, q) < ida;
-          }
-          if (a < m) {
-            v.perm[base + rank] = sa;
-            v.cellof[base + rank] = c;
-          }
-        }
-      }
-      __syncthreads();
-      for (int k = threadIdx.x; k < n; k += BLOCK_F) {
-        const int i = poff + k, q = v.perm[i];
-        v.pos_s[i] = v.pos[q];
-        v.ux_s[i] = v.ux[q];
-        v.uy_s[i] = v.uy[q];
-        v.uz_s[i] = v.uz[q];
-        v.vx_s[i] = v.vx[q];
-        v.vy_s[i] = v.vy[q];
-        v.vz_s[i] = v.vz[q];
-        v.fx_s[i] = v.fx[q];
-        v.fy_s[i] = v.fy[q];
-        v.fz_s[i] = v.fz[q];
-        v.id_s[i] = v.id[q];
-        v.act_s[i] = v.act[q];
-      }
-      __syncthreads();
-      box_stage_list(v, d, reinterpret_cast<float4 *>(fsm), cst, pre4);
-      __syncthreads();
-      for (int c = warp; c < nce; c += nwarp)
-        box_list_cell(v, d, r, reinterpret_cast<const float4 *>(fsm), cst, pre4, c, lane32, 0, 1);
-      __syncthreads();
-      for (int k = threadIdx.x; k < n; k += BLOCK_F) copy_back(v, poff + k);
-      if (threadIdx.x == 0) st.rebuilds += 1;
-      __syncthreads();
-    }
-    // pair forces, active force, second half kick; sums; thermostat chain
-    box_stage_force<PREC>(v, d, fsm);
-    __syncthreads();
-    {
-      double pe = 0.0, vir = 0.0, ke = 0.0, va = 0.0;
-      const int lane = threadIdx.x % TPP;
-      for (int t0 = 0; t0 < n; t0 += BLOCK_F / TPP) {
-        const int sl = t0 + threadIdx.x / TPP;
-        const bool valid = sl < n;
-        const int i = poff + (valid ? sl : 0);
-        const PairAcc a = box_pairs<TPP, PREC>(v, d, fsm, valid, sl, i, lane);
-        if (valid && lane == 0) particle_epilogue(v, d, st, i, 0, a, pe, vir, ke, va);
-      }
-      pe = block_sum_dyn(pe, wred);
-      vir = block_sum_dyn(vir, wred);
-      ke = block_sum_dyn(ke, wred);
-      va = block_sum_dyn(va, wred);
-      if (threadIdx.x == 0) finalize_sums(d, st, 0, pe, vir, ke, va);
-    }
-    __syncthreads();
-    // observables due at this step
-    if (s_obs) {
-      for (int e = s_lo; e < s_hi; e++) {
-        const int info = o.ev_info[e];
-        double val[OBS_NV] = {0.0, 0.0, 0.0, 0.0, 0.0};
-        for (int k = threadIdx.x; k < n; k += BLOCK_F) {
-          const int i = poff + k;
-          double w[OBS_NV] = {0.0, 0.0, 0.0, 0.0, 0.0};
-          obs_particle(o, n, info, v.id[i], v.ux[i], v.uy[i], v.uz[i], d.L, w);
-          for (int q = 0; q < OBS_NV; q++) val[q] += w[q];
-        }
-        if ((info & 1) == 0) {
-          double sum[OBS_NV];
-          for (int q = 0; q < OBS_NV; q++) sum[q] = block_sum_dyn(val[q], wred);
-          if (threadIdx.x == 0) obs_accumulate(o, n, info, sum);
-        }
-        __syncthreads();
-      }
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
 // device-side step loop control (a graph's WHILE node): one block of steps done
 __global__ void k_loop_ctl(long long *count, cudaGraphConditionalHandle h) {
   if (threadIdx.x == 0) {
@@ -2407,23 +2574,7 @@ __global__ void k_unload(View v, int r) {
 // recompute the next step's first thermostat half after a host change of the
 // chain or temperature (single thread per system)
 __global__ void k_prehalf(View v, int r) {
-  const SysDesc &d = v.desc[r];
-  SysState &st = v.st[r];
-  if (!d.thermostat) {
-    st.s1 = 1.0;
-    return;
-  }
-  double eta[NHC_M], pet[NHC_M];
-  for (int k = 0; k < NHC_M; k++) {
-    eta[k] = st.eta_end[k];
-    pet[k] = st.p_eta_end[k];
-  }
-  double s1 = nhc_half(eta, pet, d.q, d.T, d.dof, d.dt, 2.0 * st.ke_end);
-  for (int k = 0; k < NHC_M; k++) {
-    st.eta_cur[k] = eta[k];
-    st.p_eta_cur[k] = pet[k];
-  }
-  st.s1 = s1;
+  if (threadIdx.x == 0) next_first_half(v.desc[r], v.st[r], 2.0 * v.st[r].ke_end);
 }
 
 __global__ void k_shuffle_now(View v, int r) { shuffle_component(v, r, blockIdx.x, v.st[r].step); }

@@ -185,7 +185,42 @@ class Engine:
         return k[: 3 * na].reshape(3, na)
 
     def shuffle(self, sys: int = 0):
+        """ShuffleActDirec now (MDcode/active.c:45-85)."""
         check(self._lib.acg_shuffle_directions(self.h, sys))
+
+    def seed_shuffle(self, sys: int, seed: int):
+        """Reseed the system's MT19937 direction stream (gsl_rng_set)."""
+        check(self._lib.acg_seed_shuffle(self.h, sys, C.c_uint64(int(seed))))
+
+    def fix_drift(self, sys: int = 0):
+        """fixDrift now (MDcode/initialise.c:104-138)."""
+        check(self._lib.acg_fix_drift(self.h, sys))
+
+    def adjust_temperature(self, sys: int, T: float) -> float:
+        """adjustInitialTemp (MDcode/initialise.c:141-151); returns inst_T after."""
+        t = C.c_double()
+        check(self._lib.acg_adjust_temperature(self.h, sys, float(T), C.byref(t)))
+        return t.value
+
+    def start_ramp(self, sys: int, T_start: float, T_end: float, rate: float) -> int:
+        """Arm a coldstart / breakxal ramp (MDcode/initialise.c:166-201); returns
+        its step count (the ramp runs in the next that many steps)."""
+        k = C.c_int64()
+        check(self._lib.acg_start_ramp(self.h, sys, float(T_start), float(T_end), float(rate), C.byref(k)))
+        return int(k.value)
+
+    def extend_ramp(self, sys: int, total_steps: int):
+        """Pad an armed ramp to total_steps (the extra steps hold its end T)."""
+        check(self._lib.acg_extend_ramp(self.h, sys, int(total_steps)))
+
+    def set_lattice(self, sys: int, site, type_, p, act_tag):
+        """GetFccGrid placement on the device from the caller's grid sites."""
+        n = self.n(sys)
+        si = _i32(site, (n,))
+        t = _i32(type_, (n,))
+        pp = _f64(p, (n, 3))
+        a = _i32(act_tag, (n,))
+        check(self._lib.acg_set_lattice(self.h, sys, _ptr(si), _ptr(t), _ptr(pp), _ptr(a)))
 
     def set_nhc(self, sys: int, eta, p_eta):
         e = _f64(eta, (3,))

@@ -75,6 +75,7 @@ acg_engine *acg_legacy_engine(int nve) {
     p.list_mode = 0;
     p.thermostat = nve ? 0 : 1;
     p.shuffle = 0; /* ShuffleActDirec stays the program's own (host RNG) */
+    p.drift_every = 0; /* fixDrift stays the program's own call (MDcode/main.c:261) */
     const char *prec = getenv("ACG_PRECISION");
     if (prec && strcmp(prec, "fp32") == 0) p.precision = ACG_PREC_FP32;
     const char *dev = getenv("ACG_DEVICE");

@@ -58,15 +58,24 @@ typedef struct acg_params {
                              1: list cut 2.5*sigma_ab+skin per type pair */
   int thermostat;         /* 1: Nose-Hoover chain NVT (AdvanceTimeNVTNoseHoover);
                              0: NVE velocity Verlet (advance_time_NVEFrog) */
-  int shuffle;            /* 1: re-randomise active directions on the device every
-                             tau_p_steps steps (ShuffleActDirec cadence, MDcode/main.c:245);
+  int shuffle;            /* re-randomise the active directions every tau_p_steps steps
+                             (ShuffleActDirec cadence, MDcode/main.c:245-247):
+                             1: on the device in the reference's order (per component,
+                                swap k[i] with k[(int)(Nact*u)], MDcode/active.c:58-75)
+                                on an MT19937 stream seeded like gsl_rng_set(seed), so
+                                the directions equal the reference's for the same seed;
+                             2: a uniformly random permutation per component (parallel,
+                                not the reference's distribution);
                              0: the caller sets them (acg_set_directions) */
   int precision;          /* ACG_PREC_FP64 or ACG_PREC_FP32 */
   int nb_capacity;        /* neighbour-list row capacity; 0 = automatic.  Particles
                              with more neighbours are served from the cell list
                              (the reference's MaxNeibs, MDcode/global.h:19, is
                              unchecked) */
-  uint64_t seed;          /* device direction-shuffle stream */
+  uint64_t seed;          /* direction-shuffle stream (gsl_rng_set seed; 0 is taken as 4357) */
+  int drift_every;        /* remove the mean momentum (fixDrift, MDcode/initialise.c:104-138)
+                             after every step whose index is a multiple of this, as run()
+                             does every 100000 steps (MDcode/main.c:261); 0 = never */
 } acg_params;
 
 /* Scalars of one system at the last step boundary. */
@@ -129,10 +138,48 @@ int acg_get_state(acg_engine *e, int sys, double *x, double *xu, double *p, doub
 int acg_set_directions(acg_engine *e, int sys, const int *k);
 int acg_get_directions(acg_engine *e, int sys, int *k);
 
-/* Re-randomise one system's directions now on the device (a uniformly random
- * permutation per component, keeping the +1/-1 counts): ShuffleActDirec,
- * MDcode/active.c:45-85. */
+/* Re-randomise one system's directions now on the device: ShuffleActDirec,
+ * MDcode/active.c:45-85, in the reference's order on the system's MT19937
+ * stream (shuffle modes 0 and 1), or a uniformly random permutation per
+ * component (mode 2). */
 int acg_shuffle_directions(acg_engine *e, int sys);
+/* Reseed one system's MT19937 direction stream: gsl_rng_set(rng_ptr, seed)
+ * of initializeGsl (MDcode/initialise.c:5-11). */
+int acg_seed_shuffle(acg_engine *e, int sys, uint64_t seed);
+
+/* fixDrift (MDcode/initialise.c:104-138) now: subtract the mean momentum of
+ * one system (acg_step also does it by itself every drift_every steps). */
+int acg_fix_drift(acg_engine *e, int sys);
+
+/* adjustInitialTemp (MDcode/initialise.c:141-151): scale one system's momenta
+ * by sqrt(T / inst_T); *inst_T (may be NULL) receives the temperature after
+ * the scaling (calculate_temp, :153-164). */
+int acg_adjust_temperature(acg_engine *e, int sys, double T, double *inst_T);
+
+/* The heating and cooling ramps of initialisation, coldstart and breakxal
+ * (MDcode/initialise.c:166-201): rescale one system's momenta to T_start now,
+ * then, for each of the next *steps steps of that system, rescale to the ramp
+ * temperature (starting at the temperature reached, changing by
+ * dt * rate per step towards T_end until it passes T_end) and take one NVE
+ * leap-frog step (advance_time_NVEFrog, MDcode/time_evolve.c:104-171).  The
+ * ramp steps run inside the following acg_step calls; during them the
+ * system's step counter, direction shuffles, drift removal and observables
+ * wait.  coldstart(rate, T) = acg_start_ramp(e, s, 0.5 T, T, rate, ..);
+ * breakxal(rate, T) = acg_start_ramp(e, s, 1.5 T, T, rate, ..). */
+int acg_start_ramp(acg_engine *e, int sys, double T_start, double T_end, double rate, int64_t *steps);
+/* Lengthen one system's armed ramp to total_steps steps: the steps after the
+ * ramp itself rescale to T_end, so systems whose ramps differ in length can
+ * run them inside one engine and finish together.  No counterpart in the
+ * reference (one system per program). */
+int acg_extend_ramp(acg_engine *e, int sys, int64_t total_steps);
+
+/* GetFccGrid placement (MDcode/initialise.c:34-101) on the device: particle k
+ * at grid site site[k] of the troot^3 grid (troot = smallest integer with
+ * troot^3 >= n), positions with the reference's arithmetic, xu = x; type,
+ * momenta p [n][3] and act_tag as acg_set_state.  The random choices (sites,
+ * types, momenta) are the caller's, e.g. the reference's rand() draws. */
+int acg_set_lattice(acg_engine *e, int sys, const int *site, const int *type, const double *p,
+                    const int *act_tag);
 
 /* Thermostat chain state (InitialiseNoseHoover, MDcode/time_evolve.c:476-493:
  * eta = 0, p_eta drawn by the caller).  q follows from T and n. */

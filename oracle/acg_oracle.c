@@ -36,6 +36,7 @@ typedef struct {
   int idx;
 } mt_state;
 static void mt_seed(mt_state *r, unsigned long seed) {
+  if (seed == 0) seed = 4357; /* gsl_rng_set for mt19937 */
   r->mt[0] = (unsigned int)(seed & 0xffffffffUL);
   for (int i = 1; i < 624; i++) {
     unsigned int p = r->mt[i - 1];
@@ -529,14 +530,76 @@ static int nvt_step(ora_sys *s) {
   return rb;
 }
 
-/* run() loop body (MDcode/main.c:244-248) */
-int ora_run(ora_sys *s, long start, int nsteps, int do_shuffle) {
+/* fixDrift (MDcode/initialise.c:104-138): subtract the mean momentum, the
+ * sums taken over the particles in index order, one component at a time */
+void ora_fix_drift(ora_sys *s) {
+  double P[3] = {0.0, 0.0, 0.0};
+  for (int i = 0; i < s->n; i++) {
+    P[0] += s->px[i];
+    P[1] += s->py[i];
+    P[2] += s->pz[i];
+  }
+  for (int k = 0; k < 3; k++) P[k] = P[k] / (double)s->n;
+  for (int i = 0; i < s->n; i++) {
+    s->px[i] -= P[0];
+    s->py[i] -= P[1];
+    s->pz[i] -= P[2];
+  }
+}
+
+/* run() loop body (MDcode/main.c:244-265): ShuffleActDirec every TAU_per
+ * steps, the step, and fixDrift after every 100000th step when do_drift */
+int ora_run(ora_sys *s, long start, int nsteps, int do_shuffle, int do_drift) {
   int rebuilds = 0;
   for (long i = start; i < start + nsteps; i++) {
     if (do_shuffle && !(i % s->tau_p)) ora_shuffle(s);
     rebuilds += nvt_step(s);
+    if (do_drift && i % 100000 == 0) ora_fix_drift(s);
   }
   return rebuilds;
+}
+
+/* calculate_temp (MDcode/initialise.c:153-164) */
+static double inst_temp(ora_sys *s) {
+  double kb = 0.0;
+  for (int i = 0; i < s->n; i++) kb += s->px[i] * s->px[i] + s->py[i] * s->py[i] + s->pz[i] * s->pz[i];
+  s->ke = kb * 0.5;
+  s->inst_T = 2.0 * s->ke / s->dof;
+  return s->inst_T;
+}
+
+/* adjustInitialTemp (MDcode/initialise.c:141-151); returns inst_T after */
+double ora_adjust_temp(ora_sys *s, double T) {
+  double xi = sqrt(T / inst_temp(s));
+  for (int i = 0; i < s->n; i++) {
+    s->px[i] = s->px[i] * xi;
+    s->py[i] = s->py[i] * xi;
+    s->pz[i] = s->pz[i] * xi;
+  }
+  return inst_temp(s);
+}
+
+/* coldstart / breakxal (MDcode/initialise.c:166-201): rescale to T_start,
+ * rebuild and compute forces, then while T has not reached T_end (T < T_end
+ * heating, T > T_end cooling): rescale to T, one NVE leap-frog step,
+ * T +- time_step * rate.  Returns the number of ramp steps. */
+long ora_ramp(ora_sys *s, double T_start, double T_end, double rate) {
+  double T = ora_adjust_temp(s, T_start);
+  const int heat = T_end > T_start;
+  ora_rebuild(s);
+  compute_forces(s);
+  long k = 0;
+  while (heat ? T < T_end : T > T_end) {
+    inst_temp(s);
+    ora_adjust_temp(s, T);
+    ora_run_nve(s, 1);
+    if (heat)
+      T += TIME_STEP * rate;
+    else
+      T -= TIME_STEP * rate;
+    k++;
+  }
+  return k;
 }
 
 /* advance_time_NVEFrog (MDcode/time_evolve.c:104-171) */

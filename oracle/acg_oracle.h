@@ -38,7 +38,10 @@ void ora_seed_rng(ora_sys *s, unsigned long seed);
 void ora_shuffle(ora_sys *s);
 void ora_rebuild(ora_sys *s);
 void ora_forces(ora_sys *s, double *F, double *out3);
-int ora_run(ora_sys *s, long start, int nsteps, int do_shuffle);
+int ora_run(ora_sys *s, long start, int nsteps, int do_shuffle, int do_drift);
+void ora_fix_drift(ora_sys *s);
+double ora_adjust_temp(ora_sys *s, double T);
+long ora_ramp(ora_sys *s, double T_start, double T_end, double rate);
 int ora_run_nve(ora_sys *s, int nsteps);
 void ora_get_scalars(const ora_sys *s, double *out6);
 int ora_get_cells(const ora_sys *s, int *dims, int *counts, int *members);

@@ -75,7 +75,12 @@ def _oracle_lib():
         lib.ora_rebuild.argtypes = [v]
         lib.ora_forces.argtypes = [v, _dp, _dp]
         lib.ora_run.restype = C.c_int
-        lib.ora_run.argtypes = [v, C.c_long, C.c_int, C.c_int]
+        lib.ora_run.argtypes = [v, C.c_long, C.c_int, C.c_int, C.c_int]
+        lib.ora_fix_drift.argtypes = [v]
+        lib.ora_adjust_temp.restype = C.c_double
+        lib.ora_adjust_temp.argtypes = [v, C.c_double]
+        lib.ora_ramp.restype = C.c_long
+        lib.ora_ramp.argtypes = [v, C.c_double, C.c_double, C.c_double]
         lib.ora_run_nve.restype = C.c_int
         lib.ora_run_nve.argtypes = [v, C.c_int]
         lib.ora_get_scalars.argtypes = [v, _dp]
@@ -190,11 +195,20 @@ class Oracle(_Common):
     def rebuild(self):
         self._call("rebuild")
 
-    def run(self, nsteps, start=0, shuffle=False):
-        return self._call("run", int(start), int(nsteps), int(bool(shuffle)))
+    def run(self, nsteps, start=0, shuffle=False, drift=False):
+        return self._call("run", int(start), int(nsteps), int(bool(shuffle)), int(bool(drift)))
 
     def run_nve(self, nsteps):
         return self._call("run_nve", int(nsteps))
+
+    def fix_drift(self):
+        self._call("fix_drift")
+
+    def adjust_temp(self, T):
+        return self._call("adjust_temp", float(T))
+
+    def ramp(self, T_start, T_end, rate=0.1):
+        return self._call("ramp", float(T_start), float(T_end), float(rate))
 
     @staticmethod
     def cell_geometry(L):
@@ -243,7 +257,14 @@ class Reference(_Common):
             lib.ref_seed_rng.argtypes = [C.c_ulong]
             lib.ref_forces.argtypes = [_dp, _dp]
             lib.ref_run.restype = C.c_int
-            lib.ref_run.argtypes = [C.c_long, C.c_int, C.c_int]
+            lib.ref_run.argtypes = [C.c_long, C.c_int, C.c_int, C.c_int]
+            lib.ref_adjust_temp.restype = C.c_double
+            lib.ref_adjust_temp.argtypes = [C.c_double]
+            lib.ref_coldstart.argtypes = [C.c_double, C.c_double]
+            lib.ref_breakxal.argtypes = [C.c_double, C.c_double]
+            lib.ref_initialize_system.restype = C.c_int
+            lib.ref_initialize_system.argtypes = [C.c_double, C.c_double, C.c_double, C.c_int, C.c_uint,
+                                                  C.c_char_p]
             lib.ref_run_nve.restype = C.c_int
             lib.ref_run_nve.argtypes = [C.c_int]
             lib.ref_get_scalars.argtypes = [_dp]
@@ -281,8 +302,28 @@ class Reference(_Common):
     def rebuild(self):
         self.lib.ref_rebuild()
 
-    def run(self, nsteps, start=0, shuffle=False):
-        return self.lib.ref_run(int(start), int(nsteps), int(bool(shuffle)))
+    def run(self, nsteps, start=0, shuffle=False, drift=False):
+        return self.lib.ref_run(int(start), int(nsteps), int(bool(shuffle)), int(bool(drift)))
+
+    def fix_drift(self):
+        self.lib.ref_fix_drift()
+
+    def adjust_temp(self, T):
+        return self.lib.ref_adjust_temp(float(T))
+
+    def coldstart(self, rate, T):
+        self.lib.ref_coldstart(float(rate), float(T))
+
+    def breakxal(self, rate, T):
+        self.lib.ref_breakxal(float(rate), float(T))
+
+    def initialize_system(self, T, f0, jobno, srand_seed, workdir, density=1.2):
+        """The reference's fresh-start initialisation (lattice, active set,
+        coldstart, breakxal); once per process and particle count."""
+        rc = self.lib.ref_initialize_system(float(density), float(T), float(f0), int(jobno), int(srand_seed),
+                                            str(workdir).encode())
+        if rc:
+            raise RuntimeError("the reference's arrays are already set up in this process")
 
     def run_nve(self, nsteps):
         return self.lib.ref_run_nve(int(nsteps))

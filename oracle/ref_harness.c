@@ -26,6 +26,9 @@
  */
 #include "global.h"
 #include "subroutine.h"
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 extern unsigned long long int *nextStepIndex; /* MDcode/main.c:4 */
@@ -153,17 +156,62 @@ void ref_get_nhc(double *out) {
   }
 }
 
-/* run() body (MDcode/main.c:244-248) for steps [start, start+nsteps).
- * Returns the number of steps that rebuilt the cell/neighbour lists, i.e.
- * took the 3*maxmaxD > skin^2 branch (MDcode/time_evolve.c:508). */
-int ref_run(long start, int nsteps, int do_shuffle) {
+/* run() body (MDcode/main.c:244-265) for steps [start, start+nsteps):
+ * ShuffleActDirec every TAU_per steps, the step, and (do_drift) fixDrift after
+ * every 100000th step.  Returns the number of steps that rebuilt the
+ * cell/neighbour lists, i.e. took the 3*maxmaxD > skin^2 branch
+ * (MDcode/time_evolve.c:508). */
+int ref_run(long start, int nsteps, int do_shuffle, int do_drift) {
   int rebuilds = 0;
   for (long i = start; i < start + nsteps; i++) {
     if (do_shuffle && !(i % TAU_per)) ShuffleActDirec();
     AdvanceTimeNVTNoseHoover();
     if (3.0 * maxmaxD > skin * skin) rebuilds++;
+    if (do_drift && i % 100000 == 0) fixDrift();
   }
   return rebuilds;
+}
+
+/* fixDrift (MDcode/initialise.c:104-138) */
+void ref_fix_drift(void) { fixDrift(); }
+
+/* adjustInitialTemp (MDcode/initialise.c:141-151); returns inst_T after */
+double ref_adjust_temp(double Tset) {
+  adjustInitialTemp(Tset);
+  return inst_T;
+}
+
+/* coldstart / breakxal (MDcode/initialise.c:166-201) with the reference's
+ * global T left at final_temp afterwards, as they leave it */
+void ref_coldstart(double rate, double final_temp) { coldstart(rate, final_temp); }
+void ref_breakxal(double rate, double final_temp) { breakxal(rate, final_temp); }
+
+/* initializeSystem (MDcode/initialise.c:203-227) as main() runs it for a fresh
+ * start (MDcode/main.c:462-472): box from N and the density, srand(srand_seed),
+ * then the random lattice, the active particles, coldstart and breakxal at T.
+ * dir receives the files the routine writes (ini.dat, ActiveFileIndex.dat). */
+int ref_initialize_system(double density, double Tset, double f0set, int job, unsigned int srand_seed,
+                          const char *dir) {
+  /* initializeSystem allocates the reference's arrays, once per process */
+  if (arrays_ready) return -1;
+  node = 0;
+  Nprocs = 1;
+  jobno = job;
+  DENSITY = density;
+  T = Tset;
+  f0 = f0set;
+  snprintf(sub_dir, sizeof(sub_dir), "%s", dir);
+  L = pow((double)N / DENSITY, 0.33333333);
+  inv_L = 1.0 / L;
+  if (!xold) {
+    xold = calloc(N, sizeof(double));
+    yold = calloc(N, sizeof(double));
+    zold = calloc(N, sizeof(double));
+  }
+  srand(srand_seed);
+  initializeSystem();
+  arrays_ready = 1;
+  return 0;
 }
 
 int ref_run_nve(int nsteps) {

@@ -19,6 +19,7 @@ gsl_rng *gsl_rng_alloc(const gsl_rng_type *t) {
 }
 
 void gsl_rng_set(gsl_rng *r, unsigned long int seed) {
+  if (seed == 0) seed = 4357; /* GSL's mt19937 takes seed 0 as 4357 */
   r->mt[0] = (unsigned int)(seed & 0xffffffffUL);
   for (int i = 1; i < 624; i++) {
     unsigned int p = r->mt[i - 1];
