@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -34,6 +35,7 @@ int fail(int code, const std::string &msg) {
 
 constexpr double TAU_T = 0.20;  // MDcode/time_evolve.c:477
 constexpr int GRAPH_STEPS = 32;
+constexpr int BENCH_MAX_GRAPH = 256;  // acg_bench_steps: one graph for up to this many steps
 
 struct Layout {
   int nsys = 0, nslots = 0, ncells = 0, nact = 0, maxnb = 0, ngroups = 0, nboxtiles = 0, box_nmax = 0;
@@ -238,6 +240,8 @@ struct acg_engine {
   bool no_while = false;  // the device loop could not be built: launch per 32 steps
   void *flush = nullptr;  // bench-only L2 flush buffer
   size_t flush_bytes = 0;
+  std::map<int, std::pair<cudaGraph_t, cudaGraphExec_t>> bench;  // acg_bench_steps: graphs by step count
+  std::vector<std::vector<long long>> obs_events;  // per system: steps with observable events (sorted)
   std::vector<std::vector<void *>> obs_bufs;  // per system: device buffers of the observables
   std::vector<std::vector<long long>> obs_offsets;  // per system: offset (steps) of each time bin
 };
@@ -338,6 +342,11 @@ void drop_graphs(acg_engine *e) {
   e->gexec = e->gexec1 = nullptr;
   e->graph = e->graph1 = nullptr;
   e->gsteps = 0;
+  for (auto &b : e->bench) {
+    cudaGraphExecDestroy(b.second.second);
+    cudaGraphDestroy(b.second.first);
+  }
+  e->bench.clear();
   for (int k = 0; k < 3; k++) {
     if (e->wexec[k]) cudaGraphExecDestroy(e->wexec[k]);
     if (e->wgraph[k]) cudaGraphDestroy(e->wgraph[k]);
@@ -389,6 +398,8 @@ void retire_graphs(acg_engine *e) {
   std::lock_guard<std::mutex> lk(g_retire_mu);
   g_retired.push_back({e->device, e->gexec, e->graph, nullptr, ""});
   g_retired.push_back({e->device, e->gexec1, e->graph1, nullptr, ""});
+  for (auto &b : e->bench) g_retired.push_back({e->device, b.second.second, b.second.first, nullptr, ""});
+  e->bench.clear();
   e->gexec = e->gexec1 = nullptr;
   e->graph = e->graph1 = nullptr;
   for (int k = 0; k < 3; k++) {
@@ -936,6 +947,7 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   e->dirty.assign(nsys, 1);
   e->obs_bufs.assign(nsys, {});
   e->obs_offsets.assign(nsys, {});
+  e->obs_events.assign(nsys, {});
   e->any_dirty = true;
   if (cudaStreamSynchronize(e->stream) != cudaSuccess)
     return cleanup_fail(fail(ACG_ERR_CUDA, "set-up synchronisation failed"));
@@ -1615,6 +1627,8 @@ int acg_obs_configure(acg_engine *e, int sys, const acg_obs_config *c) {
   CK(cudaMemcpyAsync(&e->v.st[sys].obs_cur, &zero, sizeof(int), cudaMemcpyHostToDevice, e->stream));
   CK(cudaStreamSynchronize(e->stream));
   e->obs_offsets[sys] = offs;
+  e->obs_events[sys].assign(h_step.begin(), h_step.end());
+  e->obs_events[sys].erase(std::unique(e->obs_events[sys].begin(), e->obs_events[sys].end()), e->obs_events[sys].end());
   return ACG_OK;
 }
 
@@ -1640,15 +1654,27 @@ int acg_obs_sums(acg_engine *e, int sys, int *nbins, int64_t *offset, double *su
   return ACG_OK;
 }
 
-int acg_bench_steps(acg_engine *e, int nchunks, size_t flush_bytes, double *ms, int64_t *launches) {
-  if (!e || nchunks < 1 || !ms) return fail(ACG_ERR_INVALID, "bad arguments");
+int acg_bench_steps(acg_engine *e, int64_t nsteps, size_t flush_bytes, double *ms, int64_t *launches) {
+  if (!e || nsteps < 1 || !ms) return fail(ACG_ERR_INVALID, "bad arguments");
   CK(cudaSetDevice(e->device));
   int rc = prime(e);
   if (rc) return rc;
-  if (!e->gexec) {
-    rc = build_graph(e, GRAPH_STEPS, &e->graph, &e->gexec);
+  // exactly nsteps steps: one graph of nsteps steps when that is short, else
+  // graphs of GRAPH_STEPS steps and one of the remainder
+  std::vector<int> plan;
+  if (nsteps <= BENCH_MAX_GRAPH) {
+    plan.push_back((int)nsteps);
+  } else {
+    for (int64_t k = 0; k < nsteps / GRAPH_STEPS; k++) plan.push_back(GRAPH_STEPS);
+    if (nsteps % GRAPH_STEPS) plan.push_back((int)(nsteps % GRAPH_STEPS));
+  }
+  for (int K : plan) {
+    if (e->bench.count(K)) continue;
+    cudaGraph_t g;
+    cudaGraphExec_t x;
+    rc = build_graph(e, K, &g, &x);
     if (rc) return rc;
-    e->gsteps = GRAPH_STEPS;
+    e->bench[K] = {g, x};
   }
   if (flush_bytes > e->flush_bytes) {
     if (e->flush) cudaFree(e->flush);
@@ -1657,38 +1683,53 @@ int acg_bench_steps(acg_engine *e, int nchunks, size_t flush_bytes, double *ms, 
     CK(cudaMalloc(&e->flush, flush_bytes));
     e->flush_bytes = flush_bytes;
   }
-  std::vector<long long> rb0(e->lay.nsys);
-  for (int r = 0; r < e->lay.nsys; r++)
-    CK(cudaMemcpyAsync(&rb0[r], &e->v.st[r].rebuilds, sizeof(long long), cudaMemcpyDeviceToHost, e->stream));
-  std::vector<cudaEvent_t> ev(2 * nchunks);
+  const int nsys = e->lay.nsys;
+  std::vector<SysState> st0(nsys), st1(nsys);
+  CK(cudaMemcpyAsync(st0.data(), e->v.st, sizeof(SysState) * nsys, cudaMemcpyDeviceToHost, e->stream));
+  const size_t nl = plan.size();
+  std::vector<cudaEvent_t> ev(2 * nl);
   for (auto &x : ev) CK(cudaEventCreate(&x));
-  for (int c = 0; c < nchunks; c++) {
-    if (flush_bytes) CK(cudaMemsetAsync(e->flush, c & 0xff, flush_bytes, e->stream));
+  for (size_t c = 0; c < nl; c++) {
+    if (flush_bytes) CK(cudaMemsetAsync(e->flush, (int)(c & 0xff), flush_bytes, e->stream));
     CK(cudaEventRecord(ev[2 * c], e->stream));
-    CK(cudaGraphLaunch(e->gexec, e->stream));
+    CK(cudaGraphLaunch(e->bench[plan[c]].second, e->stream));
     CK(cudaEventRecord(ev[2 * c + 1], e->stream));
   }
   CK(cudaStreamSynchronize(e->stream));
   double tot = 0;
-  for (int c = 0; c < nchunks; c++) {
+  for (size_t c = 0; c < nl; c++) {
     float t = 0;
     CK(cudaEventElapsedTime(&t, ev[2 * c], ev[2 * c + 1]));
     tot += t;
   }
   for (auto &x : ev) cudaEventDestroy(x);
-  std::vector<long long> rb1(e->lay.nsys);
-  for (int r = 0; r < e->lay.nsys; r++)
-    CK(cudaMemcpy(&rb1[r], &e->v.st[r].rebuilds, sizeof(long long), cudaMemcpyDeviceToHost));
-  // every step launches the kick/drift kernel and one launch of each force
-  // kernel in use; a step whose rebuild conditional fires also launches the
-  // rebuild kernels with a non-empty grid (the node list of build_graph)
-  long long steps_with_rebuild = 0;
-  for (int r = 0; r < e->lay.nsys; r++) steps_with_rebuild = std::max(steps_with_rebuild, rb1[r] - rb0[r]);
-  const long long per_step = 1 + (e->ntiles_g > 0) + (e->ntiles_x > 0) + (e->ntiles_b > 0);
-  const long long per_rebuild = 3 * (e->ntiles_a > 0) + (e->lay.nsys > 0) + (e->ntiles_c > 0) +
-                                (e->ntiles_g > 0) + (e->ntiles_x > 0) + (e->ntiles_l > 0);
+  CK(cudaMemcpy(st1.data(), e->v.st, sizeof(SysState) * nsys, cudaMemcpyDeviceToHost));
   *ms = tot;
-  if (launches) *launches = per_step * GRAPH_STEPS * nchunks + per_rebuild * steps_with_rebuild;
+  if (!launches) return ACG_OK;
+  // kernels launched in the timed graphs: every step the kick/drift kernel
+  // and each force kernel in use; a step whose rebuild branch is taken the
+  // rebuild kernels with a non-empty grid; a step with a reference-order
+  // shuffle the shuffle kernel; a step with a drift removal or observable
+  // events the three kernels of that branch (the node lists of add_steps)
+  const long long per_step = 1 + (e->ntiles_g > 0) + (e->ntiles_x > 0) + (e->ntiles_b > 0);
+  const long long per_rebuild = 5 + (e->lay.box_m3max > 0) + 2 * (e->ntiles_x > 0) + (e->ntiles_g > 0) +
+                                (e->ntiles_l > 0);
+  long long steps_with_rebuild = 0, shuffles = 0, posts = 0;
+  for (int r = 0; r < nsys; r++) steps_with_rebuild = std::max(steps_with_rebuild, st1[r].rebuilds - st0[r].rebuilds);
+  for (long long k = 0; k < nsteps; k++) {
+    bool shuf = false, post = false;
+    for (int r = 0; r < nsys && !(shuf && post); r++) {
+      const SysDesc &d = e->lay.desc[r];
+      const long long step = st0[r].step + k;
+      if (d.shuffle == 1 && d.nact > 0 && d.tau_p > 0 && step % d.tau_p == 0) shuf = true;
+      if (d.drift_every > 0 && step % d.drift_every == 0) post = true;
+      const auto &evs = e->obs_events[r];
+      if (!post && std::binary_search(evs.begin(), evs.end(), step)) post = true;
+    }
+    shuffles += shuf;
+    posts += post;
+  }
+  *launches = per_step * nsteps + per_rebuild * steps_with_rebuild + shuffles + 3 * posts;
   return ACG_OK;
 }
 

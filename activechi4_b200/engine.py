@@ -309,11 +309,12 @@ class Engine:
         check(self._lib.acg_time_stage(self.h, int(stage), int(reps), C.byref(ms)))
         return ms.value
 
-    def bench_steps(self, nchunks: int, flush_bytes: int = 256 << 20):
-        """(device ms summed over the timed 32-step launches, kernel launches)"""
+    def bench_steps(self, nsteps: int, flush_bytes: int = 256 << 20):
+        """(device ms summed over the timed launches of exactly nsteps steps,
+        kernel launches inside them)"""
         ms = C.c_double()
         nl = C.c_int64()
-        check(self._lib.acg_bench_steps(self.h, int(nchunks), int(flush_bytes), C.byref(ms), C.byref(nl)))
+        check(self._lib.acg_bench_steps(self.h, int(nsteps), int(flush_bytes), C.byref(ms), C.byref(nl)))
         return ms.value, nl.value
 
     def prepare(self):

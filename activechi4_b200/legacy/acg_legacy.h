@@ -35,5 +35,12 @@ void acg_legacy_push(acg_engine *e);
 void acg_legacy_pull(acg_engine *e);
 /* print the library's last error and exit, as the reference does on errors */
 void acg_legacy_die(const char *where, int rc);
+/* refresh sphere[] and the step's globals from the device when it is ahead
+ * (the sync points call this before the reference routine runs) */
+void acg_legacy_sync_host(void);
+/* host code may have edited sphere[] / the directions: compare at the next
+ * device call */
+void acg_legacy_host_touched(void);
+void acg_legacy_dirs_touched(void);
 
 #endif

@@ -47,6 +47,7 @@ bool len_check(SPHERE s1, SPHERE s2) {
 /* update_cell_list (MDcode/cell_list+forces.c:58-148) */
 void update_cell_list() {
   acg_engine *e = acg_legacy_current();
+  acg_legacy_sync_host(); /* xold below is taken from sphere[] */
   acg_legacy_push(e);
   int rc = acg_rebuild(e);
   if (rc) acg_legacy_die("acg_rebuild", rc);

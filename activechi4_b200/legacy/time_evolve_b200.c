@@ -1,11 +1,20 @@
 /*
  * time_evolve.c on the GPU: AdvanceTimeNVTNoseHoover, advance_time_NVEFrog,
- * InitialiseNoseHoover, applypbc1/applypbc, and the host<->device mirror of
- * the reference's globals used by the drop-in files (acg_legacy.h).
+ * InitialiseNoseHoover, applypbc1/applypbc, the propagators U1..U4 on the
+ * host mirror, and the host<->device mirror of the reference's globals used
+ * by the drop-in files (acg_legacy.h).
  *
  * Compiled inside a program built from the reference's MDcode sources: it
  * includes that program's global.h (sphere[], N, Nact, L, T, f0, eta, ...).
+ *
+ * Mirror: the device holds the state.  AdvanceTimeNVTNoseHoover, the hot
+ * step, reads back only the step's scalars; sphere[] is refreshed from the
+ * device at the sync points, the routines of the reference that read or
+ * write sphere[] (sync_points_b200.c), and host edits are detected at the
+ * next device call.  With ACG_LEGACY_EAGER defined (a program linked
+ * without the sync-point wrappers), every step mirrors the whole state.
  */
+#include <math.h>
 #include <string.h>
 
 #include "acg_legacy.h"
@@ -19,6 +28,9 @@ static void params_set_skin(acg_params *p, double s) { p->skin = s; }
 
 static acg_engine *eng[2];  /* [0] Nose-Hoover NVT, [1] NVE */
 static acg_engine *owner;   /* the engine whose device state is current */
+static int host_stale;      /* the device has stepped since sphere[] was last refreshed */
+static int host_touched = 1;/* host code may have edited sphere[] since the last push */
+static int dirs_touched = 1;/* host code may have changed kx, ky, kz */
 /* what the device holds, to detect edits of the globals by host code */
 static double *sh_x, *sh_xu, *sh_p;
 static int *sh_type, *sh_act, *sh_k;
@@ -110,8 +122,50 @@ static void gather_host(void) {
   }
 }
 
+void acg_legacy_host_touched(void) {
+  host_touched = 1;
+  dirs_touched = 1;
+}
+
+void acg_legacy_dirs_touched(void) { dirs_touched = 1; }
+
+void acg_legacy_sync_host(void) {
+  if (host_stale && owner) acg_legacy_pull(owner);
+}
+
+static void gather_dirs(void) {
+  for (int a = 0; a < Nact; a++) {
+    b_k[a] = kx[a];
+    b_k[Nact + a] = ky[a];
+    b_k[2 * Nact + a] = kz[a];
+  }
+}
+
 void acg_legacy_push(acg_engine *e) {
   int rc;
+  if (e == owner && !host_touched) {
+    /* nothing on the host has been refreshed or edited since the last push:
+     * only the directions (when a shuffle ran) and the chain can differ */
+    if (Nact > 0 && dirs_touched) {
+      gather_dirs();
+      if (memcmp(b_k, sh_k, sizeof(int) * 3 * Nact)) {
+        rc = acg_set_directions(e, 0, b_k);
+        if (rc) acg_legacy_die("acg_set_directions", rc);
+        memcpy(sh_k, b_k, sizeof(int) * 3 * Nact);
+      }
+    }
+    dirs_touched = 0;
+    if (memcmp(eta, sh_eta, sizeof(sh_eta)) || memcmp(p_eta, sh_peta, sizeof(sh_peta))) {
+      rc = acg_set_nhc(e, 0, eta, p_eta);
+      if (rc) acg_legacy_die("acg_set_nhc", rc);
+      memcpy(sh_eta, eta, sizeof(sh_eta));
+      memcpy(sh_peta, p_eta, sizeof(sh_peta));
+    }
+    return;
+  }
+  /* a different engine, or host code that may have edited sphere[]: the device
+   * holds nothing newer than the host here */
+  acg_legacy_sync_host();
   gather_host();
   const size_t d3 = sizeof(double) * 3 * N;
   const int changed = e != owner || memcmp(b_x, sh_x, d3) || memcmp(b_xu, sh_xu, d3) || memcmp(b_p, sh_p, d3) ||
@@ -152,6 +206,31 @@ void acg_legacy_push(acg_engine *e) {
     memcpy(sh_eta, eta, sizeof(sh_eta));
     memcpy(sh_peta, p_eta, sizeof(sh_peta));
   }
+  host_touched = 0;
+  dirs_touched = 0;
+}
+
+/* the scalar globals a step sets (MDcode/time_evolve.c:495-526) */
+static void pull_scalars(acg_engine *e) {
+  acg_thermo th;
+  int rc = acg_get_thermo(e, 0, &th);
+  if (rc) acg_legacy_die("acg_get_thermo", rc);
+  peblk = th.pe;
+  virialblk = th.virial;
+  vir_actblk = th.vir_act;
+  maxD = th.maxD;
+  maxmaxD = th.maxD;
+  ke = th.ke;
+  inst_T = th.inst_T;
+  if (e == eng[0]) {
+    for (int k = 0; k < M; k++) {
+      eta[k] = th.eta[k];
+      p_eta[k] = th.p_eta[k];
+      q[k] = th.q[k];
+    }
+    memcpy(sh_eta, eta, sizeof(sh_eta));
+    memcpy(sh_peta, p_eta, sizeof(sh_peta));
+  }
 }
 
 void acg_legacy_pull(acg_engine *e) {
@@ -175,23 +254,9 @@ void acg_legacy_pull(acg_engine *e) {
   memcpy(sh_x, b_x, d3);
   memcpy(sh_xu, b_xu, d3);
   memcpy(sh_p, b_p, d3);
-  acg_thermo th;
-  rc = acg_get_thermo(e, 0, &th);
-  if (rc) acg_legacy_die("acg_get_thermo", rc);
-  peblk = th.pe;
-  virialblk = th.virial;
-  vir_actblk = th.vir_act;
-  maxD = th.maxD;
-  maxmaxD = th.maxD;
-  if (e == eng[0]) {
-    for (int k = 0; k < M; k++) {
-      eta[k] = th.eta[k];
-      p_eta[k] = th.p_eta[k];
-      q[k] = th.q[k];
-    }
-    memcpy(sh_eta, eta, sizeof(sh_eta));
-    memcpy(sh_peta, p_eta, sizeof(sh_peta));
-  }
+  pull_scalars(e);
+  host_stale = 0;
+  host_touched = 1; /* the caller may edit what it now sees */
 }
 
 /* applypbc1 / applypbc (MDcode/time_evolve.c:15-37): host wrap of sphere[],
@@ -250,13 +315,14 @@ void AdvanceTimeNVTNoseHoover() {
   acg_legacy_push(e);
   int rc = acg_step(e, 1);
   if (rc) acg_legacy_die("acg_step", rc);
-  acg_legacy_pull(e);
+  owner = e;
   Heff = 0;
-  acg_thermo th;
-  rc = acg_get_thermo(e, 0, &th);
-  if (rc) acg_legacy_die("acg_get_thermo", rc);
-  ke = th.ke;
-  inst_T = th.inst_T;
+#ifdef ACG_LEGACY_EAGER
+  acg_legacy_pull(e);
+#else
+  pull_scalars(e); /* sphere[] follows at the next sync point */
+  host_stale = 1;
+#endif
 }
 
 /* advance_time_NVEFrog (MDcode/time_evolve.c:104-171): one velocity-Verlet
@@ -266,9 +332,81 @@ void advance_time_NVEFrog() {
   acg_legacy_push(e);
   int rc = acg_step(e, 1);
   if (rc) acg_legacy_die("acg_step", rc);
+  /* the ramps of initialise.c read sphere[] between these steps from inside
+   * their own file (no sync point): always mirror the whole state */
   acg_legacy_pull(e);
-  acg_thermo th;
-  rc = acg_get_thermo(e, 0, &th);
-  if (rc) acg_legacy_die("acg_get_thermo", rc);
-  keblk = 2.0 * th.ke;
+  keblk = 2.0 * ke;
+}
+
+/* ---- the propagators of the NVT step (MDcode/time_evolve.c:527-609) ------
+ * AdvanceTimeNVTNoseHoover runs them fused on the device; these separate
+ * entry points keep the reference's names and act on the host mirror, for
+ * host code that composes its own step from them. */
+void U1Propagator() {
+  acg_legacy_sync_host();
+  for (int i = 0; i < N; i++) {
+    const double dx = sphere[i].px * time_step, dy = sphere[i].py * time_step, dz = sphere[i].pz * time_step;
+    sphere[i].x += dx * inv_L;
+    sphere[i].x_u += dx * inv_L;
+    sphere[i].y += dy * inv_L;
+    sphere[i].y_u += dy * inv_L;
+    sphere[i].z += dz * inv_L;
+    sphere[i].z_u += dz * inv_L;
+  }
+  applypbc1();
+  double m = 0.0;
+  for (int i = 0; i < N; i++) {
+    const double dx = sphere[i].x_u - xold[i], dy = sphere[i].y_u - yold[i], dz = sphere[i].z_u - zold[i];
+    const double t = dx * dx + dy * dy + dz * dz;
+    if (m < t) m = t;
+  }
+  maxD = m * L * L;
+  maxmaxD = maxD;
+  acg_legacy_host_touched();
+}
+
+void U2Propagator() {
+  acg_legacy_sync_host();
+  for (int i = 0; i < N; i++) {
+    sphere[i].px += sphere[i].Fx * half_time_step;
+    sphere[i].py += sphere[i].Fy * half_time_step;
+    sphere[i].pz += sphere[i].Fz * half_time_step;
+  }
+  acg_legacy_host_touched();
+}
+
+void U3Propagator(double t) {
+  acg_legacy_sync_host();
+  for (int i = 0; i < N; i++) {
+    sphere[i].px = sphere[i].px * exp(-t * p_eta[0] / q[0]);
+    sphere[i].py = sphere[i].py * exp(-t * p_eta[0] / q[0]);
+    sphere[i].pz = sphere[i].pz * exp(-t * p_eta[0] / q[0]);
+  }
+  for (int i = 0; i < M; i++) eta[i] = eta[i] + t * p_eta[i] / q[i];
+  acg_legacy_host_touched();
+}
+
+void U4Propagator(double t, int jStart, int jEnd) {
+  acg_legacy_sync_host();
+  const int dj = jStart > jEnd ? -1 : 1;
+  int j = jStart;
+  do {
+    double gj;
+    if (j == 0) {
+      double kb = 0.0;
+      for (int i = 0; i < N; i++)
+        kb += sphere[i].px * sphere[i].px + sphere[i].py * sphere[i].py + sphere[i].pz * sphere[i].pz;
+      ke = kb;
+      gj = kb - DOF * T;
+    } else {
+      gj = (p_eta[j - 1] * p_eta[j - 1]) / q[j - 1] - T;
+    }
+    if (j == M - 1) {
+      p_eta[j] = p_eta[j] + t * gj;
+    } else {
+      const double x = t * p_eta[j + 1] / q[j + 1];
+      p_eta[j] = p_eta[j] * exp(-x) + t * gj * (1.0 - exp(-x)) / x;
+    }
+    j += dj;
+  } while (j - dj != jEnd);
 }

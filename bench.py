@@ -6,8 +6,12 @@ N = 100000 at density 1.2, T = 0.45, f0 = 1.0, tau_p = 1.0 (200 steps),
 active fraction 0.1, dt = 0.005, FP64 throughout, Nose-Hoover chain NVT.
 Synthetic data: a seeded random lattice melted on the device (T = 2.0, then
 T = 0.45) before the timed region.  One bench step is one MD timestep of the
-whole system; timed iterations are CUDA-graph launches of 32 steps with a
-256 MiB write between them (untimed) so every launch starts from a cold L2.
+whole system; a timed region is exactly --steps steps as CUDA-graph launches
+(one graph up to 256 steps) with a 256 MiB write before each launch (untimed)
+so every launch starts from a cold L2, repeated --repeats times; value = all
+particle-steps / all device time.  The same line carries the drop-in program's
+throughput (the reference's own host code on the GPU path), the batched
+replicas with in-place observables and the served request stream.
 
 --gpus N under torchrun runs one independent replica per GPU (replicas only:
 the path does not shard), value = all ranks' particle-steps / max time.
@@ -27,6 +31,8 @@ import subprocess
 import sys
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -38,7 +44,9 @@ FLOPS_PER_PAIR = 30.0
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=32000, help="timed MD steps (rounded up to 32)")
+    ap.add_argument("--steps", type=int, default=2048, help="timed MD steps per repeat (exactly)")
+    ap.add_argument("--repeats", type=int, default=0,
+                    help="timed repeats of --steps steps (0: enough for ~640 steps, 5 to 50)")
     ap.add_argument("--warmup", type=int, default=512, help="untimed MD steps before timing (>= 3)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=100000)
@@ -49,7 +57,9 @@ def parse():
     ap.add_argument("--workload", default="all", choices=["all", "plain", "batch", "serve"],
                     help="plain: the headline line only; all: plus the batched and served objects")
     ap.add_argument("--replicas", type=int, default=256)
-    ap.add_argument("--requests", type=int, default=48)
+    ap.add_argument("--requests", type=int, default=0,
+                    help="served requests (0: the first requests of the seeded stream up to ~4e10 particle-steps)")
+    ap.add_argument("--no-dropin", action="store_true")
     return ap.parse_args()
 
 
@@ -200,11 +210,11 @@ def make_engine(n, precision, seed, device, equil):
     return e, st
 
 
-def e2e_run(e, st, nchunks):
+def e2e_run(e, st, nsteps):
     """Through the public C ABI with host buffers: load the state from pinned
-    host memory, run nchunks x 32 steps reading the thermodynamic scalars back
-    after every launch (the reference prints them at its frame cadence), read
-    the final state back."""
+    host memory, run nsteps steps in calls of up to 32 steps reading the
+    thermodynamic scalars back after every call (the reference prints them at
+    its frame cadence), read the final state back."""
     import numpy as np
     import torch
     n = st.n
@@ -221,17 +231,42 @@ def e2e_run(e, st, nchunks):
     lib = _abi.lib()
     ptr = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
     e.sync()
+    ncalls = 0
     t0 = time.perf_counter()
     e.set_state(0, hs)
-    for _ in range(nchunks):
-        e.step(32)
+    left = nsteps
+    while left > 0:
+        k = min(32, left)
+        e.step(k)
         e.thermo(0)
+        left -= k
+        ncalls += 1
     _abi.check(lib.acg_get_state(e.h, 0, ptr(out["x"]), ptr(out["xu"]), ptr(out["p"]), ptr(out["F"])))
     wall = time.perf_counter() - t0
-    steps = 32 * nchunks
     state_bytes = n * (3 * 8 * 3 + 4 + 4)
     thermo_bytes = C.sizeof(_abi.acg_thermo)
-    return n * steps / wall, state_bytes / steps, (state_bytes + 24 * n + thermo_bytes * nchunks) / steps
+    return n * nsteps / wall, state_bytes / nsteps, (state_bytes + 24 * n + thermo_bytes * ncalls) / nsteps
+
+
+def dropin_run(st, n, steps=64, warm=8):
+    """The reference program linked with the drop-in files (its run() loop
+    body: ShuffleActDirec + AdvanceTimeNVTNoseHoover on the device through
+    the globals), particle-steps/s on the host clock; None where that program
+    was not built for this N."""
+    from oracle import Reference, reference_available
+    if not reference_available(n, "dropin"):
+        return None
+    r = Reference(n, "dropin")
+    r.setup(st, 0.45, 1.0, p_eta=np.array([0.05, -0.02, 0.01]))
+    r.seed_rng(17)
+    r.run(warm, start=0, shuffle=True, drift=True)
+    t0 = time.perf_counter()
+    r.run(steps, start=warm, shuffle=True, drift=True)
+    wall = time.perf_counter() - t0
+    r.get_state()  # the state back in the program's globals
+    return {"value": n * steps / wall, "unit": "particle-steps/s", "steps": steps,
+            "workload": f"the reference program (MDcode, N={n}) with cell_list+forces.c and time_evolve.c "
+                        "replaced by the drop-in files: its run() loop body through the globals, host clock"}
 
 
 def batched_run(args, device):
@@ -252,32 +287,53 @@ def batched_run(args, device):
     cfg = autotune(e, reps=5)
     e.step(64)
     e.sync()
-    nchunks = max(8, args.steps // 32 // 8)
-    ms, launches = e.bench_steps(nchunks, 256 << 20)
+    # in-place observables on every replica: the log-time schedule of a
+    # 1e5-step run (200 origins, factor 1.4), Q(t) with a = 0.3, chi4, MSD
+    # and Fs at |q| = 7.25; chi4 accumulated across replicas of equal
+    # parameters (combine_chi4) after the timed steps
+    from activechi4_b200 import qvectors
+    from activechi4_b200.batch import combine_chi4
+    for r, (p, st) in enumerate(reps):
+        e.obs_configure(r, 100000, 200, 1.4, 0, 0.3, qvectors(st.L, 7.25), 128)
+    steps = max(256, args.steps)
+    ms, launches = e.bench_steps(steps, 256 << 20)
     ntot = sum(e.n(r) for r in range(e.nsys))
-    steps = 32 * nchunks
     # a speed measured on a system that blew up is no measurement
     temps = [e.thermo(r)["inst_T"] for r in range(e.nsys)]
     if not all(math.isfinite(t) and 0.0 < t < 10.0 for t in temps):
         raise RuntimeError("batched replicas left the physical range during the timed run")
+    groups = combine_chi4(e, reps)
     e.close()
     return {"value": ntot * steps / (ms * 1e-3), "unit": "particle-steps/s", "replicas": len(reps),
             "particles": ntot, "steps": steps, "ms_per_step": ms / steps, "dtype": "f32-pair/f64-state",
-            "autotune": cfg, "gpu_launches": int(launches),
+            "autotune": cfg, "gpu_launches": int(launches), "chi4_groups": len(groups),
             "workload": "256 replicas, N uniform [500,4000], T {0.45,0.5,0.6}, f0 {0,0.5,1,2}, "
-                        "tau_p {20,200,2000} steps, rho 1.2, NHC NVT, FP32 pair forces"}
+                        "tau_p {20,200,2000} steps, rho 1.2, NHC NVT, FP32 pair forces, in-place Q/chi4/MSD/Fs "
+                        "on the log schedule of a 1e5-step run"}
+
+
+SERVE_WORK = 4.0e10  # particle-steps of the served sample when --requests is 0
 
 
 def served_run(args, device, plain_value):
     """Poisson arrivals (20/s) of runs with N log-uniform in [1e3, 2.56e5] and
-    steps log-uniform in [1e4, 1e6] scaled by 1/100 (a bounded sample), FP32
-    pair forces, in-place Q/chi4/MSD/Fs; against the same requests run one by
-    one on the plain FP64 path."""
+    steps log-uniform in [1e4, 1e6], FP32 pair forces, in-place Q/chi4/MSD/Fs;
+    against the same requests run one by one on the plain FP64 path.  The
+    sample is the first requests of the seeded stream (--requests, or as many
+    as add up to SERVE_WORK particle-steps)."""
     from activechi4_b200.serve import Server, latency_stats, poisson_requests, run_serial
     # a short untimed burst first (other seeds): a running server has its
     # kernels loaded and its allocator pool grown
     Server(device=device).run(poisson_requests(12, rate=20.0, scale=0.01, seed=99, precision=1))
-    reqs = poisson_requests(args.requests, rate=20.0, scale=0.01, seed=5, precision=1)
+    reqs = poisson_requests(max(args.requests, 64), rate=20.0, seed=5, precision=1)
+    if args.requests > 0:
+        reqs = reqs[: args.requests]
+    else:
+        k, w = 0, 0.0
+        while k < len(reqs) and w < SERVE_WORK:
+            w += reqs[k].n * reqs[k].steps
+            k += 1
+        reqs = reqs[:max(k, 2)]
     res = Server(device=device).run(reqs)
     st = latency_stats(res)
     if not all(math.isfinite(r.pe) and math.isfinite(r.ke) for r in res):
@@ -287,8 +343,9 @@ def served_run(args, device, plain_value):
     st.update({"serial_fp64_particle_steps_per_s": work / wall, "serial_fp64_wall_s": wall,
                "vs_serial_fp64": st["particle_steps_per_s"] / (work / wall),
                "vs_plain_fp64": st["particle_steps_per_s"] / plain_value,
-               "workload": f"{len(reqs)} requests, Poisson 20/s, N log-uniform [1e3,2.56e5], steps log-uniform "
-                           "[1e4,1e6]/100, T/f0/tau_p from the batched sets, FP32 pair forces, lattice starts"})
+               "workload": f"{len(reqs)} requests (the first of a seeded stream), Poisson 20/s, N log-uniform "
+                           "[1e3,2.56e5], steps log-uniform [1e4,1e6], T/f0/tau_p from the batched sets, FP32 pair "
+                           "forces, lattice starts"})
     return st
 
 
@@ -325,10 +382,11 @@ def run_ours(args):
     from activechi4_b200.engine import measure_fp64_peak
 
     n = args.n
-    nchunks = max(1, math.ceil(args.steps / 32))
+    steps = max(1, args.steps)
+    repeats = args.repeats if args.repeats > 0 else int(min(50, max(5, math.ceil(640 / steps))))
     warm = max(3, args.warmup)
     e, st = make_engine(n, args.precision, 1000 + rank, local, args.equil)
-    e.step(32 * math.ceil(warm / 32))
+    e.step(warm)
     e.sync()
 
     def barrier():
@@ -337,13 +395,18 @@ def run_ours(args):
         torch.cuda.synchronize(local)
         e.sync()
 
-    barrier()
+    # `repeats` timed regions of exactly `steps` steps each (device time, max
+    # over ranks); value = all particle-steps / all time
+    rep_ms, launches = [], 0
     with ClockSampler(local) as clk:
-        dev_ms, launches = e.bench_steps(nchunks, 256 << 20)
-    barrier()
-    max_ms = reduce_across_ranks(dev_ms, dist, f"cuda:{local}", "max")
-    steps = 32 * nchunks
-    value = replica_throughput(world, n, steps, max_ms)
+        for _ in range(repeats):
+            barrier()
+            dev_ms, nl = e.bench_steps(steps, 256 << 20)
+            barrier()
+            rep_ms.append(reduce_across_ranks(dev_ms, dist, f"cuda:{local}", "max"))
+            launches += nl
+    max_ms = sum(rep_ms)
+    value = replica_throughput(world, n, steps * repeats, max_ms)
 
     # dominant kernel: pair forces (timed alone, force-only mode, warm L2)
     t_force = e.time_stage(1, reps=64)
@@ -358,8 +421,13 @@ def run_ours(args):
     if not (math.isfinite(th["ke"]) and 0.0 < th["inst_T"] < 10.0):
         raise RuntimeError("the timed system left the physical range")
 
-    e2e_val, h2d, d2h = e2e_run(e, st, nchunks)
+    e2e_val, h2d, d2h = e2e_run(e, st, steps * repeats)
+    x, xu, p, _ = e.get_state(0)
     e.close()
+    dropin = None
+    if world == 1 and not args.no_dropin:
+        from activechi4_b200.init import State
+        dropin = dropin_run(State(st.L, x, x.copy(), p, st.type, st.act_tag, st.k), n)
     extra = {}
     if world == 1 and args.workload in ("all", "batch"):
         extra["batched"] = batched_run(args, local)
@@ -383,7 +451,10 @@ def run_ours(args):
             "n_gpus": world,
             "steps": steps,
             "warmup": warm,
-            "ms_per_step": max_ms / steps,
+            "ms_per_step": max_ms / (steps * repeats),
+            "repeats": {"n": repeats, "steps_each": steps,
+                        "ms_per_step_median": statistics.median(rep_ms) / steps,
+                        "ms_per_step_min": min(rep_ms) / steps, "ms_per_step_max": max(rep_ms) / steps},
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
@@ -392,7 +463,7 @@ def run_ours(args):
             "config": {"workload": f"plain KA active glass, N={n} one system, rho=1.2, T=0.45, f0=1.0, "
                                    f"tau_p=200 steps, dt=0.005, NHC NVT, {args.precision} pair forces",
                        "n": n, "systems_per_gpu": 1, "parallelism": f"replicas x{world}",
-                       "l2": "256 MiB write between timed 32-step graph launches (cold L2 each launch)"},
+                       "l2": "256 MiB write before every timed graph launch (cold L2 each launch)"},
             "e2e": {"value": e2e_val, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches),
@@ -409,6 +480,9 @@ def run_ours(args):
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if dropin:
+            dropin["vs_e2e"] = dropin["value"] / e2e_val
+            line["dropin"] = dropin
         line.update(extra)
         print(json.dumps(line), flush=True)
     if dist is not None:

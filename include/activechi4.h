@@ -266,13 +266,15 @@ int acg_set_priority(acg_engine *e, int level);
  * 2 = full cell/neighbour rebuild. */
 int acg_time_stage(acg_engine *e, int stage, int reps, double *ms);
 
-/* Benchmark timing: advance every system nchunks * 32 steps as CUDA-graph
- * launches of 32 steps, recording CUDA events on the engine stream around each
- * launch, and write flush_bytes (> L2) with cudaMemsetAsync between launches
- * (untimed) so that every timed launch starts from a cold L2.  *ms = summed
- * device time of the launches; *launches = kernels launched inside the timed
- * launches (counted from the rebuilds they took). */
-int acg_bench_steps(acg_engine *e, int nchunks, size_t flush_bytes, double *ms, int64_t *launches);
+/* Benchmark timing: advance every system exactly nsteps steps as CUDA-graph
+ * launches (one graph of nsteps steps up to 256, else graphs of 32 steps and
+ * one of the remainder), recording CUDA events on the engine stream around
+ * each launch, and write flush_bytes (> L2) with cudaMemsetAsync before each
+ * launch (untimed) so that every timed launch starts from a cold L2.  *ms =
+ * summed device time of the launches; *launches = kernels launched inside
+ * them (counted from the rebuilds, shuffles, drift removals and observable
+ * events they took).  No counterpart in the reference. */
+int acg_bench_steps(acg_engine *e, int64_t nsteps, size_t flush_bytes, double *ms, int64_t *launches);
 
 /* Measured FP64 FMA throughput of `device` in TFLOP/s (2 flops per FMA):
  * independent DFMA chains on every SM, timed with CUDA events. */

@@ -308,6 +308,11 @@ class Reference(_Common):
     def fix_drift(self):
         self.lib.ref_fix_drift()
 
+    def step_propagators(self, nsteps):
+        """NVT steps composed from U1..U4, update_cell_list and calculate_forces."""
+        for _ in range(int(nsteps)):
+            self.lib.ref_step_propagators()
+
     def adjust_temp(self, T):
         return self.lib.ref_adjust_temp(float(T))
 

@@ -44,6 +44,19 @@ void ref_set_time(long t) { fake_time = (time_t)t; }
 
 static int arrays_ready = 0;
 
+/* In the reference program built with the drop-in files (the timestep on the
+ * GPU), the harness's direct reads and writes of the reference's globals go
+ * through the drop-in's host mirror: refresh before reading sphere[], report
+ * edits.  Absent (null) in the reference's own build. */
+void acg_legacy_sync_host(void) __attribute__((weak));
+void acg_legacy_host_touched(void) __attribute__((weak));
+static void mirror_read(void) {
+  if (acg_legacy_sync_host) acg_legacy_sync_host();
+}
+static void mirror_written(void) {
+  if (acg_legacy_host_touched) acg_legacy_host_touched();
+}
+
 int ref_n(void) { return N; }
 int ref_nact(void) { return Nact; }
 int ref_tau_per(void) { return TAU_per; }
@@ -90,6 +103,7 @@ void ref_setup(double Lbox, double Tset, double f0set, const double *x, const do
     ky[a] = k[Nact + a];
     kz[a] = k[2 * Nact + a];
   }
+  mirror_written();
   if (!arrays_ready) {
     GetDataTypeSLAB();
     GetDataTypeSLABF();
@@ -109,6 +123,7 @@ void ref_set_k(const int *k) {
     ky[a] = k[Nact + a];
     kz[a] = k[2 * Nact + a];
   }
+  mirror_written();
 }
 void ref_get_k(int *k) {
   for (int a = 0; a < Nact; a++) {
@@ -175,6 +190,30 @@ int ref_run(long start, int nsteps, int do_shuffle, int do_drift) {
 /* fixDrift (MDcode/initialise.c:104-138) */
 void ref_fix_drift(void) { fixDrift(); }
 
+/* one NVT step composed from the propagators, as AdvanceTimeNVTNoseHoover's
+ * body does (MDcode/time_evolve.c:495-526) */
+void ref_step_propagators(void) {
+  U4Propagator(time_step * 0.25, M - 1, 0);
+  U3Propagator(time_step * 0.50);
+  U4Propagator(time_step * 0.25, 0, M - 1);
+  U2Propagator();
+  U1Propagator();
+  if (3.0 * maxmaxD > skin * skin) {
+    ExchangeParticlesInBlocks();
+    CommunicateCoordinates(0);
+    update_cell_list();
+  } else {
+    CommunicateCoordinates(1);
+  }
+  calculate_forces();
+  U2Propagator();
+  U4Propagator(time_step * 0.25, M - 1, 0);
+  U3Propagator(time_step * 0.50);
+  U4Propagator(time_step * 0.25, 0, M - 1);
+  ke = ke * 0.5;
+  inst_T = 2.0 * ke / DOF;
+}
+
 /* adjustInitialTemp (MDcode/initialise.c:141-151); returns inst_T after */
 double ref_adjust_temp(double Tset) {
   adjustInitialTemp(Tset);
@@ -224,6 +263,7 @@ int ref_run_nve(int nsteps) {
 }
 
 void ref_get_state(double *x, double *xu, double *p, double *F) {
+  mirror_read();
   for (int i = 0; i < N; i++) {
     if (x) {
       x[3 * i] = sphere[i].x;

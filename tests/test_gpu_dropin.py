@@ -45,3 +45,36 @@ def test_dropin_program_matches_reference(cuda_lib, g1000):
     ref.run_nve(20)
     dro.run_nve(20)
     assert np.abs(dro.get_state()[1] - ref.get_state()[1]).max() < 1e-9
+
+
+def test_dropin_sync_points(cuda_lib, g1000):
+    """The drop-in's step reads back only scalars; the reference's own
+    routines that read or write the particles (fixDrift here, through the
+    linker's wrapper; the run loop's fixDrift every 100000 steps from index
+    0) see the device's state and their edits reach the device.  The
+    propagators U1..U4 on the host mirror compose the same NVT step."""
+    from oracle import Reference, reference_available
+    if not (reference_available(1000) and reference_available(1000, "dropin")):
+        pytest.skip("reference / drop-in programs not built")
+    st = golden_state(g1000)
+    st.p[:, 0] += 0.1  # a net momentum for fixDrift
+    ref, dro = Reference(1000), Reference(1000, "dropin")
+    for r in (ref, dro):
+        r.setup(st, 0.45, 1.0, g1000["eta0"], g1000["p_eta0"])
+        r.seed_rng(7)
+        r.run(30, start=0, shuffle=True, drift=True)  # fixDrift after loop index 0
+        r.fix_drift()
+        r.run(30, start=30, shuffle=True)
+    xr, xur, pr, _ = ref.get_state()
+    xd, xud, pd, _ = dro.get_state()
+    assert np.abs(xud - xur).max() < 1e-9
+    assert np.abs(pd - pr).max() / np.sqrt((pr ** 2).sum(axis=1).mean()) < 1e-9
+    assert abs(pd.sum(axis=0)).max() < 1e-9
+    # the same NVT step composed from the exported propagators
+    for r in (ref, dro):
+        r.step_propagators(10)
+    xr, xur, pr, _ = ref.get_state()
+    xd, xud, pd, _ = dro.get_state()
+    assert np.abs(xud - xur).max() < 1e-9
+    assert np.abs(pd - pr).max() / np.sqrt((pr ** 2).sum(axis=1).mean()) < 1e-9
+
