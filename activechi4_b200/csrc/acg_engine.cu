@@ -189,6 +189,7 @@ int plan(const acg_params *params, int nsys, Layout &lay, int nsm) {
   const size_t Gn = (size_t)lay.ngroups;
   add(8 * (Gn + 1));                      // tiles_g
   add(4 * (Gn + 1));                      // gstart
+  add(4 * (Gn + 1));                      // gflag
   add(8 * ((size_t)lay.nboxtiles + 1));   // tiles_x
   add(32 * (Gn + lay.nboxtiles + S / 4 + nsys + 1));  // part_b
   add(32 * S);                            // pacc
@@ -221,6 +222,7 @@ struct acg_engine {
   View v{};
   SysDesc *d_desc = nullptr;
   int tpp = 4, block = 128, gtpp = 2, btpp = 2;  // btpp: whole-box kernels
+  bool half = false;  // cell groups on half lists (acg_set_group_half)
   int ntiles_a = 0, ntiles_b = 0, ntiles_l = 0, ntiles_c = 0, ntiles_g = 0, ntiles_x = 0;
   int2 *d_tiles_b = nullptr;
   std::vector<int> dirty;  // systems whose forces/lists must be recomputed
@@ -259,7 +261,13 @@ GroupFn group_fn(int gtpp, int prec) {
   }
   return nullptr;
 }
-size_t group_smem(int gcap) { return 3 * (size_t)gcap * sizeof(double); }
+// group force kernel: 24 bytes of staged position per particle; with half
+// lists also the fixed-point partner-force accumulators and the staged-index
+// -> centre-index table
+size_t group_smem(int gcap, bool half) {
+  return 3 * (size_t)gcap * sizeof(double) +
+         (half ? 3 * (size_t)HALF_MCAP * sizeof(unsigned long long) + align_up(2 * (size_t)gcap, 16) : 0);
+}
 size_t list_smem(int gcap) { return ((size_t)gcap + 3 * MAX_UNION) * sizeof(float4); }
 
 GroupFn box_fn(int gtpp, int prec) {
@@ -360,8 +368,9 @@ void drop_graphs(acg_engine *e) {
 // memory) and can be updated in place instead of instantiated anew
 std::string graph_shape(const acg_engine *e, int K) {
   char b[160];
-  snprintf(b, sizeof(b), "K%d g%d x%d b%d l%d p%d t%d/%d/%d/%d", K, e->ntiles_g > 0, e->ntiles_x > 0,
-           e->ntiles_b > 0, e->ntiles_l > 0, e->lay.desc[0].precision, e->tpp, e->gtpp, e->btpp, e->block);
+  snprintf(b, sizeof(b), "K%d g%d x%d b%d l%d h%d p%d t%d/%d/%d/%d", K, e->ntiles_g > 0, e->ntiles_x > 0,
+           e->ntiles_b > 0, e->ntiles_l > 0, (int)e->half, e->lay.desc[0].precision, e->tpp, e->gtpp, e->btpp,
+           e->block);
   return b;
 }
 
@@ -431,7 +440,7 @@ int launch_rebuild(acg_engine *e) {
 
 int launch_force(acg_engine *e, int mode) {
   const int prec = e->lay.desc[0].precision;
-  if (e->ntiles_g) group_fn(e->gtpp, prec)<<<e->ntiles_g, BLOCK_G, group_smem(e->v.gcap), e->stream>>>(e->v, mode);
+  if (e->ntiles_g) group_fn(e->gtpp, prec)<<<e->ntiles_g, BLOCK_G, group_smem(e->v.gcap, e->half), e->stream>>>(e->v, mode);
   if (e->ntiles_x)
     box_fn(e->btpp, prec)<<<e->ntiles_x, BLOCK_X, box_smem(e->lay.box_nmax, prec), e->stream>>>(e->v, mode);
   if (e->ntiles_b)
@@ -561,7 +570,7 @@ int add_steps(acg_engine *e, cudaGraph_t g, int K, cudaGraphNode_t *prev_io) {
     cudaGraphNode_t last = nullptr;
     if (e->ntiles_g) {
       void *ga[] = {&v, &mode0};
-      rc = add_kernel(g, dep, ndep, &nb, (void *)gf, e->ntiles_g, BLOCK_G, ga, group_smem(v.gcap));
+      rc = add_kernel(g, dep, ndep, &nb, (void *)gf, e->ntiles_g, BLOCK_G, ga, group_smem(v.gcap, e->half));
       if (rc) return rc;
       last = nb;
       dep = &last;
@@ -803,6 +812,7 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   const size_t Gn = (size_t)L.ngroups;
   int2 *tg = (int2 *)take(8 * (Gn + 1));
   v.gstart = (int *)take(4 * (Gn + 1));
+  v.gflag = (int *)take(4 * (Gn + 1));
   const size_t Xn = (size_t)L.nboxtiles;
   int2 *tx = (int2 *)take(8 * (Xn + 1));
   v.part_b = (double4 *)take(32 * (Gn + Xn + S / 4 + nsys + 1));
@@ -887,7 +897,7 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   };
   bool attr_ok = true;
   for (int gt : {1, 2, 4})
-    for (int pr : {0, 1}) attr_ok = attr_ok && raise_smem((const void *)group_fn(gt, pr), group_smem(v.gcap));
+    for (int pr : {0, 1}) attr_ok = attr_ok && raise_smem((const void *)group_fn(gt, pr), group_smem(v.gcap, true));
   attr_ok = attr_ok && raise_smem((const void *)k_build_list_groups, list_smem(v.gcap));
   if (L.box_nmax > 0) {
     if (box_list_smem(L.box_cell_nmax) > 227 * 1024 || box_smem(L.box_nmax, 0) > 227 * 1024) {
@@ -1483,6 +1493,23 @@ int acg_set_group_tpp(acg_engine *e, int gtpp) {
   e->gtpp = gtpp;
   e->btpp = gtpp;
   drop_graphs(e);
+  return ACG_OK;
+}
+
+int acg_set_group_half(acg_engine *e, int on) {
+  if (!e) return fail(ACG_ERR_INVALID, "null engine");
+  CK(cudaSetDevice(e->device));
+  CK(cudaStreamSynchronize(e->stream));
+  e->half = on != 0;
+  for (int r = 0; r < e->lay.nsys; r++) {
+    e->lay.desc[r].half = e->half && e->lay.desc[r].ng > 0;
+    e->dirty[r] = 1;  // lists of the other kind: rebuild them and the forces
+  }
+  e->any_dirty = true;
+  CK(cudaMemcpyAsync(e->d_desc, e->lay.desc.data(), sizeof(SysDesc) * e->lay.nsys, cudaMemcpyHostToDevice,
+                     e->stream));
+  drop_graphs(e);
+  CK(cudaStreamSynchronize(e->stream));
   return ACG_OK;
 }
 

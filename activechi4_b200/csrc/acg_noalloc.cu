@@ -238,7 +238,7 @@ extern "C" int acg_forces_noalloc(const double *x, const double *xu, const int *
   const int nc = (int)((double)(int)L / 2.85);
   if (nc < 2) return na_fail(ACG_ERR_INVALID, "acg_forces_noalloc: box smaller than 2 cells of 2.85 per side");
   if ((long long)nc * nc * nc > ACG_NOALLOC_MAX_CELLS)
-    return na_fail(ACG_ERR_INVALID, "acg_forces_noalloc: " + std::to_string(nc * nc * nc) +
+    return na_fail(ACG_ERR_INVALID, "acg_forces_noalloc: " + std::to_string((long long)nc * nc * nc) +
                                         " cells exceed ACG_NOALLOC_MAX_CELLS (" +
                                         std::to_string(ACG_NOALLOC_MAX_CELLS) + ")");
   int dev = 0;

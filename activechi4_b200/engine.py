@@ -299,6 +299,11 @@ class Engine:
     def set_group_tpp(self, gtpp: int):
         check(self._lib.acg_set_group_tpp(self.h, int(gtpp)))
 
+    def set_group_half(self, on: bool):
+        """Half neighbour lists inside cell groups (pairs once, partner forces
+        in fixed point) or full lists."""
+        check(self._lib.acg_set_group_half(self.h, int(bool(on))))
+
     def get_launch(self):
         t, b = C.c_int(), C.c_int()
         check(self._lib.acg_get_launch(self.h, C.byref(t), C.byref(b)))

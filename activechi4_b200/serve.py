@@ -195,20 +195,28 @@ class Server:
         return sorted(results, key=lambda r: r.rid)
 
 
-def run_serial(requests, device=0, precision=0, clock=time.perf_counter):
+def run_serial(requests, device=0, precision=0, clock=time.perf_counter, sample_steps=None):
     """The same requests one after another, each alone on the GPU (the
-    serial baseline); returns (results, wall seconds)."""
+    serial baseline); returns (results, wall seconds).  With sample_steps,
+    each request runs only its first sample_steps steps and its stepping time
+    is scaled to its full length (set-up time counted as measured): a bounded
+    estimate of the serial wall time."""
     out = []
-    t0 = clock()
+    wall = 0.0
     for req in requests:
         r = dataclasses.replace(req, precision=precision)
+        t0 = clock()
         e = start_run(r, device)
-        a = clock() - t0
-        e.step(r.steps)
         e.sync()
-        out.append(finish_run(e, r, a, a, clock() - t0))
+        t1 = clock()
+        k = r.steps if sample_steps is None else min(r.steps, int(sample_steps))
+        e.step(k)
+        e.sync()
+        t2 = clock()
+        wall += (t1 - t0) + (t2 - t1) * (r.steps / k)
+        out.append(finish_run(e, r, t0, t1, t2))
         e.close()
-    return out, clock() - t0
+    return out, wall
 
 
 def poisson_requests(count, rate=20.0, n_range=(1000, 256000), step_range=(10000, 1000000), scale=1.0,

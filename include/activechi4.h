@@ -288,6 +288,13 @@ int acg_get_launch(acg_engine *e, int *tpp, int *block);
  * >= 5 cells per side, or larger than the whole-box limit) and of the
  * whole-box force kernel (2 to 4 cells per side, N <= 8192). */
 int acg_set_group_tpp(acg_engine *e, int gtpp);
+/* Cell-group neighbour lists: 0 = full lists (every pair from both sides, as
+ * the reference's force loop sees it per particle); 1 = half lists inside a
+ * group (a pair of two particles of the group's own cells is computed once
+ * and its partner's force summed in 2^-42 fixed point, so the result does not
+ * depend on the order of the additions).  Rebuilds the lists and forces of
+ * every system at the next call.  No counterpart in the reference. */
+int acg_set_group_half(acg_engine *e, int on);
 
 const char *acg_last_error(void);
 const char *acg_version(void);
@@ -316,7 +323,15 @@ const char *acg_version(void);
  * before any stream capture.  Calls share the array and it keeps the last
  * call's contents (each call clears what must start at zero); calls that
  * overlap on the GPU (two streams, or two host threads) race on it and must
- * be serialised by the caller. */
+ * be serialised by the caller.
+ * The looked-up address is kept per device index for the process: it belongs
+ * to the device's primary context (the one the CUDA runtime uses); after
+ * cudaDeviceReset, or from a different context made current through the
+ * driver API, it is no longer valid, so such callers must not use this entry
+ * point.  Particles are placed in their cells by atomic counters, so the
+ * order in which each particle's pair terms are summed can change from call
+ * to call: results repeat to FP64 rounding (max|dF|/rms|F| ~ 1e-15), not bit
+ * for bit. */
 #define ACG_NOALLOC_MAX_N 262144
 #define ACG_NOALLOC_MAX_CELLS 32768
 #define ACG_NOALLOC_SCRATCH_BYTES (3u << 20)

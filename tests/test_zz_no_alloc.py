@@ -20,7 +20,7 @@ pytestmark = pytest.mark.gpu
 
 def _engine_forces(st, f0):
     from activechi4_b200 import Engine, default_params
-    e = Engine(default_params(st.n, f0=f0, shuffle=0))
+    e = Engine(default_params(st.n, f0=f0, shuffle=0, nact=st.nact))
     e.set_state(0, st)
     e.compute_forces()
     F = e.get_state(0)[3]
@@ -29,18 +29,19 @@ def _engine_forces(st, f0):
     return F, th["pe"], th["virial"], th["vir_act"]
 
 
-def _noalloc_forces(lib, st, f0):
+def _noalloc_forces(lib, st, f0, with_xu=True):
     import torch
     dev = torch.device("cuda:0")
     x = torch.tensor(st.x, dtype=torch.float64, device=dev).contiguous()
-    xu = torch.tensor(st.xu, dtype=torch.float64, device=dev).contiguous()
+    xu = torch.tensor(st.xu, dtype=torch.float64, device=dev).contiguous() if with_xu else None
     ty = torch.tensor(st.type, dtype=torch.int32, device=dev).contiguous()
     act = torch.tensor(st.act_tag, dtype=torch.int32, device=dev).contiguous()
-    k = torch.tensor(np.asarray(st.k).reshape(-1), dtype=torch.int32, device=dev).contiguous()
+    k = (torch.tensor(np.asarray(st.k).reshape(-1), dtype=torch.int32, device=dev).contiguous()
+         if st.nact else None)
     F = torch.full((st.n, 3), float("nan"), dtype=torch.float64, device=dev)
     out = torch.full((3,), float("nan"), dtype=torch.float64, device=dev)
     torch.cuda.synchronize()
-    p = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    p = lambda t: None if t is None else C.c_void_p(t.data_ptr())  # noqa: E731
     rc = lib.acg_forces_noalloc(p(x), p(xu), p(ty), p(act), p(k), st.n, st.nact, st.L, f0, p(F), p(out),
                                 C.c_void_p(torch.cuda.current_stream().cuda_stream))
     assert rc == 0, lib.acg_last_error().decode()
@@ -60,6 +61,33 @@ def test_noalloc_matches_engine_twice(cuda_lib, g1000, g4000):
         assert abs(van - va) <= 1e-12 * max(1.0, abs(va))
 
 
+def test_noalloc_golden_and_small_boxes(cuda_lib, g1000, g500):
+    """Against the reference's own forces (golden N=1000) and, for a box of
+    two cells per side (N=500, neighbour offsets 0..1), against the oracle,
+    which counts each pair once there; then a system without active
+    particles and without unfolded coordinates (xu and k NULL)."""
+    from oracle import Oracle
+    lib = cuda_lib
+    st = golden_state(g1000)
+    Fn, pen, virn, van = _noalloc_forces(lib, st, 1.0)
+    assert force_err(Fn, g1000["F0"]) <= 1e-12
+    assert rel(pen, g1000["pe0"]) <= 1e-12 and rel(virn, g1000["vir0"]) <= 1e-12
+    assert abs(van - g1000["viract0"]) <= 1e-12 * max(1.0, abs(g1000["viract0"]))
+    st = golden_state(g500)
+    Fo, peo, viro, vao = Oracle.from_state(st, 0.45, 1.0).forces()
+    for _ in range(2):
+        Fn, pen, virn, van = _noalloc_forces(lib, st, 1.0)
+        assert force_err(Fn, Fo) <= 1e-12
+        assert rel(pen, peo) <= 1e-12 and rel(virn, viro) <= 1e-12
+        assert abs(van - vao) <= 1e-12 * max(1.0, abs(vao))
+    st = golden_state(g1000)
+    st.act_tag[:] = -1
+    st.k = np.zeros((3, 0), dtype=np.int32)
+    Fe, pe, vir, va = _engine_forces(st, 1.0)
+    Fn, pen, virn, van = _noalloc_forces(lib, st, 1.0, with_xu=False)
+    assert force_err(Fn, Fe) <= 1e-12 and rel(pen, pe) <= 1e-12 and van == 0.0
+
+
 def test_noalloc_rejects_oversized_input(cuda_lib):
     lib = cuda_lib
     big = 262144 + 1
@@ -67,3 +95,8 @@ def test_noalloc_rejects_oversized_input(cuda_lib):
                                 (big / 1.2) ** (1 / 3), 1.0, C.c_void_p(1), C.c_void_p(1), None)
     assert rc == -1
     assert "262144" in lib.acg_last_error().decode()
+    # more cells than the scratch array holds (33^3 = 35937 > 32768)
+    rc = lib.acg_forces_noalloc(C.c_void_p(1), None, C.c_void_p(1), C.c_void_p(1), None, 1000, 0, 95.0, 1.0,
+                                C.c_void_p(1), C.c_void_p(1), None)
+    assert rc == -1
+    assert "35937" in lib.acg_last_error().decode()
