@@ -93,7 +93,8 @@ _SIGS = {
     "acg_set_launch": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "acg_get_launch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "acg_set_group_tpp": (C.c_int, [C.c_void_p, C.c_int]),
-    "acg_set_group_half": (C.c_int, [C.c_void_p, C.c_int]),
+    "acg_set_box_cells": (C.c_int, [C.c_void_p, C.c_int]),
+    "acg_get_box_cells": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "acg_obs_configure": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(acg_obs_config)]),
     "acg_obs_sums": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "acg_bench_steps": (C.c_int, [C.c_void_p, C.c_int64, C.c_size_t, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),

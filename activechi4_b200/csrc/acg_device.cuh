@@ -77,7 +77,7 @@ struct SysDesc {
   int shuffle, list_mode, precision, goff;  // goff: offset of the system's groups
   int tile0_a, ntile_a, box, xoff;            // kick/drift tiles; box: whole-box kernels (2..4 cells per side), xoff: first box tile
   int cpb, msub, bz, soff;                    // cpb: cells per whole-box block; msub: list sub-cells per side, bz: their list bricks' depth, soff: first sub-cell start
-  int drift_every, half, pad1, pad2;          // drift_every: remove the mean momentum after every such step (0: never); half: cell groups use half lists
+  int drift_every, pad0, pad1, pad2;          // drift_every: remove the mean momentum after every such step (0: never)
   double L, invL, inv_cell;  // inv_cell: cells per unit reduced length (InvCellSize)
   double T, f0, dt, half_dt, skin2, rebuild_factor, dof;
   double q[NHC_M];
@@ -147,7 +147,6 @@ struct View {
   int *ccount_b, *cfill, *cstart, *ccount;
   const int2 *tiles_a, *tiles_b, *tiles_l, *tiles_c, *tiles_g, *tiles_x;
   int *gstart;      // per group: first centre particle (prefix over the system's groups)
-  int *gflag;       // per group: 1 = the last rebuild left it on the full cell scan (half-list systems)
   double4 *part_b;
   double4 *pacc;    // whole-box systems: per-particle pe, virial, KE, active virial
   unsigned int *counter_a;

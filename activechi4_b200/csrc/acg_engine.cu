@@ -40,6 +40,7 @@ constexpr int BENCH_MAX_GRAPH = 256;  // acg_bench_steps: one graph for up to th
 struct Layout {
   int nsys = 0, nslots = 0, ncells = 0, nact = 0, maxnb = 0, ngroups = 0, nboxtiles = 0, box_nmax = 0;
   int nact_max = 0;  // most active particles of one system
+  int nboxcap = 0;   // whole-box tiles at one cell per block (the most any partition needs)
   int box_m3max = 0;  // most list sub-cells of a whole-box system (0: none uses them)
   int box_cell_nmax = 0;  // most particles of a whole-box system listed from its cells
   int nsub = 0;           // sub-cell starts of all whole-box systems with list sub-cells
@@ -82,7 +83,7 @@ int resolve(const acg_params &p, SysDesc &d) {
     d.lcut2[t] = rl * rl;
   }
   d.tau_p = p.tau_p_steps;
-  d.thermostat = p.thermostat ? 1 : 0;
+  d.thermostat = p.thermostat;
   d.shuffle = p.shuffle;
   d.drift_every = p.drift_every;
   d.list_mode = p.list_mode;
@@ -90,6 +91,7 @@ int resolve(const acg_params &p, SysDesc &d) {
   d.seed = p.seed;
   if (p.dt <= 0 || p.skin <= 0 || p.rebuild_factor <= 0)
     return fail(ACG_ERR_INVALID, "dt, skin and rebuild_factor must be positive");
+  if (p.thermostat < 0 || p.thermostat > 2) return fail(ACG_ERR_INVALID, "thermostat must be 0, 1 or 2");
   if (p.thermostat && !(p.T > 0)) return fail(ACG_ERR_INVALID, "thermostat needs T > 0");
   if (p.shuffle < 0 || p.shuffle > 2) return fail(ACG_ERR_INVALID, "shuffle must be 0, 1 or 2");
   if (p.shuffle && p.tau_p_steps <= 0) return fail(ACG_ERR_INVALID, "shuffle needs tau_p_steps > 0");
@@ -158,7 +160,10 @@ int plan(const acg_params *params, int nsys, Layout &lay, int nsm) {
       // 2 cells per side: one cell (of up to ~100 particles) per block
       d.cpb = d.nc == 2 ? 1 : cpb;
       d.xoff = lay.nboxtiles;
-      if (d.box) lay.nboxtiles += (d.ncell + d.cpb - 1) / d.cpb;
+      if (d.box) {
+        lay.nboxtiles += (d.ncell + d.cpb - 1) / d.cpb;
+        lay.nboxcap += d.ncell;
+      }
     }
   }
   // neighbour-row capacity: 1.45x the ideal-gas count within the widest list
@@ -189,9 +194,8 @@ int plan(const acg_params *params, int nsys, Layout &lay, int nsm) {
   const size_t Gn = (size_t)lay.ngroups;
   add(8 * (Gn + 1));                      // tiles_g
   add(4 * (Gn + 1));                      // gstart
-  add(4 * (Gn + 1));                      // gflag
-  add(8 * ((size_t)lay.nboxtiles + 1));   // tiles_x
-  add(32 * (Gn + lay.nboxtiles + S / 4 + nsys + 1));  // part_b
+  add(8 * ((size_t)lay.nboxcap + 1));     // tiles_x
+  add(32 * (Gn + lay.nboxcap + S / 4 + nsys + 1));  // part_b
   add(32 * S);                            // pacc
   add(64);                                // counters
   add(sizeof(ObsDesc) * nsys);            // observables
@@ -222,9 +226,9 @@ struct acg_engine {
   View v{};
   SysDesc *d_desc = nullptr;
   int tpp = 4, block = 128, gtpp = 2, btpp = 2;  // btpp: whole-box kernels
-  bool half = false;  // cell groups on half lists (acg_set_group_half)
   int ntiles_a = 0, ntiles_b = 0, ntiles_l = 0, ntiles_c = 0, ntiles_g = 0, ntiles_x = 0;
   int2 *d_tiles_b = nullptr;
+  int2 *d_tiles_x = nullptr;
   std::vector<int> dirty;  // systems whose forces/lists must be recomputed
   bool any_dirty = false;
   cudaGraphExec_t gexec = nullptr;
@@ -261,13 +265,7 @@ GroupFn group_fn(int gtpp, int prec) {
   }
   return nullptr;
 }
-// group force kernel: 24 bytes of staged position per particle; with half
-// lists also the fixed-point partner-force accumulators and the staged-index
-// -> centre-index table
-size_t group_smem(int gcap, bool half) {
-  return 3 * (size_t)gcap * sizeof(double) +
-         (half ? 3 * (size_t)HALF_MCAP * sizeof(unsigned long long) + align_up(2 * (size_t)gcap, 16) : 0);
-}
+size_t group_smem(int gcap) { return 3 * (size_t)gcap * sizeof(double); }
 size_t list_smem(int gcap) { return ((size_t)gcap + 3 * MAX_UNION) * sizeof(float4); }
 
 GroupFn box_fn(int gtpp, int prec) {
@@ -298,6 +296,30 @@ ForceFn force_fn(int tpp, int prec) {
   }
 #undef F
   return nullptr;
+}
+
+// whole-box tiles: d.cpb cells of one system per block, the blocks of the
+// largest systems first (the partition does not change any result: the
+// per-system sums are taken per particle, in slot order)
+int build_tiles_x(acg_engine *e) {
+  std::vector<int2> h_x;
+  int nt = 0;
+  for (int r = 0; r < e->lay.nsys; r++) {
+    SysDesc &d = e->lay.desc[r];
+    d.xoff = nt;
+    if (!d.box) continue;
+    const int k = (d.ncell + d.cpb - 1) / d.cpb;
+    for (int b = 0; b < k; b++) h_x.push_back(make_int2(r, b));
+    nt += k;
+  }
+  if (nt > e->lay.nboxcap) return fail(ACG_ERR_INVALID, "internal: more whole-box tiles than the layout holds");
+  std::stable_sort(h_x.begin(), h_x.end(), [&](int2 a, int2 b) { return e->lay.desc[a.x].n > e->lay.desc[b.x].n; });
+  e->lay.nboxtiles = nt;
+  e->ntiles_x = nt;
+  e->v.ntiles_x = nt;
+  if (!h_x.empty())
+    CK(cudaMemcpyAsync(e->d_tiles_x, h_x.data(), h_x.size() * sizeof(int2), cudaMemcpyHostToDevice, e->stream));
+  return ACG_OK;
 }
 
 // force tiles: one block per cell group for systems with >= 3 cells per
@@ -368,9 +390,8 @@ void drop_graphs(acg_engine *e) {
 // memory) and can be updated in place instead of instantiated anew
 std::string graph_shape(const acg_engine *e, int K) {
   char b[160];
-  snprintf(b, sizeof(b), "K%d g%d x%d b%d l%d h%d p%d t%d/%d/%d/%d", K, e->ntiles_g > 0, e->ntiles_x > 0,
-           e->ntiles_b > 0, e->ntiles_l > 0, (int)e->half, e->lay.desc[0].precision, e->tpp, e->gtpp, e->btpp,
-           e->block);
+  snprintf(b, sizeof(b), "K%d g%d x%d b%d l%d p%d t%d/%d/%d/%d", K, e->ntiles_g > 0, e->ntiles_x > 0,
+           e->ntiles_b > 0, e->ntiles_l > 0, e->lay.desc[0].precision, e->tpp, e->gtpp, e->btpp, e->block);
   return b;
 }
 
@@ -440,7 +461,7 @@ int launch_rebuild(acg_engine *e) {
 
 int launch_force(acg_engine *e, int mode) {
   const int prec = e->lay.desc[0].precision;
-  if (e->ntiles_g) group_fn(e->gtpp, prec)<<<e->ntiles_g, BLOCK_G, group_smem(e->v.gcap, e->half), e->stream>>>(e->v, mode);
+  if (e->ntiles_g) group_fn(e->gtpp, prec)<<<e->ntiles_g, BLOCK_G, group_smem(e->v.gcap), e->stream>>>(e->v, mode);
   if (e->ntiles_x)
     box_fn(e->btpp, prec)<<<e->ntiles_x, BLOCK_X, box_smem(e->lay.box_nmax, prec), e->stream>>>(e->v, mode);
   if (e->ntiles_b)
@@ -570,7 +591,7 @@ int add_steps(acg_engine *e, cudaGraph_t g, int K, cudaGraphNode_t *prev_io) {
     cudaGraphNode_t last = nullptr;
     if (e->ntiles_g) {
       void *ga[] = {&v, &mode0};
-      rc = add_kernel(g, dep, ndep, &nb, (void *)gf, e->ntiles_g, BLOCK_G, ga, group_smem(v.gcap, e->half));
+      rc = add_kernel(g, dep, ndep, &nb, (void *)gf, e->ntiles_g, BLOCK_G, ga, group_smem(v.gcap));
       if (rc) return rc;
       last = nb;
       dep = &last;
@@ -812,8 +833,7 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   const size_t Gn = (size_t)L.ngroups;
   int2 *tg = (int2 *)take(8 * (Gn + 1));
   v.gstart = (int *)take(4 * (Gn + 1));
-  v.gflag = (int *)take(4 * (Gn + 1));
-  const size_t Xn = (size_t)L.nboxtiles;
+  const size_t Xn = (size_t)L.nboxcap;
   int2 *tx = (int2 *)take(8 * (Xn + 1));
   v.part_b = (double4 *)take(32 * (Gn + Xn + S / 4 + nsys + 1));
   v.pacc = (double4 *)take(32 * S);
@@ -836,7 +856,7 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   v.nsys = nsys;
   v.maxnb = L.maxnb;
 
-  std::vector<int2> h_a, h_l, h_c, h_g, h_x;
+  std::vector<int2> h_a, h_l, h_c, h_g;
   for (int r = 0; r < nsys; r++) {
     SysDesc &d = e->lay.desc[r];
     d.tile0_a = (int)h_a.size();
@@ -846,7 +866,7 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
     if (d.ng > 0)
       for (int g = 0; g < d.ng * d.ng * d.ng; g++) h_g.push_back(make_int2(r, g));
     else if (d.box)
-      for (int b = 0; b < (d.ncell + d.cpb - 1) / d.cpb; b++) h_x.push_back(make_int2(r, b));
+      continue;  // whole-box tiles: build_tiles_x
     else
       for (int s = 0; s < d.n; s += PART_L) h_l.push_back(make_int2(r, s));
   }
@@ -861,15 +881,7 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
     return c;
   };
   std::stable_sort(h_g.begin(), h_g.end(), [&](int2 a, int2 b) { return group_cells(a) > group_cells(b); });
-  // whole-box blocks of the largest systems first
-  std::stable_sort(h_x.begin(), h_x.end(),
-                   [&](int2 a, int2 b) { return e->lay.desc[a.x].n > e->lay.desc[b.x].n; });
-  e->ntiles_x = (int)h_x.size();
-  v.ntiles_x = e->ntiles_x;
-  if (e->ntiles_x != L.nboxtiles) {  // the arena holds exactly nboxtiles tiles and partials
-    acg_destroy(e);
-    return fail(ACG_ERR_INVALID, "internal: whole-box tile count differs from the layout");
-  }
+  e->d_tiles_x = tx;
   e->ntiles_a = (int)h_a.size();
   e->ntiles_l = (int)h_l.size();
   e->ntiles_c = (int)h_c.size();
@@ -897,7 +909,7 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   };
   bool attr_ok = true;
   for (int gt : {1, 2, 4})
-    for (int pr : {0, 1}) attr_ok = attr_ok && raise_smem((const void *)group_fn(gt, pr), group_smem(v.gcap, true));
+    for (int pr : {0, 1}) attr_ok = attr_ok && raise_smem((const void *)group_fn(gt, pr), group_smem(v.gcap));
   attr_ok = attr_ok && raise_smem((const void *)k_build_list_groups, list_smem(v.gcap));
   if (L.box_nmax > 0) {
     if (box_list_smem(L.box_cell_nmax) > 227 * 1024 || box_smem(L.box_nmax, 0) > 227 * 1024) {
@@ -931,9 +943,7 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
       (!h_l.empty() &&
        cudaMemcpyAsync(tl, h_l.data(), h_l.size() * sizeof(int2), cudaMemcpyHostToDevice, e->stream) !=
            cudaSuccess) ||
-      (!h_x.empty() &&
-       cudaMemcpyAsync(tx, h_x.data(), h_x.size() * sizeof(int2), cudaMemcpyHostToDevice, e->stream) !=
-           cudaSuccess))
+      build_tiles_x(e) != ACG_OK)
     return cleanup_fail(fail(ACG_ERR_CUDA, "initial upload failed"));
   std::vector<SysState> st(nsys);
   memset(st.data(), 0, sizeof(SysState) * nsys);
@@ -1496,20 +1506,29 @@ int acg_set_group_tpp(acg_engine *e, int gtpp) {
   return ACG_OK;
 }
 
-int acg_set_group_half(acg_engine *e, int on) {
+int acg_set_box_cells(acg_engine *e, int cells) {
   if (!e) return fail(ACG_ERR_INVALID, "null engine");
+  if (cells < 1 || cells > BOX_CELLS) return fail(ACG_ERR_INVALID, "cells per whole-box block must be in [1, 8]");
   CK(cudaSetDevice(e->device));
   CK(cudaStreamSynchronize(e->stream));
-  e->half = on != 0;
   for (int r = 0; r < e->lay.nsys; r++) {
-    e->lay.desc[r].half = e->half && e->lay.desc[r].ng > 0;
-    e->dirty[r] = 1;  // lists of the other kind: rebuild them and the forces
+    SysDesc &d = e->lay.desc[r];
+    if (d.box && d.nc > 2) d.cpb = cells;
   }
-  e->any_dirty = true;
-  CK(cudaMemcpyAsync(e->d_desc, e->lay.desc.data(), sizeof(SysDesc) * e->lay.nsys, cudaMemcpyHostToDevice,
-                     e->stream));
+  int rc = build_tiles_x(e);
+  if (rc) return rc;
   drop_graphs(e);
+  rc = build_tiles_b(e);  // partial-sum slots and the descriptors
+  if (rc) return rc;
   CK(cudaStreamSynchronize(e->stream));
+  return ACG_OK;
+}
+
+int acg_get_box_cells(acg_engine *e, int *cells) {
+  if (!e || !cells) return fail(ACG_ERR_INVALID, "bad arguments");
+  *cells = 0;
+  for (int r = 0; r < e->lay.nsys; r++)
+    if (e->lay.desc[r].box && e->lay.desc[r].nc > 2) *cells = e->lay.desc[r].cpb;
   return ACG_OK;
 }
 

@@ -815,7 +815,7 @@ __device__ void next_first_half(const SysDesc &d, SysState &st, double kb) {
   if (st.ramp_left > 0) {
     const double inst = 2.0 * (kb * 0.5) / d.dof;
     st.s1 = sqrt(st.ramp_T / inst);
-  } else if (d.thermostat) {
+  } else if (d.thermostat == 1) {
     double eta[NHC_M], pet[NHC_M];
     for (int k = 0; k < NHC_M; k++) {
       eta[k] = st.eta_end[k];
@@ -851,8 +851,21 @@ __device__ void finalize_sums(const SysDesc &d, SysState &st, int mode, double p
     st.ramp_left -= 1;
     st.ramp_real -= 1;
     if (st.ramp_left > 0) st.ramp_T = st.ramp_real > 0 ? __dadd_rn(st.ramp_T, st.ramp_dT) : st.ramp_end;
+  } else if (mode == 0 && d.thermostat == 2) {
+    // advance_time_NVT_Berendsen (MDcode/time_evolve.c:173-256): after the
+    // NVE step the momenta are scaled by chi = sqrt(1 + (T/inst_T - 1) dt /
+    // tau_T); the step's KE and inst_T are reported before the scaling, as
+    // the reference's globals hold them
+    const double inst = 2.0 * (ke * 0.5) / d.dof;
+    st.s2 = sqrt(1.00 + (d.T / inst - 1.00) * d.dt / 0.20);
+    kb = ke;
+    st.step += 1;
+    if (st.shuf) {
+      st.mt_cur ^= 1;
+      st.shuf = 0;
+    }
   } else if (mode == 0) {
-    if (d.thermostat) {
+    if (d.thermostat == 1) {
       double eta[NHC_M], pet[NHC_M];
       for (int k = 0; k < NHC_M; k++) {
         eta[k] = st.eta_cur[k];
@@ -1290,17 +1303,6 @@ __device__ void group_prologue(const View &v, const SysDesc &d, const GroupGeom 
   __syncthreads();
 }
 
-// half lists (SysDesc::half): a list entry with this bit is a partner in one
-// of the group's own cells, listed once per pair; its force reaches the
-// partner through the block's fixed-point accumulators
-constexpr unsigned LIST_CENTRE = 1u << 14;
-constexpr int HALF_MCAP = 384;  // centre particles a half-list group can hold
-// fixed-point unit of the accumulated forces: 2^-42 (integer sums do not
-// depend on the order of the additions; |F| stays below 2^21 per component)
-constexpr double FIX_SCALE = 4398046511104.0;
-constexpr double FIX_UNIT = 1.0 / 4398046511104.0;
-__device__ __forceinline__ bool inner_cell(int c, int nu) { return c >= 1 && c <= nu - 2; }
-
 __device__ __forceinline__ double shift_of(int code, int k) { return (double)(((code >> (2 * k)) & 3) - 1); }
 
 // staged coordinate of a particle of union cell u along dimension k: the
@@ -1378,8 +1380,6 @@ __global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
   const int Q = S.Q, M = S.M, nux = G.nu[0], nuy = G.nu[1];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int maxnb = v.maxnb;
-  const bool half = d.half;
-  int over = 0;
   if (Q <= v.gcap) {
     if (threadIdx.x == 0) {
       int m = 0;
@@ -1417,84 +1417,46 @@ __global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
       const int cu = S.cu[kc];
       const int m = S.cpre[kc + 1] - S.cpre[kc];
       const int ux = cu % nux, uy = (cu / nux) % nuy, uz = cu / (nux * nuy);
-      // lane l takes particles w0 + l and, when the cell holds more than 32
-      // (a warp-uniform case), also w0 + 32 + l in the same candidate sweep:
-      // a cell a little above a warp costs one sweep, not two
-      for (int w0 = 0; w0 < m; w0 += 64) {
-        const int w = w0 + lane, w2 = w + 32;
-        const bool valid = w < m, valid2 = w2 < m, has2 = m - w0 > 32;
+      for (int w0 = 0; w0 < m; w0 += 32) {
+        const int w = w0 + lane;
+        const bool valid = w < m;
         const int t = S.cpre[kc] + w, ps = pre4[cu] + w;
-        const int t2 = t + 32, ps2 = ps + 32;
         const float4 fi = valid ? stg[ps] : make_float4(-1e18f, -1e18f, -1e18f, __int_as_float(0));
-        const float4 fi2 = valid2 ? stg[ps2] : make_float4(-1e18f, -1e18f, -1e18f, __int_as_float(0));
-        const int ti = __float_as_int(fi.w) >> 15, ti2 = __float_as_int(fi2.w) >> 15;
+        const int ti = __float_as_int(fi.w) >> 15;
         // cut for a partner of type 0 / 1 (the sum of the two types indexes lc)
         const float c0 = ti == 0 ? lc[0] : lc[1], c1 = ti == 0 ? lc[1] : lc[2];
-        const float c02 = ti2 == 0 ? lc[0] : lc[1], c12 = ti2 == 0 ? lc[1] : lc[2];
-        ListWriter lw, lw2;
-        // half lists: first the partners in the group's own (centre) cells,
-        // each pair once (listed by the particle with the smaller staged
-        // index) and flagged LIST_CENTRE; then the halo partners.  Full
-        // lists: all neighbour cells in one pass.
-        for (int pass = half ? 0 : 1; pass < 2; pass++)
-          for (int dz = -1; dz <= 1; dz++)
-            for (int dy = -1; dy <= 1; dy++)
-              for (int dx = -1; dx <= 1; dx++) {
-                const bool cen = half && inner_cell(ux + dx, nux) && inner_cell(uy + dy, nuy) &&
-                                 inner_cell(uz + dz, G.nu[2]);
-                if (half && (pass == 0) != cen) continue;
-                const unsigned cflag = cen ? LIST_CENTRE : 0u;
-                const int u2 = (ux + dx) + (uy + dy) * nux + (uz + dz) * nux * nuy;
-                const int q1 = pre4[u2 + 1];
-                for (int q = pre4[u2]; q < q1; q += 4) {
-                  int code[4];
-                  bool ok[4], ok2[4];
+        ListWriter lw;
+        for (int dz = -1; dz <= 1; dz++)
+          for (int dy = -1; dy <= 1; dy++)
+            for (int dx = -1; dx <= 1; dx++) {
+              const int u2 = (ux + dx) + (uy + dy) * nux + (uz + dz) * nux * nuy;
+              const int q1 = pre4[u2 + 1];
+              for (int q = pre4[u2]; q < q1; q += 4) {
+                int code[4];
+                bool ok[4];
 #pragma unroll
-                  for (int e = 0; e < 4; e++) {
-                    const float4 fj = stg[q + e];
-                    code[e] = __float_as_int(fj.w);
-                    const bool tb = (code[e] >> 15) != 0;
-                    {
-                      const float ex = fi.x - fj.x, ey = fi.y - fj.y, ez = fi.z - fj.z;
-                      const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
-                      const float cut = one_cut ? c0 : (tb ? c1 : c0);
-                      ok[e] = valid && r2 < cut && (cen ? q + e > ps : q + e != ps);
-                    }
-                    ok2[e] = false;
-                    if (has2) {
-                      const float ex = fi2.x - fj.x, ey = fi2.y - fj.y, ez = fi2.z - fj.z;
-                      const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
-                      const float cut = one_cut ? c02 : (tb ? c12 : c02);
-                      ok2[e] = valid2 && r2 < cut && (cen ? q + e > ps2 : q + e != ps2);
-                    }
-                  }
-#pragma unroll
-                  for (int e = 0; e < 4; e++) {
-                    if (ok[e]) lw.add(((unsigned)code[e] & 0xffffu) | cflag, lst, M, t, maxnb);
-                    if (ok2[e]) lw2.add(((unsigned)code[e] & 0xffffu) | cflag, lst, M, t2, maxnb);
-                  }
+                for (int e = 0; e < 4; e++) {
+                  const float4 fj = stg[q + e];
+                  const float ex = fi.x - fj.x, ey = fi.y - fj.y, ez = fi.z - fj.z;
+                  const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+                  code[e] = __float_as_int(fj.w);
+                  const float cut = one_cut ? c0 : ((code[e] >> 15) ? c1 : c0);
+                  ok[e] = valid && r2 < cut && q + e != ps;
                 }
+#pragma unroll
+                for (int e = 0; e < 4; e++)
+                  if (ok[e]) lw.add((unsigned)code[e] & 0xffffu, lst, M, t, maxnb);
               }
+            }
         if (valid) {
           lw.finish(lst, M, t, maxnb);
+          const int n = lw.n;
           const int i = S.ustart[cu] + w;
-          if (lw.n > maxnb) {
+          if (n > maxnb) {
             v.nbn[i] = -1;
             atomicAdd(&v.st[r].overflow, 1);
-            over = 1;
           } else {
-            v.nbn[i] = lw.n;
-          }
-        }
-        if (valid2) {
-          lw2.finish(lst, M, t2, maxnb);
-          const int i = S.ustart[cu] + w2;
-          if (lw2.n > maxnb) {
-            v.nbn[i] = -1;
-            atomicAdd(&v.st[r].overflow, 1);
-            over = 1;
-          } else {
-            v.nbn[i] = lw2.n;
+            v.nbn[i] = n;
           }
         }
       }
@@ -1507,13 +1469,8 @@ __global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
       v.nbn[i] = -1;
       atomicAdd(&v.st[r].overflow, 1);
     }
-    over = 1;
   }
-  // a group with half lists falls back to the full cell scan for all its
-  // particles when one of them overflowed its row, the union did not fit, or
-  // it has more centre particles than the force kernel's accumulators
-  const int full = __syncthreads_or(over || (half && M > HALF_MCAP));
-  if (threadIdx.x == 0) v.gflag[d.goff + g] = full;
+  __syncthreads();
   for (int t = threadIdx.x; t < M; t += blockDim.x) {
     int kc, i, qs;
     group_centre(S, t, kc, i, qs);
@@ -1605,38 +1562,6 @@ __device__ __forceinline__ void pair_f32(PairAccF &a, float dx, float dy, float 
   a.vir = fmaf(g, dr2, a.vir);
 }
 
-// FP32 pair term of a half list: a pair listed once (LIST_CENTRE) counts
-// twice in pe and virial (the finaliser halves the sums, which count the
-// other pairs from both sides) and sends the partner its force, -f, through
-// the block's fixed-point accumulators acc[3][HALF_MCAP] (q2t: staged index ->
-// centre index)
-__device__ __forceinline__ void pair_f32_h(PairAccF &a, float dx, float dy, float dz, const PairParamsF &P,
-                                           int code, unsigned long long *acc, const short *q2t) {
-  const bool tj = code >> 15, cen = (code & LIST_CENTRE) != 0;
-  const float is2 = tj ? P.is2[1] : P.is2[0];
-  const float dr2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-  const float rs2 = dr2 * is2;
-  const bool in = rs2 < (float)KA_RC2;
-  const float wgt = cen ? 2.0f : 1.0f;
-  const float e4 = in ? (tj ? P.e4[1] : P.e4[0]) : 0.0f, ge = in ? (tj ? P.ge[1] : P.ge[0]) : 0.0f;
-  const float s2 = rcp_approx(rs2);
-  const float s6 = s2 * s2 * s2;
-  a.pe = fmaf(wgt * e4, fmaf(s6, s6, -s6) + fmaf((float)KA_C2, rs2, (float)KA_C0), a.pe);
-  const float g = ge * fmaf(s6 * fmaf(6.0f, s6, -3.0f), s2, -(float)KA_C2);
-  const float fx = g * dx, fy = g * dy, fz = g * dz;
-  a.fx += fx;
-  a.fy += fy;
-  a.fz += fz;
-  a.vir = fmaf(wgt * g, dr2, a.vir);
-  if (cen && in) {
-    const int tq = q2t[code & 0x3fff];
-    const float sc = (float)FIX_SCALE;
-    atomicAdd(acc + tq, (unsigned long long)__float2ll_rn(-fx * sc));
-    atomicAdd(acc + HALF_MCAP + tq, (unsigned long long)__float2ll_rn(-fy * sc));
-    atomicAdd(acc + 2 * HALF_MCAP + tq, (unsigned long long)__float2ll_rn(-fz * sc));
-  }
-}
-
 // FP64 pair constants of particle i against a partner of type 0 and of type 1:
 // 1/sigma^2, 4 eps and 8 eps/sigma^2 (MDcode/cell_list+forces.c:19-20)
 struct PairParamsD {
@@ -1674,41 +1599,13 @@ __device__ __forceinline__ void pair_f64(PairAcc &a, double dx, double dy, doubl
   }
 }
 
-// FP64 pair term of a half list (see pair_f32_h)
-__device__ __forceinline__ void pair_f64_h(PairAcc &a, double dx, double dy, double dz, const PairParamsD &P,
-                                           int code, unsigned long long *acc, const short *q2t) {
-  const bool tj = code >> 15, cen = (code & LIST_CENTRE) != 0;
-  const double is2 = tj ? P.is2[1] : P.is2[0];
-  const double dr2 = fma(dx, dx, fma(dy, dy, dz * dz));
-  const double rs2 = dr2 * is2;
-  if (rs2 < KA_RC2) {
-    const double wgt = cen ? 2.0 : 1.0;
-    const double e4 = tj ? P.e4[1] : P.e4[0], ge = tj ? P.ge[1] : P.ge[0];
-    const double s2 = rcp_nr(rs2);
-    const double s6 = s2 * s2 * s2;
-    a.pe = fma(wgt * e4, fma(s6, s6, -s6) + fma(KA_C2, rs2, KA_C0), a.pe);
-    const double g = ge * fma(s6 * fma(6.0, s6, -3.0), s2, -KA_C2);
-    const double fx = g * dx, fy = g * dy, fz = g * dz;
-    a.fx += fx;
-    a.fy += fy;
-    a.fz += fz;
-    a.vir = fma(wgt * g, dr2, a.vir);
-    if (cen) {
-      const int tq = q2t[code & 0x3fff];
-      atomicAdd(acc + tq, (unsigned long long)__double2ll_rn(-fx * FIX_SCALE));
-      atomicAdd(acc + HALF_MCAP + tq, (unsigned long long)__double2ll_rn(-fy * FIX_SCALE));
-      atomicAdd(acc + 2 * HALF_MCAP + tq, (unsigned long long)__double2ll_rn(-fz * FIX_SCALE));
-    }
-  }
-}
-
 // launch-bounds occupancy targets of the cell-group force kernel (blocks per
 // SM; measured best: 3 for both precisions, 80 registers without spills)
 #ifndef ACG_FORCE_MINB64
-#define ACG_FORCE_MINB64 3
+#define ACG_FORCE_MINB64 4
 #endif
 #ifndef ACG_FORCE_MINB32
-#define ACG_FORCE_MINB32 3
+#define ACG_FORCE_MINB32 4
 #endif
 
 // per-particle end of the force pass: active force (MDcode/cell_list+forces.c:
@@ -1796,22 +1693,8 @@ __global__ void __launch_bounds__(BLOCK_G, PREC ? ACG_FORCE_MINB32 : ACG_FORCE_M
   group_geom(g, d.nc, d.ng, G);
   group_prologue(v, d, G, S);
   const int Q = S.Q, M = S.M;
-  // half lists: pairs inside the group once, partner forces accumulated in
-  // fixed point in shared memory after the staged positions; a group the last
-  // rebuild marked full scans its cells instead
-  const bool hm = d.half && !v.gflag[d.goff + g] && M <= HALF_MCAP;
-  const bool staged = Q <= v.gcap && (hm || !d.half);
-  unsigned long long *acc = reinterpret_cast<unsigned long long *>(gsm_raw + 24 * (size_t)v.gcap);
-  short *q2t = reinterpret_cast<short *>(gsm_raw + 24 * (size_t)v.gcap + 3 * HALF_MCAP * sizeof(unsigned long long));
+  const bool staged = Q <= v.gcap;
   const double L = d.L;
-  if (hm) {
-    for (int k = threadIdx.x; k < 3 * HALF_MCAP; k += blockDim.x) acc[k] = 0ull;
-    for (int t = threadIdx.x; t < M; t += blockDim.x) {
-      int kc, i, qs;
-      group_centre(S, t, kc, i, qs);
-      q2t[qs] = (short)t;
-    }
-  }
   if (staged) {
     // one warp per union cell: coalesced loads, no search
     const int wl = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -1864,16 +1747,13 @@ __global__ void __launch_bounds__(BLOCK_G, PREC ? ACG_FORCE_MINB32 : ACG_FORCE_M
         for (int e = 0; e < 4; e++) {
           const int code = ((e < 2 ? w.x : w.y) >> (16 * (e & 1))) & 0xffff;
           if (e == 0 || k0 + e < nn) {
-            const int q = code & 0x3fff;
+            const int q = code & 0x7fff;
             const float4 hj = shi[q];
             const float2 lj = slo[q];
             const float dx = (hi.x - hj.x) + (hi.w - hj.w);
             const float dy = (hi.y - hj.y) + (li.x - lj.x);
             const float dz = (hi.z - hj.z) + (li.y - lj.y);
-            if (hm)
-              pair_f32_h(e & 1 ? fb : fa, dx, dy, dz, P, code, acc, q2t);
-            else
-              pair_f32(e & 1 ? fb : fa, dx, dy, dz, P, code >> 15);
+            pair_f32(e & 1 ? fb : fa, dx, dy, dz, P, code >> 15);
           }
         }
         flush_chunk(fa, fb, a);
@@ -1892,40 +1772,21 @@ __global__ void __launch_bounds__(BLOCK_G, PREC ? ACG_FORCE_MINB32 : ACG_FORCE_M
         const uint2 wn = c + TPP < nch ? __ldg(lp + (size_t)(c + TPP) * M) : make_uint2(0u, 0u);
         const int e0 = w.x & 0xffff, e1 = w.x >> 16, e2 = w.y & 0xffff, e3 = w.y >> 16;
         const int k0 = 4 * c;
-        if (hm) {
-          {
-            const int q = e0 & 0x3fff;
-            pair_f64_h(a, xi - sx[q], yi - sy[q], zi - sz[q], P, e0, acc, q2t);
-          }
-          if (k0 + 1 < nn) {
-            const int q = e1 & 0x3fff;
-            pair_f64_h(b, xi - sx[q], yi - sy[q], zi - sz[q], P, e1, acc, q2t);
-          }
-          if (k0 + 2 < nn) {
-            const int q = e2 & 0x3fff;
-            pair_f64_h(a, xi - sx[q], yi - sy[q], zi - sz[q], P, e2, acc, q2t);
-          }
-          if (k0 + 3 < nn) {
-            const int q = e3 & 0x3fff;
-            pair_f64_h(b, xi - sx[q], yi - sy[q], zi - sz[q], P, e3, acc, q2t);
-          }
-        } else {
-          {
-            const int q = e0 & 0x3fff;
-            pair_f64(a, xi - sx[q], yi - sy[q], zi - sz[q], P, e0 >> 15);
-          }
-          if (k0 + 1 < nn) {
-            const int q = e1 & 0x3fff;
-            pair_f64(b, xi - sx[q], yi - sy[q], zi - sz[q], P, e1 >> 15);
-          }
-          if (k0 + 2 < nn) {
-            const int q = e2 & 0x3fff;
-            pair_f64(a, xi - sx[q], yi - sy[q], zi - sz[q], P, e2 >> 15);
-          }
-          if (k0 + 3 < nn) {
-            const int q = e3 & 0x3fff;
-            pair_f64(b, xi - sx[q], yi - sy[q], zi - sz[q], P, e3 >> 15);
-          }
+        {
+          const int q = e0 & 0x7fff;
+          pair_f64(a, xi - sx[q], yi - sy[q], zi - sz[q], P, e0 >> 15);
+        }
+        if (k0 + 1 < nn) {
+          const int q = e1 & 0x7fff;
+          pair_f64(b, xi - sx[q], yi - sy[q], zi - sz[q], P, e1 >> 15);
+        }
+        if (k0 + 2 < nn) {
+          const int q = e2 & 0x7fff;
+          pair_f64(a, xi - sx[q], yi - sy[q], zi - sz[q], P, e2 >> 15);
+        }
+        if (k0 + 3 < nn) {
+          const int q = e3 & 0x7fff;
+          pair_f64(b, xi - sx[q], yi - sy[q], zi - sz[q], P, e3 >> 15);
         }
         w = wn;
       }
@@ -1964,27 +1825,7 @@ __global__ void __launch_bounds__(BLOCK_G, PREC ? ACG_FORCE_MINB32 : ACG_FORCE_M
       a.vir += __shfl_xor_sync(0xffffffffu, a.vir, o);
     }
     if (!valid || lane != 0) continue;
-    if (hm) {
-      // this particle's own side into its accumulator; the epilogue waits
-      // for the partners' contributions
-      pe += a.pe;
-      vir += a.vir;
-      atomicAdd(acc + t, (unsigned long long)__double2ll_rn(a.fx * FIX_SCALE));
-      atomicAdd(acc + HALF_MCAP + t, (unsigned long long)__double2ll_rn(a.fy * FIX_SCALE));
-      atomicAdd(acc + 2 * HALF_MCAP + t, (unsigned long long)__double2ll_rn(a.fz * FIX_SCALE));
-      continue;
-    }
     particle_epilogue(v, d, st, i, mode, a, pe, vir, ke, va);
-  }
-  if (hm) {
-    __syncthreads();
-    for (int t = threadIdx.x; t < M; t += blockDim.x) {
-      int kc, i, qs;
-      group_centre(S, t, kc, i, qs);
-      const PairAcc f = {(double)(long long)acc[t] * FIX_UNIT, (double)(long long)acc[HALF_MCAP + t] * FIX_UNIT,
-                         (double)(long long)acc[2 * HALF_MCAP + t] * FIX_UNIT, 0.0, 0.0};
-      particle_epilogue(v, d, st, i, mode, f, pe, vir, ke, va);
-    }
   }
   end_force_block(v, r, g, mode, pe, vir, ke, va);
 }

@@ -299,10 +299,14 @@ class Engine:
     def set_group_tpp(self, gtpp: int):
         check(self._lib.acg_set_group_tpp(self.h, int(gtpp)))
 
-    def set_group_half(self, on: bool):
-        """Half neighbour lists inside cell groups (pairs once, partner forces
-        in fixed point) or full lists."""
-        check(self._lib.acg_set_group_half(self.h, int(bool(on))))
+    def set_box_cells(self, cells: int):
+        """Cells per block of the whole-box kernels (1..8)."""
+        check(self._lib.acg_set_box_cells(self.h, int(cells)))
+
+    def get_box_cells(self) -> int:
+        c = C.c_int()
+        check(self._lib.acg_get_box_cells(self.h, C.byref(c)))
+        return c.value
 
     def get_launch(self):
         t, b = C.c_int(), C.c_int()

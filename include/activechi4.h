@@ -57,7 +57,10 @@ typedef struct acg_params {
   int list_mode;          /* 0: list cut 2.5+skin for all pairs (Cell_cut, global.h:29);
                              1: list cut 2.5*sigma_ab+skin per type pair */
   int thermostat;         /* 1: Nose-Hoover chain NVT (AdvanceTimeNVTNoseHoover);
-                             0: NVE velocity Verlet (advance_time_NVEFrog) */
+                             0: NVE velocity Verlet (advance_time_NVEFrog);
+                             2: Berendsen NVT, the momenta scaled by
+                                sqrt(1 + (T/inst_T - 1) dt/tau_T) after each step
+                                (advance_time_NVT_Berendsen, MDcode/time_evolve.c:173-256) */
   int shuffle;            /* re-randomise the active directions every tau_p_steps steps
                              (ShuffleActDirec cadence, MDcode/main.c:245-247):
                              1: on the device in the reference's order (per component,
@@ -288,13 +291,13 @@ int acg_get_launch(acg_engine *e, int *tpp, int *block);
  * >= 5 cells per side, or larger than the whole-box limit) and of the
  * whole-box force kernel (2 to 4 cells per side, N <= 8192). */
 int acg_set_group_tpp(acg_engine *e, int gtpp);
-/* Cell-group neighbour lists: 0 = full lists (every pair from both sides, as
- * the reference's force loop sees it per particle); 1 = half lists inside a
- * group (a pair of two particles of the group's own cells is computed once
- * and its partner's force summed in 2^-42 fixed point, so the result does not
- * depend on the order of the additions).  Rebuilds the lists and forces of
- * every system at the next call.  No counterpart in the reference. */
-int acg_set_group_half(acg_engine *e, int on);
+/* Cells per block of the whole-box kernels (systems with 3 or 4 cells per
+ * side; two-cell boxes keep one cell per block), 1 to 8: the partition of
+ * the force and list grids over the batch.  Results do not depend on it (the
+ * per-system sums are taken per particle, in slot order).  No counterpart in
+ * the reference. */
+int acg_set_box_cells(acg_engine *e, int cells);
+int acg_get_box_cells(acg_engine *e, int *cells);
 
 const char *acg_last_error(void);
 const char *acg_version(void);

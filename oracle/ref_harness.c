@@ -190,6 +190,15 @@ int ref_run(long start, int nsteps, int do_shuffle, int do_drift) {
 /* fixDrift (MDcode/initialise.c:104-138) */
 void ref_fix_drift(void) { fixDrift(); }
 
+/* advance_time_NVT_Berendsen (MDcode/time_evolve.c:173-256), nsteps times; a
+ * weak reference: the drop-in build does not provide it (returns -1 there) */
+void advance_time_NVT_Berendsen(void) __attribute__((weak));
+int ref_run_berendsen(int nsteps) {
+  if (!advance_time_NVT_Berendsen) return -1;
+  for (int i = 0; i < nsteps; i++) advance_time_NVT_Berendsen();
+  return 0;
+}
+
 /* one NVT step composed from the propagators, as AdvanceTimeNVTNoseHoover's
  * body does (MDcode/time_evolve.c:495-526) */
 void ref_step_propagators(void) {

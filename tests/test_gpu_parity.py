@@ -121,15 +121,13 @@ def test_oracle_random_states(cuda_lib):
         x, xu, p, _ = o.get_state()
         st.x, st.xu, st.p = x, xu, p
         Fo, pe, vir, va = Oracle.from_state(st, 1.0, 2.0).forces()
-        for half in (False, True):  # cell-group lists full, and half inside a group
-            e = Engine(default_params(n, T=1.0, f0=2.0, shuffle=0))
-            e.set_group_half(half)
-            e.set_state(0, st)
-            e.compute_forces()
-            assert force_err(e.get_state()[3], Fo) <= 1e-12, (n, half)
-            th = e.thermo()
-            assert rel(th["pe"], pe) <= 1e-12 and rel(th["virial"], vir) <= 1e-12, (n, half)
-            e.close()
+        e = Engine(default_params(n, T=1.0, f0=2.0, shuffle=0))
+        e.set_state(0, st)
+        e.compute_forces()
+        assert force_err(e.get_state()[3], Fo) <= 1e-12
+        th = e.thermo()
+        assert rel(th["pe"], pe) <= 1e-12 and rel(th["virial"], vir) <= 1e-12
+        e.close()
 
 
 def test_fp32_pair_forces(cuda_lib, g4000):

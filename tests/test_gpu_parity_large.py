@@ -50,11 +50,10 @@ def ref100k(s100k):
 P_ETA = np.array([0.05, -0.02, 0.01])
 
 
-def gpu(st, half=False, **kw):
+def gpu(st, **kw):
     from activechi4_b200 import Engine, default_params
     kw.setdefault("shuffle", 0)
     e = Engine(default_params(st.n, T=0.45, f0=1.0, **kw))
-    e.set_group_half(half)
     e.set_state(0, st)
     e.set_nhc(0, np.zeros(3), P_ETA)
     return e
@@ -75,30 +74,19 @@ def test_cells_forces_n100k(s100k, ref100k):
     assert abs(th["vir_act"] - va) <= 1e-12 * max(1.0, abs(va))
     assert th["overflow"] == 0
     e.close()
-    for half in (False, True):
-        e = gpu(s100k, half=half, precision=1)
-        e.compute_forces()
-        assert force_err(e.get_state()[3], Fr) <= 1e-5
-        e.close()
-    # half lists inside the cell groups (pairs once, partner forces in fixed point)
-    e = gpu(s100k, half=True)
+    e = gpu(s100k, precision=1)
     e.compute_forces()
-    th = e.thermo()
-    assert force_err(e.get_state()[3], Fr) <= 1e-12
-    assert rel(th["pe"], pe) <= 1e-12 and rel(th["virial"], vir) <= 1e-12
-    assert abs(th["vir_act"] - va) <= 1e-12 * max(1.0, abs(va))
+    assert force_err(e.get_state()[3], Fr) <= 1e-5
     e.close()
 
 
-@pytest.mark.parametrize("half", [False, True])
-def test_nvt_50_steps_n100k(s100k, ref100k, half):
+def test_nvt_50_steps_n100k(s100k, ref100k):
     """The run loop's first 50 steps: shuffle at step 0 (device MT19937 with
-    the reference's seed), NHC NVT, the drift removal after step 0; full and
-    half cell-group lists."""
+    the reference's seed), NHC NVT, the drift removal after step 0."""
     ref100k.setup(s100k, 0.45, 1.0, p_eta=P_ETA)
     ref100k.seed_rng(606)
     nref = ref100k.run(50, start=0, shuffle=True, drift=True)
-    e = gpu(s100k, half=half, shuffle=1, seed=606)
+    e = gpu(s100k, shuffle=1, seed=606)
     e.step(50)
     th = e.thermo()
     assert th["step"] == 50
@@ -134,14 +122,7 @@ def test_forces_n256k_against_oracle(cuda_lib):
     assert force_err(e.get_state()[3], Fo) <= 1e-12
     assert rel(th["pe"], pe) <= 1e-12 and rel(th["virial"], vir) <= 1e-12
     e.close()
-    for half in (False, True):
-        e = gpu(st, half=half)
-        e.compute_forces()
-        th = e.thermo()
-        assert force_err(e.get_state()[3], Fo) <= 1e-12
-        assert rel(th["pe"], pe) <= 1e-12 and rel(th["virial"], vir) <= 1e-12
-        e.close()
-        e = gpu(st, half=half, precision=1)
-        e.compute_forces()
-        assert force_err(e.get_state()[3], Fo) <= 1e-5
-        e.close()
+    e = gpu(st, precision=1)
+    e.compute_forces()
+    assert force_err(e.get_state()[3], Fo) <= 1e-5
+    e.close()
