@@ -112,6 +112,14 @@ struct SysState {
   double ramp_end;           // the ramp's final temperature (target of the padding steps)
   long long ramp_left;       // ramp steps still to run (NVE with a velocity rescale before each)
   long long ramp_real;       // of these, steps of the ramp itself; the rest hold ramp_end
+  // Gaussian isokinetic integrator (thermostat 3): the next first half kick
+  // is p = s1 (p + g1 F); ga = this step's second half kick p = ga0 (p + ga1 F);
+  // gmode = work due in the Gaussian kernels after the forces (1: the second
+  // half kick and the next first half, 2: the next first half only)
+  double g1;
+  double ga[2];
+  int gmode;
+  unsigned int counter_g;    // last-block counter of the Gaussian kernels
 };
 
 // In-place observables of one system (set by acg_obs_configure): events of the

@@ -91,7 +91,7 @@ int resolve(const acg_params &p, SysDesc &d) {
   d.seed = p.seed;
   if (p.dt <= 0 || p.skin <= 0 || p.rebuild_factor <= 0)
     return fail(ACG_ERR_INVALID, "dt, skin and rebuild_factor must be positive");
-  if (p.thermostat < 0 || p.thermostat > 2) return fail(ACG_ERR_INVALID, "thermostat must be 0, 1 or 2");
+  if (p.thermostat < 0 || p.thermostat > 3) return fail(ACG_ERR_INVALID, "thermostat must be 0, 1, 2 or 3");
   if (p.thermostat && !(p.T > 0)) return fail(ACG_ERR_INVALID, "thermostat needs T > 0");
   if (p.shuffle < 0 || p.shuffle > 2) return fail(ACG_ERR_INVALID, "shuffle must be 0, 1 or 2");
   if (p.shuffle && p.tau_p_steps <= 0) return fail(ACG_ERR_INVALID, "shuffle needs tau_p_steps > 0");
@@ -231,6 +231,7 @@ struct acg_engine {
   int2 *d_tiles_x = nullptr;
   std::vector<int> dirty;  // systems whose forces/lists must be recomputed
   bool any_dirty = false;
+  bool any_gauss = false;  // a system runs the Gaussian isokinetic integrator (thermostat 3)
   cudaGraphExec_t gexec = nullptr;
   cudaGraph_t graph = nullptr;
   int gsteps = 0;
@@ -265,7 +266,8 @@ GroupFn group_fn(int gtpp, int prec) {
   }
   return nullptr;
 }
-size_t group_smem(int gcap) { return 3 * (size_t)gcap * sizeof(double); }
+// group force kernel: 24 bytes per staged particle and one dummy slot
+size_t group_smem(int gcap) { return 3 * ((size_t)gcap + 1) * sizeof(double); }
 size_t list_smem(int gcap) { return ((size_t)gcap + 3 * MAX_UNION) * sizeof(float4); }
 
 GroupFn box_fn(int gtpp, int prec) {
@@ -470,6 +472,14 @@ int launch_force(acg_engine *e, int mode) {
   return ACG_OK;
 }
 
+// the Gaussian isokinetic kernels: the second half kick and the next first
+// half (with_sum, after a step's forces) or the next first half only
+void launch_gauss(acg_engine *e, bool with_sum) {
+  if (!e->any_gauss) return;
+  if (with_sum) k_gauss_sum<<<e->ntiles_a, BLOCK_A, 0, e->stream>>>(e->v);
+  k_gauss_apply<<<e->ntiles_a, BLOCK_A, 0, e->stream>>>(e->v);
+}
+
 int launch_step_eager(acg_engine *e) {
   k_kick_drift<<<e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, 0, e->stream>>>(e->v, 0, 0, 0, 0);
   k_shuffle_ref<<<3 * e->lay.nsys, BLOCK_SHUF, shuffle_smem(e->lay), e->stream>>>(e->v, -1);
@@ -478,8 +488,10 @@ int launch_step_eager(acg_engine *e) {
   if (rc) return rc;
   rc = launch_force(e, 0);
   if (rc) return rc;
+  launch_gauss(e, true);
   k_drift_sum<<<e->ntiles_a, BLOCK_A, 0, e->stream>>>(e->v);
   k_drift_apply<<<e->ntiles_a, BLOCK_A, 0, e->stream>>>(e->v);
+  launch_gauss(e, false);
   k_observe<<<e->ntiles_a, BLOCK_A, 0, e->stream>>>(e->v);
   CK(cudaGetLastError());
   return ACG_OK;
@@ -500,6 +512,8 @@ int prime(acg_engine *e) {
   if (rc) return rc;
   rc = launch_force(e, 1);
   if (rc) return rc;
+  launch_gauss(e, false);
+  CK(cudaGetLastError());
   e->any_dirty = false;
   return ACG_OK;
 }
@@ -613,6 +627,16 @@ int add_steps(acg_engine *e, cudaGraph_t g, int K, cudaGraphNode_t *prev_io) {
       dep = &last;
       ndep = 1;
     }
+    if (e->any_gauss) {  // Gaussian isokinetic: second half kick, next first half
+      rc = add_kernel(g, dep, ndep, &nb, (void *)k_gauss_sum, e->ntiles_a, BLOCK_A, va);
+      if (rc) return rc;
+      last = nb;
+      dep = &last;
+      ndep = 1;
+      rc = add_kernel(g, dep, ndep, &nb, (void *)k_gauss_apply, e->ntiles_a, BLOCK_A, va);
+      if (rc) return rc;
+      last = nb;
+    }
     // after the step: drift removal and observables at the scheduled steps
     // (device-decided, like the rebuild)
     cudaGraphNodeParams op = {};
@@ -627,6 +651,12 @@ int add_steps(acg_engine *e, cudaGraph_t g, int K, cudaGraphNode_t *prev_io) {
     if (rc) return rc;
     rc = add_kernel(ob, &nk0, 1, &nk1, (void *)k_drift_apply, e->ntiles_a, BLOCK_A, va);
     if (rc) return rc;
+    if (e->any_gauss) {  // the first half after a drift removal
+      cudaGraphNode_t nkg;
+      rc = add_kernel(ob, &nk1, 1, &nkg, (void *)k_gauss_apply, e->ntiles_a, BLOCK_A, va);
+      if (rc) return rc;
+      nk1 = nkg;
+    }
     rc = add_kernel(ob, &nk1, 1, &nk2, (void *)k_observe, e->ntiles_a, BLOCK_A, va);
     if (rc) return rc;
     prev = no;
@@ -776,6 +806,7 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
     return rc;
   }
   e->device = device;
+  for (int r = 0; r < nsys; r++) e->any_gauss |= e->lay.desc[r].thermostat == 3;
   cudaError_t ce = cudaSetDevice(device);
   if (ce != cudaSuccess) {
     delete e;
@@ -1163,6 +1194,7 @@ int acg_fix_drift(acg_engine *e, int sys) {
   k_flag_drift<<<1, 32, 0, e->stream>>>(e->v, sys);
   k_drift_sum<<<e->ntiles_a, BLOCK_A, 0, e->stream>>>(e->v);
   k_drift_apply<<<e->ntiles_a, BLOCK_A, 0, e->stream>>>(e->v);
+  launch_gauss(e, false);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(e->stream));
   return ACG_OK;
@@ -1176,6 +1208,7 @@ int acg_adjust_temperature(acg_engine *e, int sys, double T, double *inst_T) {
   rc = prime(e);
   if (rc) return rc;
   k_rescale<<<1, 1024, 0, e->stream>>>(e->v, sys, T);
+  launch_gauss(e, false);
   CK(cudaGetLastError());
   double ke = 0;
   CK(cudaMemcpyAsync(&ke, &e->v.st[sys].ke_end, sizeof(double), cudaMemcpyDeviceToHost, e->stream));
@@ -1190,6 +1223,8 @@ int acg_start_ramp(acg_engine *e, int sys, double T_start, double T_end, double 
   if (!(T_start > 0) || !(T_end > 0) || !(rate > 0) || !std::isfinite(T_start) || !std::isfinite(T_end))
     return fail(ACG_ERR_INVALID, "ramp temperatures and rate must be positive");
   const SysDesc &d = e->lay.desc[sys];
+  if (d.thermostat == 3)
+    return fail(ACG_ERR_INVALID, "temperature ramps run on NVE, Nose-Hoover or Berendsen systems, not Gaussian isokinetic");
   double T0 = 0;
   rc = acg_adjust_temperature(e, sys, T_start, &T0);
   if (rc) return rc;
@@ -1280,6 +1315,7 @@ int acg_set_nhc(acg_engine *e, int sys, const double *eta3, const double *p_eta3
     return ACG_OK;
   }
   k_prehalf<<<1, 1, 0, e->stream>>>(e->v, sys);
+  launch_gauss(e, false);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(e->stream));
   return ACG_OK;
@@ -1295,7 +1331,10 @@ int acg_set_temperature(acg_engine *e, int sys, double T) {
   d.q[0] = d.dof * T * TAU_T * TAU_T;
   CK(cudaSetDevice(e->device));
   CK(cudaMemcpyAsync(e->d_desc + sys, &d, sizeof(SysDesc), cudaMemcpyHostToDevice, e->stream));
-  if (!e->dirty[sys]) k_prehalf<<<1, 1, 0, e->stream>>>(e->v, sys);
+  if (!e->dirty[sys]) {
+    k_prehalf<<<1, 1, 0, e->stream>>>(e->v, sys);
+    launch_gauss(e, false);
+  }
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(e->stream));
   return ACG_OK;
@@ -1756,8 +1795,9 @@ int acg_bench_steps(acg_engine *e, int64_t nsteps, size_t flush_bytes, double *m
   // and each force kernel in use; a step whose rebuild branch is taken the
   // rebuild kernels with a non-empty grid; a step with a reference-order
   // shuffle the shuffle kernel; a step with a drift removal or observable
-  // events the three kernels of that branch (the node lists of add_steps)
-  const long long per_step = 1 + (e->ntiles_g > 0) + (e->ntiles_x > 0) + (e->ntiles_b > 0);
+  // events the three kernels of that branch (the node lists of add_steps);
+  // with a Gaussian isokinetic system two more per step and one more per branch
+  const long long per_step = 1 + (e->ntiles_g > 0) + (e->ntiles_x > 0) + (e->ntiles_b > 0) + 2 * e->any_gauss;
   const long long per_rebuild = 5 + (e->lay.box_m3max > 0) + 2 * (e->ntiles_x > 0) + (e->ntiles_g > 0) +
                                 (e->ntiles_l > 0);
   long long steps_with_rebuild = 0, shuffles = 0, posts = 0;
@@ -1775,7 +1815,7 @@ int acg_bench_steps(acg_engine *e, int64_t nsteps, size_t flush_bytes, double *m
     shuffles += shuf;
     posts += post;
   }
-  *launches = per_step * nsteps + per_rebuild * steps_with_rebuild + shuffles + 3 * posts;
+  *launches = per_step * nsteps + per_rebuild * steps_with_rebuild + shuffles + (3 + e->any_gauss) * posts;
   return ACG_OK;
 }
 

@@ -235,12 +235,22 @@ __global__ void k_mt_flip(View v, int r) {
 // U3 U2 (pending thermostat scales and the half kick) and U1 for one
 // particle, in the reference's order of roundings; returns |x_u - x_old|^2
 // (reduced units) for the rebuild test
-__device__ __forceinline__ double kick_drift_one(const View &v, const SysDesc &d, int i, double s1, double s2) {
+__device__ __forceinline__ double kick_drift_one(const View &v, const SysDesc &d, int i, double s1, double s2,
+                                                 double g1, bool gauss) {
   const double hdt = d.half_dt, dt = d.dt, il = d.invL;
-  // v_b * s1 + F dt/2
-  double px = __dadd_rn(__dmul_rn(__dmul_rn(v.vx[i], s2), s1), __dmul_rn(v.fx[i], hdt));
-  double py = __dadd_rn(__dmul_rn(__dmul_rn(v.vy[i], s2), s1), __dmul_rn(v.fy[i], hdt));
-  double pz = __dadd_rn(__dmul_rn(__dmul_rn(v.vz[i], s2), s1), __dmul_rn(v.fz[i], hdt));
+  double px, py, pz;
+  if (gauss) {
+    // Gaussian isokinetic half kick p = factor1 (p + factor2 F)
+    // (MDcode/time_evolve.c:388-394)
+    px = __dmul_rn(s1, __dadd_rn(__dmul_rn(v.vx[i], s2), __dmul_rn(g1, v.fx[i])));
+    py = __dmul_rn(s1, __dadd_rn(__dmul_rn(v.vy[i], s2), __dmul_rn(g1, v.fy[i])));
+    pz = __dmul_rn(s1, __dadd_rn(__dmul_rn(v.vz[i], s2), __dmul_rn(g1, v.fz[i])));
+  } else {
+    // v_b * s1 + F dt/2
+    px = __dadd_rn(__dmul_rn(__dmul_rn(v.vx[i], s2), s1), __dmul_rn(v.fx[i], hdt));
+    py = __dadd_rn(__dmul_rn(__dmul_rn(v.vy[i], s2), s1), __dmul_rn(v.fy[i], hdt));
+    pz = __dadd_rn(__dmul_rn(__dmul_rn(v.vz[i], s2), s1), __dmul_rn(v.fz[i], hdt));
+  }
   double ddx = __dmul_rn(__dmul_rn(px, dt), il);
   double ddy = __dmul_rn(__dmul_rn(py, dt), il);
   double ddz = __dmul_rn(__dmul_rn(pz, dt), il);
@@ -312,7 +322,10 @@ __global__ void __launch_bounds__(BLOCK_A) k_kick_drift(View v, int use_cond, cu
     r = t.x;
     const SysDesc &d = v.desc[r];
     int loc = t.y + threadIdx.x;
-    if (loc < d.n) mymax = kick_drift_one(v, d, d.poff + loc, v.st[r].s1, v.st[r].s2);
+    if (loc < d.n) {
+      const SysState &st = v.st[r];
+      mymax = kick_drift_one(v, d, d.poff + loc, st.s1, st.s2, st.g1, d.thermostat == 3);
+    }
     // per-system block max (a tile never straddles systems)
     for (int o = 16; o > 0; o >>= 1) mymax = fmax(mymax, __shfl_down_sync(0xffffffffu, mymax, o));
     if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = mymax;
@@ -827,6 +840,12 @@ __device__ void next_first_half(const SysDesc &d, SysState &st, double kb) {
       st.p_eta_cur[k] = pet[k];
     }
     st.s1 = s1;
+  } else if (d.thermostat == 3) {
+    // Gaussian isokinetic: the factors need sums of p.F and F^2 over the
+    // system; k_gauss_apply computes them (no half kick until it has run)
+    st.s1 = 1.0;
+    st.g1 = 0.0;
+    st.gmode = 2;
   } else {
     st.s1 = 1.0;
   }
@@ -864,6 +883,17 @@ __device__ void finalize_sums(const SysDesc &d, SysState &st, int mode, double p
       st.mt_cur ^= 1;
       st.shuf = 0;
     }
+  } else if (mode == 0 && d.thermostat == 3) {
+    // AdvanceTimeNVTGaussOSM (MDcode/time_evolve.c:351-470): the second half
+    // kick and the next first half need sums over the new forces; the
+    // Gaussian kernels after this pass apply them (gmode 1)
+    st.s2 = 1.0;
+    kb = ke;
+    st.step += 1;
+    if (st.shuf) {
+      st.mt_cur ^= 1;
+      st.shuf = 0;
+    }
   } else if (mode == 0) {
     if (d.thermostat == 1) {
       double eta[NHC_M], pet[NHC_M];
@@ -893,6 +923,7 @@ __device__ void finalize_sums(const SysDesc &d, SysState &st, int mode, double p
   }
   st.ke_end = kb * 0.5;
   next_first_half(d, st, kb);
+  if (mode == 0 && d.thermostat == 3 && st.gmode == 2) st.gmode = 1;
   if (!(ke == ke) || ke > 1.0e300) st.status = 1;
   st.prime = 0;
   __threadfence();
@@ -984,6 +1015,129 @@ __global__ void __launch_bounds__(BLOCK_A) k_drift_apply(View v) {
   st.drift = 0;
   __threadfence();
   st.counter_d = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Gaussian isokinetic thermostat (AdvanceTimeNVTGaussOSM, MDcode/time_evolve.c:
+// 351-470).  Each half kick p = factor1 (p + factor2 F) takes its factors from
+// X1 = sum p.F, X2 = sum F^2 and K0 = sum p^2 over the system:
+// alpha = sqrt(X2/K0), zeta0 = -X1/K0, beta = exp(-alpha dt/2),
+// gamma = (zeta0 - alpha)/(zeta0 + alpha), factor1 = (1 - gamma)/(beta -
+// gamma/beta), factor2 = (1 + gamma - beta - gamma/beta)/((1 - gamma) alpha).
+// With F = 0 or p = 0 these are 0/0; the limit (p unchanged) is used there.
+__device__ __forceinline__ void gauss_factors(double x1, double x2, double k0, double dt, double &f1,
+                                              double &f2) {
+  if (!(x2 > 0.0) || !(k0 > 0.0)) {
+    f1 = 1.0;
+    f2 = 0.0;
+    return;
+  }
+  const double alpha = sqrt(x2 / k0);
+  const double zeta0 = -x1 / k0;
+  const double beta = exp(-alpha * dt * 0.5);
+  const double gamma = (zeta0 - alpha) / (zeta0 + alpha);
+  f1 = (1.0 - gamma) / (beta - gamma / beta);
+  f2 = (1.0 + gamma - beta - gamma / beta) / ((1.0 - gamma) * alpha);
+}
+
+// block sums of one tile's X1, X2, K0 into the tile's partial slot; returns
+// (in every thread) whether this block is the system's last (counter_g)
+__device__ __forceinline__ bool gauss_block_sums(const View &v, const SysDesc &d, SysState &st, double x1,
+                                                 double x2, double k0) {
+  __shared__ double sh[BLOCK_A / 32];
+  __shared__ int s_last;
+  x1 = block_sum<BLOCK_A / 32>(x1, sh);
+  x2 = block_sum<BLOCK_A / 32>(x2, sh);
+  k0 = block_sum<BLOCK_A / 32>(k0, sh);
+  double *part = v.part_o + (size_t)blockIdx.x * OBS_EMAX * OBS_NV;
+  if (threadIdx.x == 0) {
+    part[0] = x1;
+    part[1] = x2;
+    part[2] = k0;
+    __threadfence();
+    s_last = atomicAdd(&st.counter_g, 1u) == (unsigned)(d.ntile_a - 1);
+  }
+  __syncthreads();
+  return s_last != 0;
+}
+
+// the system's X1, X2, K0 from the tile partials, in tile order
+__device__ __forceinline__ void gauss_totals(const View &v, const SysDesc &d, double &x1, double &x2,
+                                             double &k0) {
+  __threadfence();
+  x1 = x2 = k0 = 0.0;
+  for (int b = 0; b < d.ntile_a; b++) {
+    const double *pb = v.part_o + (size_t)(d.tile0_a + b) * OBS_EMAX * OBS_NV;
+    x1 += __ldcg(pb);
+    x2 += __ldcg(pb + 1);
+    k0 += __ldcg(pb + 2);
+  }
+}
+
+// after a step's forces (gmode 1): the sums over the momenta after the first
+// half kick and drift and the new forces give the second half kick's factors
+__global__ void __launch_bounds__(BLOCK_A) k_gauss_sum(View v) {
+  const int2 t = v.tiles_a[blockIdx.x];
+  const int r = t.x;
+  SysState &st = v.st[r];
+  if (st.gmode != 1) return;
+  const SysDesc &d = v.desc[r];
+  const int loc = t.y + threadIdx.x;
+  double x1 = 0.0, x2 = 0.0, k0 = 0.0;
+  if (loc < d.n) {
+    const int i = d.poff + loc;
+    const double px = v.vx[i], py = v.vy[i], pz = v.vz[i];
+    const double fx = v.fx[i], fy = v.fy[i], fz = v.fz[i];
+    x1 = px * fx + py * fy + pz * fz;
+    x2 = fx * fx + fy * fy + fz * fz;
+    k0 = px * px + py * py + pz * pz;
+  }
+  if (!gauss_block_sums(v, d, st, x1, x2, k0) || threadIdx.x != 0) return;
+  gauss_totals(v, d, x1, x2, k0);
+  gauss_factors(x1, x2, k0, d.dt, st.ga[0], st.ga[1]);
+  __threadfence();
+  st.counter_g = 0;
+}
+
+// the second half kick (gmode 1) or none (gmode 2: after a host change of the
+// momenta, a drift removal or a rescale), then the sums over the momenta at the
+// step boundary give the next step's first half kick factors (s1, g1); KE at
+// the boundary as the reference reports it (0.5 sum p^2)
+__global__ void __launch_bounds__(BLOCK_A) k_gauss_apply(View v) {
+  const int2 t = v.tiles_a[blockIdx.x];
+  const int r = t.x;
+  SysState &st = v.st[r];
+  const int gm = st.gmode;
+  if (gm == 0) return;
+  const SysDesc &d = v.desc[r];
+  const int loc = t.y + threadIdx.x;
+  double x1 = 0.0, x2 = 0.0, k0 = 0.0;
+  if (loc < d.n) {
+    const int i = d.poff + loc;
+    double px = v.vx[i], py = v.vy[i], pz = v.vz[i];
+    const double fx = v.fx[i], fy = v.fy[i], fz = v.fz[i];
+    if (gm == 1) {
+      const double f1 = st.ga[0], f2 = st.ga[1];
+      px = __dmul_rn(f1, __dadd_rn(px, __dmul_rn(f2, fx)));
+      py = __dmul_rn(f1, __dadd_rn(py, __dmul_rn(f2, fy)));
+      pz = __dmul_rn(f1, __dadd_rn(pz, __dmul_rn(f2, fz)));
+      v.vx[i] = px;
+      v.vy[i] = py;
+      v.vz[i] = pz;
+    }
+    x1 = px * fx + py * fy + pz * fz;
+    x2 = fx * fx + fy * fy + fz * fz;
+    k0 = px * px + py * py + pz * pz;
+  }
+  if (!gauss_block_sums(v, d, st, x1, x2, k0) || threadIdx.x != 0) return;
+  gauss_totals(v, d, x1, x2, k0);
+  gauss_factors(x1, x2, k0, d.dt, st.s1, st.g1);
+  st.s2 = 1.0;
+  st.ke_end = k0 * 0.5;
+  if (!(k0 == k0) || k0 > 1.0e300) st.status = 1;
+  st.gmode = 0;
+  __threadfence();
+  st.counter_g = 0;
 }
 
 // host request: remove the mean momentum of system r now (with k_drift_sum and
@@ -1186,6 +1340,10 @@ __global__ void __launch_bounds__(512) k_force_kick(View v, int mode, int tile_b
     double px, py, pz;
     if (mode == 2) {
       px = py = pz = 0.0;
+    } else if (mode == 0 && d.thermostat == 3) {  // Gaussian: the kick waits for k_gauss_sum
+      px = v.vx[i];
+      py = v.vy[i];
+      pz = v.vz[i];
     } else if (mode == 0) {  // U2 (MDcode/time_evolve.c:558-567)
       px = __dadd_rn(v.vx[i], __dmul_rn(fx, d.half_dt));
       py = __dadd_rn(v.vy[i], __dmul_rn(fy, d.half_dt));
@@ -1351,10 +1509,11 @@ struct ListWriter {
     if ((n & 3) == 0 && n <= maxnb) lst[(size_t)((n >> 2) - 1) * stride + row] = make_uint2(lo, hi);
   }
   // the last, partial chunk: its k pending entries sit in the top 16k bits
-  __device__ __forceinline__ void finish(uint2 *lst, size_t stride, int row, int maxnb) {
+  __device__ __forceinline__ void finish(uint2 *lst, size_t stride, int row, int maxnb, unsigned pad = 0u) {
     const int k = n & 3;
     if (k && n <= maxnb) {
-      const unsigned long long p = (((unsigned long long)hi << 32) | lo) >> (16 * (4 - k));
+      unsigned long long p = (((unsigned long long)hi << 32) | lo) >> (16 * (4 - k));
+      for (int e = k; e < 4; e++) p |= (unsigned long long)pad << (16 * e);
       lst[(size_t)(n >> 2) * stride + row] = make_uint2((unsigned)p, (unsigned)(p >> 32));
     }
   }
@@ -1449,7 +1608,7 @@ __global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
               }
             }
         if (valid) {
-          lw.finish(lst, M, t, maxnb);
+          lw.finish(lst, M, t, maxnb, (unsigned)v.gcap);
           const int n = lw.n;
           const int i = S.ustart[cu] + w;
           if (n > maxnb) {
@@ -1630,20 +1789,23 @@ __device__ __forceinline__ void particle_epilogue(const View &v, const SysDesc &
   v.fz[i] = fz;
   if (mode != 2) {
     const double vx0 = v.vx[i], vy0 = v.vy[i], vz0 = v.vz[i];
-    double px, py, pz;
-    if (mode == 0) {
+    double px = vx0, py = vy0, pz = vz0;
+    if (mode == 0 && d.thermostat != 3) {
       px = __dadd_rn(vx0, __dmul_rn(fx, d.half_dt));
       py = __dadd_rn(vy0, __dmul_rn(fy, d.half_dt));
       pz = __dadd_rn(vz0, __dmul_rn(fz, d.half_dt));
-    } else {
+    } else if (mode != 0) {
       const double s2 = st.s2;
       px = __dmul_rn(vx0, s2);
       py = __dmul_rn(vy0, s2);
       pz = __dmul_rn(vz0, s2);
     }
-    v.vx[i] = px;
-    v.vy[i] = py;
-    v.vz[i] = pz;
+    // (Gaussian isokinetic step: the second half kick waits for k_gauss_sum)
+    if (mode != 0 || d.thermostat != 3) {
+      v.vx[i] = px;
+      v.vy[i] = py;
+      v.vz[i] = pz;
+    }
     ke += px * px + py * py + pz * pz;
   }
   pe += a.pe;
@@ -1680,9 +1842,12 @@ __global__ void __launch_bounds__(BLOCK_G, PREC ? ACG_FORCE_MINB32 : ACG_FORCE_M
   // 24 bytes per staged particle either way
   extern __shared__ __align__(16) unsigned char gsm_raw[];
   double *gsm = reinterpret_cast<double *>(gsm_raw);
-  double *sx = gsm, *sy = gsm + v.gcap, *sz = gsm + 2 * v.gcap;
+  // one slot past the union (index gcap) holds a far-away dummy that pads
+  // the last list chunk of every particle, so chunks need no length tests
+  const int gs = v.gcap + 1;
+  double *sx = gsm, *sy = gsm + gs, *sz = gsm + 2 * gs;
   float4 *shi = reinterpret_cast<float4 *>(gsm_raw);
-  float2 *slo = reinterpret_cast<float2 *>(gsm_raw + 16 * (size_t)v.gcap);
+  float2 *slo = reinterpret_cast<float2 *>(gsm_raw + 16 * (size_t)gs);
   __shared__ GroupStage S;
   const int2 tile = v.tiles_g[blockIdx.x];
   const int r = tile.x, g = tile.y;
@@ -1696,6 +1861,16 @@ __global__ void __launch_bounds__(BLOCK_G, PREC ? ACG_FORCE_MINB32 : ACG_FORCE_M
   const bool staged = Q <= v.gcap;
   const double L = d.L;
   if (staged) {
+    if (threadIdx.x == 0) {
+      if (PREC == 0) {
+        sx[v.gcap] = 1e18;
+        sy[v.gcap] = 1e18;
+        sz[v.gcap] = 1e18;
+      } else {
+        shi[v.gcap] = make_float4(1e18f, 1e18f, 1e18f, 0.0f);
+        slo[v.gcap] = make_float2(0.0f, 0.0f);
+      }
+    }
     // one warp per union cell: coalesced loads, no search
     const int wl = threadIdx.x & 31, nw = blockDim.x >> 5;
     for (int u = threadIdx.x >> 5; u < S.nU; u += nw) {
@@ -1742,19 +1917,16 @@ __global__ void __launch_bounds__(BLOCK_G, PREC ? ACG_FORCE_MINB32 : ACG_FORCE_M
       uint2 w = lane < nch ? __ldg(lp + (size_t)lane * M) : make_uint2(0u, 0u);
       for (int c = lane; c < nch; c += TPP) {
         const uint2 wn = c + TPP < nch ? __ldg(lp + (size_t)(c + TPP) * M) : make_uint2(0u, 0u);
-        const int k0 = 4 * c;
 #pragma unroll
         for (int e = 0; e < 4; e++) {
           const int code = ((e < 2 ? w.x : w.y) >> (16 * (e & 1))) & 0xffff;
-          if (e == 0 || k0 + e < nn) {
-            const int q = code & 0x7fff;
-            const float4 hj = shi[q];
-            const float2 lj = slo[q];
-            const float dx = (hi.x - hj.x) + (hi.w - hj.w);
-            const float dy = (hi.y - hj.y) + (li.x - lj.x);
-            const float dz = (hi.z - hj.z) + (li.y - lj.y);
-            pair_f32(e & 1 ? fb : fa, dx, dy, dz, P, code >> 15);
-          }
+          const int q = code & 0x7fff;
+          const float4 hj = shi[q];
+          const float2 lj = slo[q];
+          const float dx = (hi.x - hj.x) + (hi.w - hj.w);
+          const float dy = (hi.y - hj.y) + (li.x - lj.x);
+          const float dz = (hi.z - hj.z) + (li.y - lj.y);
+          pair_f32(e & 1 ? fb : fa, dx, dy, dz, P, code >> 15);
         }
         flush_chunk(fa, fb, a);
         w = wn;
@@ -1771,20 +1943,19 @@ __global__ void __launch_bounds__(BLOCK_G, PREC ? ACG_FORCE_MINB32 : ACG_FORCE_M
       for (int c = lane; c < nch; c += TPP) {
         const uint2 wn = c + TPP < nch ? __ldg(lp + (size_t)(c + TPP) * M) : make_uint2(0u, 0u);
         const int e0 = w.x & 0xffff, e1 = w.x >> 16, e2 = w.y & 0xffff, e3 = w.y >> 16;
-        const int k0 = 4 * c;
         {
           const int q = e0 & 0x7fff;
           pair_f64(a, xi - sx[q], yi - sy[q], zi - sz[q], P, e0 >> 15);
         }
-        if (k0 + 1 < nn) {
+        {
           const int q = e1 & 0x7fff;
           pair_f64(b, xi - sx[q], yi - sy[q], zi - sz[q], P, e1 >> 15);
         }
-        if (k0 + 2 < nn) {
+        {
           const int q = e2 & 0x7fff;
           pair_f64(a, xi - sx[q], yi - sy[q], zi - sz[q], P, e2 >> 15);
         }
-        if (k0 + 3 < nn) {
+        {
           const int q = e3 & 0x7fff;
           pair_f64(b, xi - sx[q], yi - sy[q], zi - sz[q], P, e3 >> 15);
         }

@@ -23,9 +23,10 @@
 
 #include "activechi4.h"
 
-/* the engine that holds the system (created on first use from the globals);
- * nve = 1 selects the constant-energy engine used by advance_time_NVEFrog */
-acg_engine *acg_legacy_engine(int nve);
+/* the engine that holds the system (created on first use from the globals)
+ * for one integrator: kind 0 = Nose-Hoover NVT, 1 = NVE (advance_time_NVEFrog),
+ * 2 = Berendsen NVT, 3 = Gaussian isokinetic */
+acg_engine *acg_legacy_engine(int kind);
 /* the engine holding the current state (the NVT engine before any step) */
 acg_engine *acg_legacy_current(void);
 /* host sphere[] / kx,ky,kz / thermostat globals -> device, when the host

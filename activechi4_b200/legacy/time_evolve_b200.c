@@ -26,7 +26,7 @@ static void params_set_skin(acg_params *p, double s) { p->skin = s; }
 #include "global.h"
 #include "subroutine.h"
 
-static acg_engine *eng[2];  /* [0] Nose-Hoover NVT, [1] NVE */
+static acg_engine *eng[4];  /* [0] Nose-Hoover NVT, [1] NVE, [2] Berendsen NVT, [3] Gaussian isokinetic */
 static acg_engine *owner;   /* the engine whose device state is current */
 static int host_stale;      /* the device has stepped since sphere[] was last refreshed */
 static int host_touched = 1;/* host code may have edited sphere[] since the last push */
@@ -52,7 +52,7 @@ static void *xalloc(size_t n) {
   return p;
 }
 
-acg_engine *acg_legacy_engine(int nve) {
+acg_engine *acg_legacy_engine(int kind) {
   if (Nprocs > 1) {
     fprintf(stderr, "activechi4: run one MPI rank per system (the whole system lives on one GPU)\n");
     exit(1);
@@ -72,7 +72,8 @@ acg_engine *acg_legacy_engine(int nve) {
     sh_k = xalloc(sizeof(int) * 3 * (Nact + 1));
     b_k = xalloc(sizeof(int) * 3 * (Nact + 1));
   }
-  if (!eng[nve]) {
+  if (!eng[kind]) {
+    static const int thermostat_of[4] = {1, 0, 2, 3};
     acg_params p;
     acg_params_default(&p, N);
     p.nact = Nact;
@@ -85,16 +86,16 @@ acg_engine *acg_legacy_engine(int nve) {
     params_set_skin(&p, skin);
     p.rebuild_factor = 3.0; /* MDcode/time_evolve.c:508 */
     p.list_mode = 0;
-    p.thermostat = nve ? 0 : 1;
+    p.thermostat = thermostat_of[kind];
     p.shuffle = 0; /* ShuffleActDirec stays the program's own (host RNG) */
     p.drift_every = 0; /* fixDrift stays the program's own call (MDcode/main.c:261) */
     const char *prec = getenv("ACG_PRECISION");
     if (prec && strcmp(prec, "fp32") == 0) p.precision = ACG_PREC_FP32;
     const char *dev = getenv("ACG_DEVICE");
-    int rc = acg_create(&p, 1, dev ? atoi(dev) : 0, &eng[nve]);
+    int rc = acg_create(&p, 1, dev ? atoi(dev) : 0, &eng[kind]);
     if (rc) acg_legacy_die("acg_create", rc);
   }
-  return eng[nve];
+  return eng[kind];
 }
 
 acg_engine *acg_legacy_current(void) { return owner ? owner : acg_legacy_engine(0); }
@@ -221,7 +222,9 @@ static void pull_scalars(acg_engine *e) {
   maxD = th.maxD;
   maxmaxD = th.maxD;
   ke = th.ke;
-  inst_T = th.inst_T;
+  /* the Gaussian isokinetic step leaves inst_T = 2 sum p^2 / DOF
+   * (MDcode/time_evolve.c:464-465) */
+  inst_T = e == eng[3] ? 4.0 * th.ke / DOF : th.inst_T;
   if (e == eng[0]) {
     for (int k = 0; k < M; k++) {
       eta[k] = th.eta[k];
@@ -308,22 +311,36 @@ void InitialiseNoseHoover() {
   }
 }
 
-/* AdvanceTimeNVTNoseHoover (MDcode/time_evolve.c:495-526): one NHC step of
- * the whole system on the device */
-void AdvanceTimeNVTNoseHoover() {
-  acg_engine *e = acg_legacy_engine(0);
+/* one step of the whole system on the device with engine `kind`; sphere[]
+ * follows at the next sync point */
+static void legacy_step(int kind) {
+  acg_engine *e = acg_legacy_engine(kind);
   acg_legacy_push(e);
   int rc = acg_step(e, 1);
   if (rc) acg_legacy_die("acg_step", rc);
   owner = e;
-  Heff = 0;
 #ifdef ACG_LEGACY_EAGER
   acg_legacy_pull(e);
 #else
-  pull_scalars(e); /* sphere[] follows at the next sync point */
+  pull_scalars(e);
   host_stale = 1;
 #endif
 }
+
+/* AdvanceTimeNVTNoseHoover (MDcode/time_evolve.c:495-526): one NHC step of
+ * the whole system on the device */
+void AdvanceTimeNVTNoseHoover() {
+  legacy_step(0);
+  Heff = 0;
+}
+
+/* advance_time_NVT_Berendsen (MDcode/time_evolve.c:173-256): one NVE step,
+ * then the momenta scaled by sqrt(1 + (T/inst_T - 1) dt/tau_T), on the device */
+void advance_time_NVT_Berendsen() { legacy_step(2); }
+
+/* AdvanceTimeNVTGaussOSM (MDcode/time_evolve.c:351-470): one Gaussian
+ * isokinetic step on the device */
+void AdvanceTimeNVTGaussOSM() { legacy_step(3); }
 
 /* advance_time_NVEFrog (MDcode/time_evolve.c:104-171): one velocity-Verlet
  * step without thermostat (used by the set-up ramps of initialise.c) */

@@ -109,7 +109,7 @@ class Server:
     event marks the end of each), so the GPU has work from every run while the
     host admits new requests or builds their graphs."""
 
-    def __init__(self, device=0, hbm_budget=None, max_active=16, chunk_work=2.0e7, depth=2, size_priority=True):
+    def __init__(self, device=0, hbm_budget=None, max_active=16, chunk_work=2.0e7, depth=2, priority="time"):
         self.device = device
         if hbm_budget is None:
             import torch
@@ -119,7 +119,21 @@ class Server:
         self.max_active = max_active
         self.chunk_work = chunk_work
         self.depth = max(1, int(depth))
-        self.size_priority = size_priority
+        # stream priority of a run: "time" = the runs expected to take longest
+        # first (a small system with many steps is bound by per-step latency
+        # and sets the end of the stream; queued behind the kernels of other
+        # runs it ends later still), "size" = larger systems first, "none"
+        self.priority = priority
+
+    def _level(self, req) -> int:
+        if self.priority == "size":
+            return int(np.clip(2.0 * (math.log10(req.n) - 3.0), 0, 4))
+        if self.priority == "time":
+            # expected device time alone: a step costs at least ~45 us (kernel
+            # latency) and about 1 ns per particle beyond that
+            est = req.steps * max(45e-6, 1.0e-9 * req.n)
+            return int(np.clip(np.floor(np.log2(max(est, 1.0))), 0, 4))
+        return 0
 
     def _chunk(self, n, left):
         # about chunk_work particle-steps, and no more than ~20 ms of device
@@ -158,10 +172,8 @@ class Server:
                     break
                 req = queue.pop(0)
                 e = start_run(req, self.device, setup_priority=5)
-                # stepping priority: by size if asked (larger systems first:
-                # their kernels fill the GPU, latency-bound small runs use
-                # the gaps), else the default
-                e.set_priority(int(np.clip(2.0 * (math.log10(req.n) - 3.0), 0, 4)) if self.size_priority else 0)
+                # stepping priority by the policy (`priority`)
+                e.set_priority(self._level(req))
                 used += fp
                 run = {"engine": e, "req": req, "left": req.steps, "adm": clock() - t0, "fp": fp,
                        "stream": torch.cuda.ExternalStream(e.stream, device=torch.device("cuda", self.device)),

@@ -60,7 +60,11 @@ typedef struct acg_params {
                              0: NVE velocity Verlet (advance_time_NVEFrog);
                              2: Berendsen NVT, the momenta scaled by
                                 sqrt(1 + (T/inst_T - 1) dt/tau_T) after each step
-                                (advance_time_NVT_Berendsen, MDcode/time_evolve.c:173-256) */
+                                (advance_time_NVT_Berendsen, MDcode/time_evolve.c:173-256);
+                             3: Gaussian isokinetic, each half kick p = f1 (p + f2 F)
+                                with f1, f2 from sum p.F, sum F^2, sum p^2
+                                (AdvanceTimeNVTGaussOSM, MDcode/time_evolve.c:351-470);
+                                T is not used and acg_start_ramp is refused */
   int shuffle;            /* re-randomise the active directions every tau_p_steps steps
                              (ShuffleActDirec cadence, MDcode/main.c:245-247):
                              1: on the device in the reference's order (per component,

@@ -260,6 +260,8 @@ class Reference(_Common):
             lib.ref_run.argtypes = [C.c_long, C.c_int, C.c_int, C.c_int]
             lib.ref_run_berendsen.restype = C.c_int
             lib.ref_run_berendsen.argtypes = [C.c_int]
+            lib.ref_run_gauss.restype = C.c_int
+            lib.ref_run_gauss.argtypes = [C.c_int]
             lib.ref_adjust_temp.restype = C.c_double
             lib.ref_adjust_temp.argtypes = [C.c_double]
             lib.ref_coldstart.argtypes = [C.c_double, C.c_double]
@@ -309,6 +311,11 @@ class Reference(_Common):
 
     def fix_drift(self):
         self.lib.ref_fix_drift()
+
+    def run_gauss(self, nsteps):
+        """AdvanceTimeNVTGaussOSM nsteps times (the reference's own build)."""
+        if self.lib.ref_run_gauss(int(nsteps)):
+            raise RuntimeError("this build has no AdvanceTimeNVTGaussOSM")
 
     def run_berendsen(self, nsteps):
         """advance_time_NVT_Berendsen nsteps times (the reference's own build)."""

@@ -199,6 +199,15 @@ int ref_run_berendsen(int nsteps) {
   return 0;
 }
 
+/* AdvanceTimeNVTGaussOSM (MDcode/time_evolve.c:351-470), nsteps times; weak
+ * like the Berendsen step */
+void AdvanceTimeNVTGaussOSM(void) __attribute__((weak));
+int ref_run_gauss(int nsteps) {
+  if (!AdvanceTimeNVTGaussOSM) return -1;
+  for (int i = 0; i < nsteps; i++) AdvanceTimeNVTGaussOSM();
+  return 0;
+}
+
 /* one NVT step composed from the propagators, as AdvanceTimeNVTNoseHoover's
  * body does (MDcode/time_evolve.c:495-526) */
 void ref_step_propagators(void) {

@@ -78,3 +78,25 @@ def test_dropin_sync_points(cuda_lib, g1000):
     assert np.abs(xud - xur).max() < 1e-9
     assert np.abs(pd - pr).max() / np.sqrt((pr ** 2).sum(axis=1).mean()) < 1e-9
 
+
+
+def test_dropin_berendsen_and_gaussian_steps(cuda_lib, g1000):
+    """advance_time_NVT_Berendsen and AdvanceTimeNVTGaussOSM of the drop-in
+    (each on its own device engine, the state handed over through sphere[])
+    against the reference program's own, 30 steps each in a row."""
+    from oracle import Reference, reference_available
+    if not (reference_available(1000) and reference_available(1000, "dropin")):
+        pytest.skip("reference / drop-in programs not built")
+    st = golden_state(g1000)
+    ref, dro = Reference(1000), Reference(1000, "dropin")
+    for r in (ref, dro):
+        r.setup(st, 0.45, 1.0, g1000["eta0"], g1000["p_eta0"])
+        r.run_berendsen(30)
+        r.run_gauss(30)
+    xr, xur, pr, _ = ref.get_state()
+    xd, xud, pd, _ = dro.get_state()
+    assert np.abs(xud - xur).max() < 1e-9
+    assert np.abs(pd - pr).max() / np.sqrt((pr ** 2).sum(axis=1).mean()) < 1e-9
+    sr, sd = ref.scalars(), dro.scalars()
+    assert rel(sd["ke"], sr["ke"]) < 1e-9 and rel(sd["pe"], sr["pe"]) < 1e-9
+    assert rel(sd["inst_T"], sr["inst_T"]) < 1e-9

@@ -195,3 +195,48 @@ def test_berendsen_nvt_matches_reference(cuda_lib, g1000):
     assert np.abs(p - pr).max() / np.sqrt((pr ** 2).sum(axis=1).mean()) < 1e-9
     th, sr = e.thermo(), ref.scalars()
     assert abs(th["ke"] - sr["ke"]) < 1e-9 * sr["ke"] and abs(th["pe"] - sr["pe"]) < 1e-9 * abs(sr["pe"])
+
+
+def test_gaussian_isokinetic_matches_reference(cuda_lib, g1000):
+    """thermostat = 3: the reference's AdvanceTimeNVTGaussOSM (each half kick
+    p = f1 (p + f2 F), the factors from sum p.F, sum F^2 and sum p^2) for 50
+    steps, against the reference program itself; the kinetic energy stays at
+    its starting value."""
+    from oracle import Reference, reference_available
+    if not reference_available(1000):
+        pytest.skip("reference library not built")
+    st = golden_state(g1000)
+    ref = Reference(1000)
+    ref.setup(st, 0.45, 1.0)
+    ref.run_gauss(50)
+    e = engine_for(st, shuffle=0, drift_every=0, thermostat=3)
+    ke0 = e.thermo()["ke"]
+    e.step(20)
+    e.step(30)
+    x, xu, p, F = e.get_state()
+    xr, xur, pr, Fr = ref.get_state()
+    assert np.abs(xu - xur).max() < 1e-9
+    assert np.abs(p - pr).max() / np.sqrt((pr ** 2).sum(axis=1).mean()) < 1e-9
+    th, sr = e.thermo(), ref.scalars()
+    assert abs(th["ke"] - sr["ke"]) < 1e-9 * sr["ke"] and abs(th["pe"] - sr["pe"]) < 1e-9 * abs(sr["pe"])
+    assert abs(th["ke"] - ke0) < 1e-9 * ke0
+    assert abs(0.5 * (p ** 2).sum() - ke0) < 1e-9 * ke0
+
+
+def test_gaussian_isokinetic_drift_and_graph_match_eager(cuda_lib, g1000):
+    """The Gaussian isokinetic step in the CUDA graph (with a drift removal
+    every 7 steps, which re-derives the next first half from the corrected
+    momenta) equals the same steps launched kernel by kernel, bit for bit; a
+    ramp is refused on such a system."""
+    from activechi4_b200._abi import AcgError
+    st = golden_state(g1000)
+    a = engine_for(st, shuffle=0, drift_every=7, thermostat=3)
+    b = engine_for(st, shuffle=0, drift_every=7, thermostat=3)
+    a.step(40)
+    b.step_eager(40)
+    for u, w in zip(a.get_state(), b.get_state()):
+        assert np.array_equal(u, w)
+    p = a.get_state()[2]
+    assert np.abs(p.sum(axis=0)).max() < 1e-9 * np.abs(p).sum()
+    with pytest.raises(AcgError):
+        a.start_ramp(0, 0.2, 0.45, 0.1)
