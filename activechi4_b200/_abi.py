@@ -27,7 +27,7 @@ class acg_params(C.Structure):
         ("T", C.c_double), ("f0", C.c_double), ("tau_p_steps", C.c_int), ("dt", C.c_double),
         ("skin", C.c_double), ("rebuild_factor", C.c_double), ("list_mode", C.c_int),
         ("thermostat", C.c_int), ("shuffle", C.c_int), ("precision", C.c_int),
-        ("nb_capacity", C.c_int), ("seed", C.c_uint64), ("drift_every", C.c_int),
+        ("nb_capacity", C.c_int), ("seed", C.c_uint64), ("drift_every", C.c_int), ("P", C.c_double),
     ]
 
 
@@ -37,6 +37,8 @@ class acg_thermo(C.Structure):
         ("inst_T", C.c_double), ("maxD", C.c_double), ("heff", C.c_double),
         ("eta", C.c_double * 3), ("p_eta", C.c_double * 3), ("q", C.c_double * 3),
         ("step", C.c_int64), ("rebuilds", C.c_int64), ("overflow", C.c_int), ("status", C.c_int),
+        ("L", C.c_double), ("pressure", C.c_double), ("eps", C.c_double), ("p_eps", C.c_double),
+        ("eta_baro", C.c_double * 3), ("p_eta_baro", C.c_double * 3),
     ]
 
 
@@ -74,6 +76,7 @@ _SIGS = {
     "acg_extend_ramp": (C.c_int, [C.c_void_p, C.c_int, C.c_int64]),
     "acg_set_lattice": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "acg_set_nhc": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "acg_set_barostat": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_double]),
     "acg_set_temperature": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
     "acg_rebuild": (C.c_int, [C.c_void_p]),
     "acg_compute_forces": (C.c_int, [C.c_void_p]),

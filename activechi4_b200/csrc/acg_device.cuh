@@ -35,6 +35,8 @@ constexpr int MAX_UNION = 64;     // 4 x 4 x 4 union cells of a 2 x 2 x 2 group
 constexpr int BLOCK_X = 256;      // threads of the whole-box kernels
 constexpr int BOX_CELLS = 8;      // most cells per whole-box block
 constexpr int LIST_SPLIT = 4;     // blocks sharing a whole-box tile in the list build
+constexpr int GSPLIT_MAX = 8;     // most force blocks per cell group (small boxes)
+constexpr int GSPLIT_BLOCKS = 296;  // cell-group force blocks aimed at per system (2 per SM)
 constexpr int BLOCK_SORT = 1024;   // threads of the per-system sub-cell sort
 constexpr int BLOCK_COMPACT = 1024; // threads of the rebuild-list compaction (one block)
 constexpr int MAX_BOX_NC = 4;     // whole-box mode for 2..4 cells per side
@@ -69,6 +71,7 @@ __device__ __forceinline__ void group_geom(int g, int nc, int ng, GroupGeom &G) 
 constexpr double KA_C0 = 0.0162665594880;
 constexpr double KA_C2 = -0.001949973872640;
 constexpr double KA_RC2 = 6.25;  // (r/sigma)^2 cut
+constexpr double TAU_P = 2.0;    // barostat time (tau_P, MDcode/global.h:42)
 
 struct SysDesc {
   int n, nact, poff, aoff;
@@ -77,12 +80,21 @@ struct SysDesc {
   int shuffle, list_mode, precision, goff;  // goff: offset of the system's groups
   int tile0_a, ntile_a, box, xoff;            // kick/drift tiles; box: whole-box kernels (2..4 cells per side), xoff: first box tile
   int cpb, msub, bz, soff;                    // cpb: cells per whole-box block; msub: list sub-cells per side, bz: their list bricks' depth, soff: first sub-cell start
-  int drift_every, pad0, pad1, pad2;          // drift_every: remove the mean momentum after every such step (0: never)
+  int drift_every, gsplit, gtile0, pad2;      // drift_every: remove the mean momentum after every such step (0: never);
+                                              // gsplit: force blocks per cell group, gtile0: first group force tile
   double L, invL, inv_cell;  // inv_cell: cells per unit reduced length (InvCellSize)
   double T, f0, dt, half_dt, skin2, rebuild_factor, dof;
   double q[NHC_M];
   double lcut2[3];           // list cut^2 (absolute units) for type sums 0 (AA), 1 (AB), 2 (BB)
   unsigned long long seed;
+  // constant pressure (thermostat 4): L, invL and density above change on the
+  // device before every step (k_npt_box); invL is the inverse of the length
+  // before the last change, as the reference's drift uses it
+  double density, P, cell_cut;
+  // Nose-Hoover NPT (thermostat 5): L = L0 exp(eps); barostat mass w_eps =
+  // DOF T tau_baro^2 and chain masses q_baro = T tau_baro^2
+  // (InitialiseNoseHooverNPT, MDcode/time_evolve.c:614-652)
+  double L0, w_eps, q_baro[NHC_M];
 };
 
 struct SysState {
@@ -120,6 +132,13 @@ struct SysState {
   double ga[2];
   int gmode;
   unsigned int counter_g;    // last-block counter of the Gaussian kernels
+  double pressure;           // constant pressure: pressure at the last box update
+  // Nose-Hoover NPT (thermostat 5): barostat chain, p_eps and eps at the step
+  // boundary and after the next step's first half; u2 = the half kicks'
+  // p = p f1 + f2 F dt/2 factors of the current step
+  double eta_baro_end[NHC_M], p_eta_baro_end[NHC_M], eta_baro_cur[NHC_M], p_eta_baro_cur[NHC_M];
+  double p_eps_end, p_eps_cur, eps_end, eps_cur;
+  double u2[2];
 };
 
 // In-place observables of one system (set by acg_obs_configure): events of the
@@ -239,6 +258,60 @@ __device__ inline double nhc_half(double *eta, double *p_eta, const double *q, d
   double s2k = (s * s) * ksum;
   nhc_u4(p_eta, q, T, dof, t4, 0, NHC_M - 1, s2k);
   return s;
+}
+
+// Nose-Hoover NPT chains (MDcode/time_evolve.c:700-822).  U4PropagatorNPT:
+// the particle chain as nhc_u4, then the barostat chain the same way with
+// G_0 = p_eps^2 / w_eps - T.
+__device__ inline void baro_u4(double *p_eta_b, const double *q_b, double T, double t, int j0, int j1,
+                               double p_eps, double w_eps) {
+  int dj = j0 > j1 ? -1 : 1;
+  int j = j0;
+  double gj;
+  do {
+    if (j == 0)
+      gj = p_eps * p_eps / w_eps - T;
+    else
+      gj = (p_eta_b[j - 1] * p_eta_b[j - 1]) / q_b[j - 1] - T;
+    if (j == NHC_M - 1) {
+      p_eta_b[j] = p_eta_b[j] + t * gj;
+    } else {
+      double x = t * p_eta_b[j + 1] / q_b[j + 1];
+      double e = exp(-x);
+      p_eta_b[j] = p_eta_b[j] * e + t * gj * (1.0 - e) / x;
+    }
+    j += dj;
+  } while (j - dj != j1);
+}
+
+// U4 U3 U4 of the NPT split (:660-662, :690-692) on the particle chain
+// (eta, p_eta), the barostat chain (eta_b, p_eta_b) and p_eps, with sum p^2 =
+// ksum before U3; returns the particles' U3 velocity scale.
+__device__ inline double npt_half(double *eta, double *p_eta, double *eta_b, double *p_eta_b, double &p_eps,
+                                  const double *q, const double *q_b, double w_eps, double T, double dof,
+                                  double dt, double ksum) {
+  const double t4 = dt * 0.25, t3 = dt * 0.50;
+  nhc_u4(p_eta, q, T, dof, t4, NHC_M - 1, 0, ksum);
+  baro_u4(p_eta_b, q_b, T, t4, NHC_M - 1, 0, p_eps, w_eps);
+  const double s = exp(-t3 * p_eta[0] / q[0]);
+  for (int i = 0; i < NHC_M; i++) {
+    eta[i] = eta[i] + t3 * p_eta[i] / q[i];
+    eta_b[i] += t3 * p_eta_b[i] / q_b[i];
+  }
+  p_eps = p_eps * exp(-t3 * p_eta_b[0] / q_b[0]);
+  const double s2k = (s * s) * ksum;
+  nhc_u4(p_eta, q, T, dof, t4, 0, NHC_M - 1, s2k);
+  baro_u4(p_eta_b, q_b, T, t4, 0, NHC_M - 1, p_eps, w_eps);
+  return s;
+}
+
+// U2PrimePropagatorNPT (:737-755): p_eps += 3 (PV - P L^3) dt/2 with PV =
+// alpha sum p^2 / 3 + virial, alpha = 1 + 3/DOF
+__device__ inline void npt_u2prime(double &p_eps, double ksum, double virial, double P, double L, double dof,
+                                   double half_dt) {
+  const double alpha = 1.0 + 3.0 / dof;
+  const double PV = alpha * (ksum) / (3.00) + virial;
+  p_eps += 3.00 * (PV - P * L * L * L) * half_dt;
 }
 
 // MT19937 (Matsumoto & Nishimura 1998): seeding by their 2002 initialisation

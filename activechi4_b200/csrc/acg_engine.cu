@@ -38,7 +38,7 @@ constexpr int GRAPH_STEPS = 32;
 constexpr int BENCH_MAX_GRAPH = 256;  // acg_bench_steps: one graph for up to this many steps
 
 struct Layout {
-  int nsys = 0, nslots = 0, ncells = 0, nact = 0, maxnb = 0, ngroups = 0, nboxtiles = 0, box_nmax = 0;
+  int nsys = 0, nslots = 0, ncells = 0, nact = 0, maxnb = 0, ngroups = 0, ngtiles = 0, nboxtiles = 0, box_nmax = 0;
   int nact_max = 0;  // most active particles of one system
   int nboxcap = 0;   // whole-box tiles at one cell per block (the most any partition needs)
   int box_m3max = 0;  // most list sub-cells of a whole-box system (0: none uses them)
@@ -69,6 +69,11 @@ int resolve(const acg_params &p, SysDesc &d) {
   d.L = L;
   d.invL = 1.0 / L;
   d.inv_cell = L / cs;  // InvCellSize (MDcode/Parallel.c:78)
+  d.cell_cut = cell_cut;
+  // DENSITY: read from the parameter file where L follows from it, else N / L^3
+  d.density = p.L > 0 ? (double)p.n / (L * L * L) : p.density;
+  d.P = p.P;
+  d.L0 = L;
   d.T = p.T;
   d.f0 = p.f0;
   d.dt = p.dt;
@@ -78,6 +83,8 @@ int resolve(const acg_params &p, SysDesc &d) {
   d.dof = 3.0 * (double)p.n - 3.0;  // DOF (MDcode/global.h:35)
   for (int i = 0; i < NHC_M; i++) d.q[i] = p.T * TAU_T * TAU_T;
   d.q[0] = d.dof * p.T * TAU_T * TAU_T;
+  for (int i = 0; i < NHC_M; i++) d.q_baro[i] = p.T * TAU_P * TAU_P;
+  d.w_eps = d.dof * p.T * TAU_P * TAU_P;
   for (int t = 0; t < 3; t++) {
     double rl = p.list_mode == 0 ? cell_cut : 2.5 * sigma_of(t) + p.skin;
     d.lcut2[t] = rl * rl;
@@ -91,7 +98,7 @@ int resolve(const acg_params &p, SysDesc &d) {
   d.seed = p.seed;
   if (p.dt <= 0 || p.skin <= 0 || p.rebuild_factor <= 0)
     return fail(ACG_ERR_INVALID, "dt, skin and rebuild_factor must be positive");
-  if (p.thermostat < 0 || p.thermostat > 3) return fail(ACG_ERR_INVALID, "thermostat must be 0, 1, 2 or 3");
+  if (p.thermostat < 0 || p.thermostat > 5) return fail(ACG_ERR_INVALID, "thermostat must be 0 to 5");
   if (p.thermostat && !(p.T > 0)) return fail(ACG_ERR_INVALID, "thermostat needs T > 0");
   if (p.shuffle < 0 || p.shuffle > 2) return fail(ACG_ERR_INVALID, "shuffle must be 0, 1 or 2");
   if (p.shuffle && p.tau_p_steps <= 0) return fail(ACG_ERR_INVALID, "shuffle needs tau_p_steps > 0");
@@ -120,6 +127,13 @@ int plan(const acg_params *params, int nsys, Layout &lay, int nsm) {
     d.ng = d.nc >= 3 && !d.box ? (d.nc + 1) / 2 : 0;
     d.goff = lay.ngroups;
     lay.ngroups += d.ng * d.ng * d.ng;
+    // force blocks per cell group: a small box has few groups, each split over
+    // up to GSPLIT_MAX blocks (contiguous runs of its centre particles) so that
+    // about GSPLIT_BLOCKS blocks share the pair work; depends on the system
+    // alone, so its results do not depend on the engine it is in
+    d.gsplit = d.ng > 0 ? std::max(1, std::min(GSPLIT_MAX, GSPLIT_BLOCKS / (d.ng * d.ng * d.ng))) : 1;
+    d.gtile0 = lay.ngtiles;
+    lay.ngtiles += d.ng * d.ng * d.ng * d.gsplit;
     if (d.box) lay.box_nmax = std::max(lay.box_nmax, d.n);
     // list sub-cells of a whole box: side >= 1.45 and >= half the widest list
     // cut, so a partner is at most two sub-cells away on each axis; at least 5
@@ -191,11 +205,11 @@ int plan(const acg_params *params, int nsys, Layout &lay, int nsm) {
   add(8 * (S / 4 + nsys + 1));            // tiles_b (>= 4 particles per block)
   add(8 * (S / PART_L + nsys + 1));       // tiles_l
   add(8 * (Cn / CELLS_PER_TILE + nsys + 1));
-  const size_t Gn = (size_t)lay.ngroups;
-  add(8 * (Gn + 1));                      // tiles_g
+  const size_t Gn = (size_t)lay.ngroups, Gt = (size_t)lay.ngtiles;
+  add(8 * (Gt + 1));                      // tiles_g
   add(4 * (Gn + 1));                      // gstart
   add(8 * ((size_t)lay.nboxcap + 1));     // tiles_x
-  add(32 * (Gn + lay.nboxcap + S / 4 + nsys + 1));  // part_b
+  add(32 * (Gt + lay.nboxcap + S / 4 + nsys + 1));  // part_b
   add(32 * S);                            // pacc
   add(64);                                // counters
   add(sizeof(ObsDesc) * nsys);            // observables
@@ -232,6 +246,9 @@ struct acg_engine {
   std::vector<int> dirty;  // systems whose forces/lists must be recomputed
   bool any_dirty = false;
   bool any_gauss = false;  // a system runs the Gaussian isokinetic integrator (thermostat 3)
+  bool any_npt = false;    // a system runs the Berendsen barostat (thermostat 4)
+  bool any_box = false;    // a system's box length changes on the device (thermostats 4 and 5)
+  bool desc_live = false;  // the descriptors on the device are the current ones
   cudaGraphExec_t gexec = nullptr;
   cudaGraph_t graph = nullptr;
   int gsteps = 0;
@@ -324,21 +341,40 @@ int build_tiles_x(acg_engine *e) {
   return ACG_OK;
 }
 
+// constant-pressure systems change L, invL and density on the device (k_npt_box);
+// the host copy of the descriptors takes them back before it is uploaded again
+int sync_box(acg_engine *e) {
+  if (!e->any_box || !e->desc_live) return ACG_OK;
+  for (int r = 0; r < e->lay.nsys; r++) {
+    SysDesc &d = e->lay.desc[r];
+    if (d.thermostat != 4 && d.thermostat != 5) continue;
+    SysDesc dd;
+    CK(cudaMemcpyAsync(&dd, e->d_desc + r, sizeof(SysDesc), cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    d.L = dd.L;
+    d.invL = dd.invL;
+    d.density = dd.density;
+  }
+  return ACG_OK;
+}
+
 // force tiles: one block per cell group for systems with >= 3 cells per
 // side (partials [0, ntiles_g)), block/tpp particles per block for the others
 // (partials [ntiles_g, ntiles_g + ntiles_b))
 int build_tiles_b(acg_engine *e) {
+  int rc0 = sync_box(e);
+  if (rc0) return rc0;
   const int pb = e->block / e->tpp;
   std::vector<int2> tb;
   int ng_total = 0;
   for (int r = 0; r < e->lay.nsys; r++) {
     SysDesc &d = e->lay.desc[r];
     if (d.ng > 0) {
-      d.tile0_b = d.goff;
-      d.ntile_b = d.ng * d.ng * d.ng;
+      d.tile0_b = d.gtile0;
+      d.ntile_b = d.ng * d.ng * d.ng * d.gsplit;
     }
   }
-  ng_total = e->lay.ngroups;
+  ng_total = e->lay.ngtiles;
   for (int r = 0; r < e->lay.nsys; r++) {
     SysDesc &d = e->lay.desc[r];
     if (d.box) {
@@ -363,6 +399,7 @@ int build_tiles_b(acg_engine *e) {
   CK(cudaMemcpyAsync(e->d_desc, e->lay.desc.data(), sizeof(SysDesc) * e->lay.nsys,
                      cudaMemcpyHostToDevice, e->stream));
   e->v.ntiles_b = e->ntiles_b;
+  e->desc_live = true;
   return ACG_OK;
 }
 
@@ -480,8 +517,18 @@ void launch_gauss(acg_engine *e, bool with_sum) {
   k_gauss_apply<<<e->ntiles_a, BLOCK_A, 0, e->stream>>>(e->v);
 }
 
+// constant pressure: the box update, then the forces at the new length
+int launch_npt(acg_engine *e) {
+  if (!e->any_npt) return ACG_OK;
+  k_npt_box<<<1, 32, 0, e->stream>>>(e->v);
+  CK(cudaGetLastError());
+  return launch_force(e, 3);
+}
+
 int launch_step_eager(acg_engine *e) {
-  k_kick_drift<<<e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, 0, e->stream>>>(e->v, 0, 0, 0, 0);
+  int rc0 = launch_npt(e);
+  if (rc0) return rc0;
+  k_kick_drift<<<e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, 0, e->stream>>>(e->v, 0, 0, 0);
   k_shuffle_ref<<<3 * e->lay.nsys, BLOCK_SHUF, shuffle_smem(e->lay), e->stream>>>(e->v, -1);
   CK(cudaGetLastError());
   int rc = launch_rebuild(e);
@@ -542,25 +589,50 @@ int add_steps(acg_engine *e, cudaGraph_t g, int K, cudaGraphNode_t *prev_io) {
   GroupFn xf = box_fn(e->btpp, prec);
   int mode0 = 0, use_cond = 1, tbase = e->ntiles_g + e->ntiles_x;
   for (int s = 0; s < K; s++) {
-    // per step: kick/drift, then two device-decided branches side by side (the
-    // list rebuild; the reference-order direction shuffle), the force kernels,
-    // and one device-decided branch after them (drift removal, observables)
-    cudaGraphConditionalHandle h, ho, hs;
-    CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+    // per step: kick/drift, then one device-decided switch (the list rebuild,
+    // the reference-order direction shuffle, both side by side, or nothing),
+    // the force kernels, and one device-decided branch after them (drift
+    // removal, observables)
+    cudaGraphConditionalHandle h, ho;
+    CK(cudaGraphConditionalHandleCreate(&h, g, 3, cudaGraphCondAssignDefault));
     CK(cudaGraphConditionalHandleCreate(&ho, g, 0, cudaGraphCondAssignDefault));
-    CK(cudaGraphConditionalHandleCreate(&hs, g, 0, cudaGraphCondAssignDefault));
-    cudaGraphNode_t na, nc, ns, nb;
-    void *aa[] = {&v, &use_cond, &h, &ho, &hs};
-    int rc = add_kernel(g, prev ? &prev : nullptr, prev ? 1 : 0, &na, (void *)k_kick_drift,
-                        e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, aa);
+    cudaGraphNode_t na, nc, nb;
+    int rc;
+    if (e->any_npt) {  // constant pressure: box update, forces at the new length
+      void *va0[] = {&v};
+      rc = add_kernel(g, prev ? &prev : nullptr, prev ? 1 : 0, &nb, (void *)k_npt_box, 1, 32, va0);
+      if (rc) return rc;
+      prev = nb;
+      int mode3 = 3;
+      if (e->ntiles_g) {
+        void *ga[] = {&v, &mode3};
+        rc = add_kernel(g, &prev, 1, &nb, (void *)gf, e->ntiles_g, BLOCK_G, ga, group_smem(v.gcap));
+        if (rc) return rc;
+        prev = nb;
+      }
+      if (e->ntiles_x) {
+        void *xa[] = {&v, &mode3};
+        rc = add_kernel(g, &prev, 1, &nb, (void *)xf, e->ntiles_x, BLOCK_X, xa, box_smem(e->lay.box_nmax, prec));
+        if (rc) return rc;
+        prev = nb;
+      }
+      if (e->ntiles_b) {
+        void *ba[] = {&v, &mode3, &tbase};
+        rc = add_kernel(g, &prev, 1, &nb, (void *)ff, e->ntiles_b, e->block, ba);
+        if (rc) return rc;
+        prev = nb;
+      }
+    }
+    void *aa[] = {&v, &use_cond, &h, &ho};
+    rc = add_kernel(g, prev ? &prev : nullptr, prev ? 1 : 0, &na, (void *)k_kick_drift,
+                    e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, aa);
     if (rc) return rc;
     cudaGraphNodeParams cp = {};
     cp.type = cudaGraphNodeTypeConditional;
     cp.conditional.handle = h;
-    cp.conditional.type = cudaGraphCondTypeIf;
-    cp.conditional.size = 1;
+    cp.conditional.type = cudaGraphCondTypeSwitch;
+    cp.conditional.size = 3;
     CK(cudaGraphAddNode(&nc, g, &na, 1, &cp));
-    cudaGraph_t body = cp.conditional.phGraph_out[0];
     void *va[] = {&v};
     struct {
       void *fn;
@@ -577,31 +649,29 @@ int add_steps(acg_engine *e, cudaGraph_t g, int K, cudaGraphNode_t *prev_io) {
               {(void *)k_build_list_groups, e->ntiles_g, BLOCK_G, list_smem(v.gcap)},
               {(void *)k_build_list_box, e->ntiles_x * LIST_SPLIT, BLOCK_X, box_list_smem(e->lay.box_cell_nmax)},
               {(void *)k_build_list, e->ntiles_l, BLOCK_L, 0}};
-    cudaGraphNode_t bp = nullptr;
-    for (auto &k : rb) {
-      if (k.grid == 0) continue;
-      cudaGraphNode_t nn;
-      rc = add_kernel(body, bp ? &bp : nullptr, bp ? 1 : 0, &nn, k.fn, k.grid, k.block, va, k.smem);
-      if (rc) return rc;
-      bp = nn;
+    int all = -1;
+    void *sa[] = {&v, &all};
+    for (int c = 0; c < 3; c++) {
+      cudaGraph_t body = cp.conditional.phGraph_out[c];
+      if (c != 1) {  // the rebuild chain
+        cudaGraphNode_t bp = nullptr;
+        for (auto &k : rb) {
+          if (k.grid == 0) continue;
+          cudaGraphNode_t nn;
+          rc = add_kernel(body, bp ? &bp : nullptr, bp ? 1 : 0, &nn, k.fn, k.grid, k.block, va, k.smem);
+          if (rc) return rc;
+          bp = nn;
+        }
+      }
+      if (c != 0) {  // the shuffle, independent of the rebuild chain
+        cudaGraphNode_t nk;
+        rc = add_kernel(body, nullptr, 0, &nk, (void *)k_shuffle_ref, 3 * e->lay.nsys, BLOCK_SHUF, sa,
+                        shuffle_smem(e->lay));
+        if (rc) return rc;
+      }
     }
-    cudaGraphNodeParams sp = {};
-    sp.type = cudaGraphNodeTypeConditional;
-    sp.conditional.handle = hs;
-    sp.conditional.type = cudaGraphCondTypeIf;
-    sp.conditional.size = 1;
-    CK(cudaGraphAddNode(&ns, g, &na, 1, &sp));
-    {
-      cudaGraphNode_t nk;
-      int all = -1;
-      void *sa[] = {&v, &all};
-      rc = add_kernel(sp.conditional.phGraph_out[0], nullptr, 0, &nk, (void *)k_shuffle_ref, 3 * e->lay.nsys,
-                      BLOCK_SHUF, sa, shuffle_smem(e->lay));
-      if (rc) return rc;
-    }
-    cudaGraphNode_t pre[2] = {nc, ns};
-    const cudaGraphNode_t *dep = pre;
-    size_t ndep = 2;
+    const cudaGraphNode_t *dep = &nc;
+    size_t ndep = 1;
     cudaGraphNode_t last = nullptr;
     if (e->ntiles_g) {
       void *ga[] = {&v, &mode0};
@@ -806,7 +876,11 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
     return rc;
   }
   e->device = device;
-  for (int r = 0; r < nsys; r++) e->any_gauss |= e->lay.desc[r].thermostat == 3;
+  for (int r = 0; r < nsys; r++) {
+    e->any_gauss |= e->lay.desc[r].thermostat == 3;
+    e->any_npt |= e->lay.desc[r].thermostat == 4;
+    e->any_box |= e->lay.desc[r].thermostat == 4 || e->lay.desc[r].thermostat == 5;
+  }
   cudaError_t ce = cudaSetDevice(device);
   if (ce != cudaSuccess) {
     delete e;
@@ -861,12 +935,12 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   e->d_tiles_b = (int2 *)take(8 * (S / 4 + nsys + 1));
   int2 *tl = (int2 *)take(8 * (S / PART_L + nsys + 1));
   int2 *tc = (int2 *)take(8 * (Cn / CELLS_PER_TILE + nsys + 1));
-  const size_t Gn = (size_t)L.ngroups;
-  int2 *tg = (int2 *)take(8 * (Gn + 1));
+  const size_t Gn = (size_t)L.ngroups, Gt = (size_t)L.ngtiles;
+  int2 *tg = (int2 *)take(8 * (Gt + 1));
   v.gstart = (int *)take(4 * (Gn + 1));
   const size_t Xn = (size_t)L.nboxcap;
   int2 *tx = (int2 *)take(8 * (Xn + 1));
-  v.part_b = (double4 *)take(32 * (Gn + Xn + S / 4 + nsys + 1));
+  v.part_b = (double4 *)take(32 * (Gt + Xn + S / 4 + nsys + 1));
   v.pacc = (double4 *)take(32 * S);
   v.counter_a = (unsigned int *)take(64);
   v.obs = (ObsDesc *)take(sizeof(ObsDesc) * nsys);
@@ -895,7 +969,7 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
     d.ntile_a = (int)h_a.size() - d.tile0_a;
     for (int s = 0; s < d.ncell; s += CELLS_PER_TILE) h_c.push_back(make_int2(r, s));
     if (d.ng > 0)
-      for (int g = 0; g < d.ng * d.ng * d.ng; g++) h_g.push_back(make_int2(r, g));
+      for (int g = 0; g < d.ng * d.ng * d.ng * d.gsplit; g++) h_g.push_back(make_int2(r, g));
     else if (d.box)
       continue;  // whole-box tiles: build_tiles_x
     else
@@ -908,7 +982,7 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   auto group_cells = [&](int2 t) {
     const SysDesc &d = e->lay.desc[t.x];
     int c = 1;
-    for (int k = 0, q = t.y; k < 3; k++, q /= d.ng) c *= std::min(2 * (q % d.ng) + 2, d.nc) - 2 * (q % d.ng);
+    for (int k = 0, q = t.y / d.gsplit; k < 3; k++, q /= d.ng) c *= std::min(2 * (q % d.ng) + 2, d.nc) - 2 * (q % d.ng);
     return c;
   };
   std::stable_sort(h_g.begin(), h_g.end(), [&](int2 a, int2 b) { return group_cells(a) > group_cells(b); });
@@ -1223,8 +1297,8 @@ int acg_start_ramp(acg_engine *e, int sys, double T_start, double T_end, double 
   if (!(T_start > 0) || !(T_end > 0) || !(rate > 0) || !std::isfinite(T_start) || !std::isfinite(T_end))
     return fail(ACG_ERR_INVALID, "ramp temperatures and rate must be positive");
   const SysDesc &d = e->lay.desc[sys];
-  if (d.thermostat == 3)
-    return fail(ACG_ERR_INVALID, "temperature ramps run on NVE, Nose-Hoover or Berendsen systems, not Gaussian isokinetic");
+  if (d.thermostat == 3 || d.thermostat == 5)
+    return fail(ACG_ERR_INVALID, "temperature ramps are refused for Gaussian isokinetic and Nose-Hoover NPT systems");
   double T0 = 0;
   rc = acg_adjust_temperature(e, sys, T_start, &T0);
   if (rc) return rc;
@@ -1321,15 +1395,37 @@ int acg_set_nhc(acg_engine *e, int sys, const double *eta3, const double *p_eta3
   return ACG_OK;
 }
 
+int acg_set_barostat(acg_engine *e, int sys, const double *eta_baro3, const double *p_eta_baro3, double p_eps) {
+  int rc = check_sys(e, sys);
+  if (rc) return rc;
+  if (!eta_baro3 || !p_eta_baro3 || !std::isfinite(p_eps)) return fail(ACG_ERR_INVALID, "bad barostat state");
+  if (e->lay.desc[sys].thermostat != 5) return fail(ACG_ERR_INVALID, "the system is not Nose-Hoover NPT (thermostat 5)");
+  CK(cudaSetDevice(e->device));
+  SysState *s = e->v.st + sys;
+  CK(cudaMemcpyAsync(s->eta_baro_end, eta_baro3, 3 * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+  CK(cudaMemcpyAsync(s->p_eta_baro_end, p_eta_baro3, 3 * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+  CK(cudaMemcpyAsync(&s->p_eps_end, &p_eps, sizeof(double), cudaMemcpyHostToDevice, e->stream));
+  if (!e->dirty[sys]) {
+    k_prehalf<<<1, 1, 0, e->stream>>>(e->v, sys);
+    CK(cudaGetLastError());
+  }
+  CK(cudaStreamSynchronize(e->stream));
+  return ACG_OK;
+}
+
 int acg_set_temperature(acg_engine *e, int sys, double T) {
   int rc = check_sys(e, sys);
   if (rc) return rc;
   if (!(T > 0)) return fail(ACG_ERR_INVALID, "T must be positive");
+  CK(cudaSetDevice(e->device));
+  rc = sync_box(e);
+  if (rc) return rc;
   SysDesc &d = e->lay.desc[sys];
   d.T = T;
   for (int i = 0; i < NHC_M; i++) d.q[i] = T * TAU_T * TAU_T;
   d.q[0] = d.dof * T * TAU_T * TAU_T;
-  CK(cudaSetDevice(e->device));
+  for (int i = 0; i < NHC_M; i++) d.q_baro[i] = T * TAU_P * TAU_P;
+  d.w_eps = d.dof * T * TAU_P * TAU_P;
   CK(cudaMemcpyAsync(e->d_desc + sys, &d, sizeof(SysDesc), cudaMemcpyHostToDevice, e->stream));
   if (!e->dirty[sys]) {
     k_prehalf<<<1, 1, 0, e->stream>>>(e->v, sys);
@@ -1493,6 +1589,26 @@ int acg_get_thermo(acg_engine *e, int sys, acg_thermo *out) {
   out->step = s.step;
   out->rebuilds = s.rebuilds;
   out->overflow = s.overflow;
+  out->L = d.L;
+  out->eps = s.eps_end;
+  out->p_eps = s.p_eps_end;
+  for (int i = 0; i < NHC_M; i++) {
+    out->eta_baro[i] = s.eta_baro_end[i];
+    out->p_eta_baro[i] = s.p_eta_baro_end[i];
+  }
+  if (d.thermostat == 5) out->L = d.L0 * std::exp(s.eps_end);
+  if (d.thermostat == 4) {
+    double Ld = 0;
+    CK(cudaMemcpyAsync(&Ld, &e->d_desc[sys].L, sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    out->L = Ld;
+    out->pressure = s.pressure;
+  }
+  if (s.status == 2) {
+    out->status = ACG_ERR_BOX;
+    return fail(ACG_ERR_BOX, "system " + std::to_string(sys) + ": the box left its cell grid (L = " +
+                                 std::to_string(out->L) + ")");
+  }
   out->status = s.status ? ACG_ERR_NONFINITE : 0;
   if (s.status) return fail(ACG_ERR_NONFINITE, "system " + std::to_string(sys) + ": non-finite kinetic energy");
   return ACG_OK;
@@ -1592,7 +1708,7 @@ int acg_time_stage(acg_engine *e, int stage, int reps, double *ms) {
   CK(cudaEventRecord(a, e->stream));
   for (int i = 0; i < reps; i++) {
     if (stage == 0) {
-      k_kick_drift<<<e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, 0, e->stream>>>(e->v, 0, 0, 0, 0);
+      k_kick_drift<<<e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, 0, e->stream>>>(e->v, 0, 0, 0);
     } else if (stage == 1) {
       rc = launch_force(e, 2);
     } else {
@@ -1797,7 +1913,9 @@ int acg_bench_steps(acg_engine *e, int64_t nsteps, size_t flush_bytes, double *m
   // shuffle the shuffle kernel; a step with a drift removal or observable
   // events the three kernels of that branch (the node lists of add_steps);
   // with a Gaussian isokinetic system two more per step and one more per branch
-  const long long per_step = 1 + (e->ntiles_g > 0) + (e->ntiles_x > 0) + (e->ntiles_b > 0) + 2 * e->any_gauss;
+  const long long nforce = (e->ntiles_g > 0) + (e->ntiles_x > 0) + (e->ntiles_b > 0);
+  // (constant pressure: the box update and a second force pass every step)
+  const long long per_step = 1 + nforce + 2 * e->any_gauss + e->any_npt * (1 + nforce);
   const long long per_rebuild = 5 + (e->lay.box_m3max > 0) + 2 * (e->ntiles_x > 0) + (e->ntiles_g > 0) +
                                 (e->ntiles_l > 0);
   long long steps_with_rebuild = 0, shuffles = 0, posts = 0;

@@ -235,11 +235,19 @@ __global__ void k_mt_flip(View v, int r) {
 // U3 U2 (pending thermostat scales and the half kick) and U1 for one
 // particle, in the reference's order of roundings; returns |x_u - x_old|^2
 // (reduced units) for the rebuild test
-__device__ __forceinline__ double kick_drift_one(const View &v, const SysDesc &d, int i, double s1, double s2,
-                                                 double g1, bool gauss) {
+__device__ __forceinline__ double kick_drift_one(const View &v, const SysDesc &d, const SysState &st, int i) {
   const double hdt = d.half_dt, dt = d.dt, il = d.invL;
+  const double s1 = st.s1, s2 = st.s2;
   double px, py, pz;
-  if (gauss) {
+  if (d.thermostat == 5 && st.ramp_left == 0) {
+    // Nose-Hoover NPT: U3 scale, then U2PropagatorNPT p f1 + f2 F dt/2
+    // (MDcode/time_evolve.c:721-735)
+    const double f1 = st.u2[0], f2 = st.u2[1];
+    px = __dadd_rn(__dmul_rn(__dmul_rn(__dmul_rn(v.vx[i], s2), s1), f1), __dmul_rn(__dmul_rn(f2, v.fx[i]), hdt));
+    py = __dadd_rn(__dmul_rn(__dmul_rn(__dmul_rn(v.vy[i], s2), s1), f1), __dmul_rn(__dmul_rn(f2, v.fy[i]), hdt));
+    pz = __dadd_rn(__dmul_rn(__dmul_rn(__dmul_rn(v.vz[i], s2), s1), f1), __dmul_rn(__dmul_rn(f2, v.fz[i]), hdt));
+  } else if (d.thermostat == 3) {
+    const double g1 = st.g1;
     // Gaussian isokinetic half kick p = factor1 (p + factor2 F)
     // (MDcode/time_evolve.c:388-394)
     px = __dmul_rn(s1, __dadd_rn(__dmul_rn(v.vx[i], s2), __dmul_rn(g1, v.fx[i])));
@@ -309,9 +317,11 @@ __device__ __forceinline__ bool shuffle_due(const SysDesc &d, const SysState &st
 }
 
 // stage 1: kick + drift (+ uniform-shuffle blocks) + rebuild decision
-__global__ void __launch_bounds__(BLOCK_A) k_kick_drift(View v, int use_cond, cudaGraphConditionalHandle h,
-                                                        cudaGraphConditionalHandle h_obs,
-                                                        cudaGraphConditionalHandle h_shuf) {
+// The last block sets the step's two graph branches: h_pre (a switch before
+// the forces: 0 = list rebuild, 1 = reference-order shuffle, 2 = both, 3 =
+// neither) and h_obs (after the forces: drift removal and observables).
+__global__ void __launch_bounds__(BLOCK_A) k_kick_drift(View v, int use_cond, cudaGraphConditionalHandle h_pre,
+                                                        cudaGraphConditionalHandle h_obs) {
   __shared__ double sm[BLOCK_A / 32];
   __shared__ int s_last;
   const int b = blockIdx.x;
@@ -323,8 +333,7 @@ __global__ void __launch_bounds__(BLOCK_A) k_kick_drift(View v, int use_cond, cu
     const SysDesc &d = v.desc[r];
     int loc = t.y + threadIdx.x;
     if (loc < d.n) {
-      const SysState &st = v.st[r];
-      mymax = kick_drift_one(v, d, d.poff + loc, st.s1, st.s2, st.g1, d.thermostat == 3);
+      mymax = kick_drift_one(v, d, v.st[r], d.poff + loc);
     }
     // per-system block max (a tile never straddles systems)
     for (int o = 16; o > 0; o >>= 1) mymax = fmax(mymax, __shfl_down_sync(0xffffffffu, mymax, o));
@@ -372,9 +381,8 @@ __global__ void __launch_bounds__(BLOCK_A) k_kick_drift(View v, int use_cond, cu
   if (threadIdx.x == 0) {
     *v.counter_a = 0;
     if (use_cond) {
-      cudaGraphSetConditional(h, any ? 1u : 0u);
+      cudaGraphSetConditional(h_pre, any ? (any_shuf ? 2u : 0u) : (any_shuf ? 1u : 3u));
       cudaGraphSetConditional(h_obs, any_post ? 1u : 0u);
-      cudaGraphSetConditional(h_shuf, any_shuf ? 1u : 0u);
     }
   }
 }
@@ -840,6 +848,45 @@ __device__ void next_first_half(const SysDesc &d, SysState &st, double kb) {
       st.p_eta_cur[k] = pet[k];
     }
     st.s1 = s1;
+  } else if (d.thermostat == 5) {
+    // Nose-Hoover NPT first half (MDcode/time_evolve.c:660-665): U4 U3 U4 on
+    // both chains and p_eps from the boundary state, U2Prime with sum p^2 after
+    // U3 and the last forces' virial at the boundary length L0 exp(eps), the
+    // U2 factors, then U1's box change eps += dt p_eps / w_eps, L = L0 exp(eps)
+    // (:680-683); the drift keeps inv_L of the boundary length
+    // (UpdateBoxForNPT ran at the end of the previous step)
+    SysDesc &dm = const_cast<SysDesc &>(d);
+    double eta[NHC_M], pet[NHC_M], etab[NHC_M], petb[NHC_M];
+    for (int k = 0; k < NHC_M; k++) {
+      eta[k] = st.eta_end[k];
+      pet[k] = st.p_eta_end[k];
+      etab[k] = st.eta_baro_end[k];
+      petb[k] = st.p_eta_baro_end[k];
+    }
+    double p_eps = st.p_eps_end;
+    const double s1 = npt_half(eta, pet, etab, petb, p_eps, d.q, d.q_baro, d.w_eps, d.T, d.dof, d.dt, kb);
+    const double Lb = d.L0 * exp(st.eps_end);
+    npt_u2prime(p_eps, (s1 * s1) * kb, st.virial, d.P, Lb, d.dof, d.half_dt);
+    const double alpha = 1.0 + 3.0 / d.dof;
+    const double x = d.half_dt * alpha * p_eps / d.w_eps;
+    const double f1 = exp(-x);
+    st.u2[0] = f1;
+    st.u2[1] = (1.0 - f1) / x;
+    const double eps = st.eps_end + d.dt * p_eps / d.w_eps;
+    const double Ln = d.L0 * exp(eps);
+    for (int k = 0; k < NHC_M; k++) {
+      st.eta_cur[k] = eta[k];
+      st.p_eta_cur[k] = pet[k];
+      st.eta_baro_cur[k] = etab[k];
+      st.p_eta_baro_cur[k] = petb[k];
+    }
+    st.p_eps_cur = p_eps;
+    st.eps_cur = eps;
+    st.s1 = s1;
+    dm.invL = 1.0 / Lb;
+    dm.L = Ln;
+    dm.density = (double)d.n / (Ln * Ln * Ln);
+    if (!(Ln > 0.0) || (int)((double)(int)Ln / d.cell_cut) != d.nc) st.status = 2;
   } else if (d.thermostat == 3) {
     // Gaussian isokinetic: the factors need sums of p.F and F^2 over the
     // system; k_gauss_apply computes them (no half kick until it has run)
@@ -855,7 +902,7 @@ __device__ void finalize_sums(const SysDesc &d, SysState &st, int mode, double p
   st.pe = 0.5 * pe;
   st.virial = (0.5 * vir) / 3.0;
   st.vir_act = va;
-  if (mode == 2) {  // force evaluation only (calculate_forces)
+  if (mode >= 2) {  // force evaluation only (calculate_forces)
     __threadfence();
     st.counter_b = 0;
     return;
@@ -870,7 +917,7 @@ __device__ void finalize_sums(const SysDesc &d, SysState &st, int mode, double p
     st.ramp_left -= 1;
     st.ramp_real -= 1;
     if (st.ramp_left > 0) st.ramp_T = st.ramp_real > 0 ? __dadd_rn(st.ramp_T, st.ramp_dT) : st.ramp_end;
-  } else if (mode == 0 && d.thermostat == 2) {
+  } else if (mode == 0 && (d.thermostat == 2 || d.thermostat == 4)) {
     // advance_time_NVT_Berendsen (MDcode/time_evolve.c:173-256): after the
     // NVE step the momenta are scaled by chi = sqrt(1 + (T/inst_T - 1) dt /
     // tau_T); the step's KE and inst_T are reported before the scaling, as
@@ -878,6 +925,35 @@ __device__ void finalize_sums(const SysDesc &d, SysState &st, int mode, double p
     const double inst = 2.0 * (ke * 0.5) / d.dof;
     st.s2 = sqrt(1.00 + (d.T / inst - 1.00) * d.dt / 0.20);
     kb = ke;
+    st.step += 1;
+    if (st.shuf) {
+      st.mt_cur ^= 1;
+      st.shuf = 0;
+    }
+  } else if (mode == 0 && d.thermostat == 5) {
+    // AdvanceTimeNPTNoseHoover's second half (MDcode/time_evolve.c:685-692):
+    // U2 ran in the force pass; U2Prime with its sum p^2 and the new virial at
+    // this step's length, then U4 U3 U4 on both chains and p_eps
+    double eta[NHC_M], pet[NHC_M], etab[NHC_M], petb[NHC_M];
+    for (int k = 0; k < NHC_M; k++) {
+      eta[k] = st.eta_cur[k];
+      pet[k] = st.p_eta_cur[k];
+      etab[k] = st.eta_baro_cur[k];
+      petb[k] = st.p_eta_baro_cur[k];
+    }
+    double p_eps = st.p_eps_cur;
+    npt_u2prime(p_eps, ke, st.virial, d.P, d.L0 * exp(st.eps_cur), d.dof, d.half_dt);
+    const double s2 = npt_half(eta, pet, etab, petb, p_eps, d.q, d.q_baro, d.w_eps, d.T, d.dof, d.dt, ke);
+    for (int k = 0; k < NHC_M; k++) {
+      st.eta_end[k] = eta[k];
+      st.p_eta_end[k] = pet[k];
+      st.eta_baro_end[k] = etab[k];
+      st.p_eta_baro_end[k] = petb[k];
+    }
+    st.p_eps_end = p_eps;
+    st.eps_end = st.eps_cur;
+    st.s2 = s2;
+    kb = (s2 * s2) * ke;
     st.step += 1;
     if (st.shuf) {
       st.mt_cur ^= 1;
@@ -1140,6 +1216,39 @@ __global__ void __launch_bounds__(BLOCK_A) k_gauss_apply(View v) {
   st.counter_g = 0;
 }
 
+// ---------------------------------------------------------------------------
+// Berendsen NPT (thermostat 4, advance_time_NPT, MDcode/time_evolve.c:258-348):
+// at the start of each step (not during a ramp) the box is rescaled and the
+// forces recomputed at the new length (force mode 3) before the kick.
+__device__ __forceinline__ bool npt_due(const SysDesc &d, const SysState &st) {
+  return d.thermostat == 4 && st.ramp_left == 0;
+}
+
+// one thread per system: the pressure from the last forces' virial and
+// calculate_temp's inst_T of the momenta at the step boundary (v * s2, sum
+// p^2 = s2^2 * 2 ke_end), chi_P = (1 + dt (pressure - P) / tau_P)^0.33333333;
+// UpdateBoxForNPT (:823-850) sets DENSITY and inv_L from the length before the
+// change, then L *= chi_P (:266-269).  The cell grid stays; a length whose
+// reference cell count differs sets status 2.
+__global__ void k_npt_box(View v) {
+  for (int r = threadIdx.x; r < v.nsys; r += blockDim.x) {
+    SysDesc &d = const_cast<SysDesc &>(v.desc[r]);
+    SysState &st = v.st[r];
+    if (!npt_due(d, st)) continue;
+    const double keb = (st.s2 * st.s2) * st.ke_end;
+    const double inst = 2.0 * keb / d.dof;
+    const double L = d.L;
+    const double pressure = d.density * inst + st.virial / (L * L * L);
+    const double chi = pow(1.0 + d.dt * (pressure - d.P) / TAU_P, 0.33333333);
+    d.density = (double)d.n / (L * L * L);
+    d.invL = 1.00 / L;
+    const double Ln = chi * L;
+    d.L = Ln;
+    st.pressure = pressure;
+    if (!(Ln > 0.0) || (int)((double)(int)Ln / d.cell_cut) != d.nc) st.status = 2;
+  }
+}
+
 // host request: remove the mean momentum of system r now (with k_drift_sum and
 // k_drift_apply after it)
 __global__ void k_flag_drift(View v, int r) {
@@ -1255,6 +1364,7 @@ __global__ void __launch_bounds__(512) k_force_kick(View v, int mode, int tile_b
   SysState &st = v.st[r];
   if (mode == 1 && !st.prime) return;
   const SysDesc &d = v.desc[r];
+  if (mode == 3 && !npt_due(d, st)) return;
   const int grp = threadIdx.x / TPP, lane = threadIdx.x % TPP;
   const int loc = t.y + grp;
   const bool valid = loc < d.n;
@@ -1338,12 +1448,17 @@ __global__ void __launch_bounds__(512) k_force_kick(View v, int mode, int tile_b
     v.fy[i] = fy;
     v.fz[i] = fz;
     double px, py, pz;
-    if (mode == 2) {
+    if (mode >= 2) {
       px = py = pz = 0.0;
     } else if (mode == 0 && d.thermostat == 3) {  // Gaussian: the kick waits for k_gauss_sum
       px = v.vx[i];
       py = v.vy[i];
       pz = v.vz[i];
+    } else if (mode == 0 && d.thermostat == 5 && st.ramp_left == 0) {  // U2PropagatorNPT
+      const double f1 = st.u2[0], f2 = st.u2[1];
+      px = __dadd_rn(__dmul_rn(v.vx[i], f1), __dmul_rn(__dmul_rn(f2, fx), d.half_dt));
+      py = __dadd_rn(__dmul_rn(v.vy[i], f1), __dmul_rn(__dmul_rn(f2, fy), d.half_dt));
+      pz = __dadd_rn(__dmul_rn(v.vz[i], f1), __dmul_rn(__dmul_rn(f2, fz), d.half_dt));
     } else if (mode == 0) {  // U2 (MDcode/time_evolve.c:558-567)
       px = __dadd_rn(v.vx[i], __dmul_rn(fx, d.half_dt));
       py = __dadd_rn(v.vy[i], __dmul_rn(fy, d.half_dt));
@@ -1354,7 +1469,7 @@ __global__ void __launch_bounds__(512) k_force_kick(View v, int mode, int tile_b
       py = __dmul_rn(v.vy[i], s2);
       pz = __dmul_rn(v.vz[i], s2);
     }
-    if (mode != 2) {
+    if (mode < 2) {
       v.vx[i] = px;
       v.vy[i] = py;
       v.vz[i] = pz;
@@ -1530,9 +1645,12 @@ __global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
   __shared__ GroupStage S;
   __shared__ int pre4[MAX_UNION + 1];
   const int2 tile = v.tiles_g[blockIdx.x];
-  const int r = tile.x, g = tile.y;
+  const int r = tile.x;
   if (!v.st[r].rebuild) return;
   const SysDesc &d = v.desc[r];
+  // the force tiles split a group; its list is built by the first of them
+  if (tile.y % d.gsplit) return;
+  const int g = tile.y / d.gsplit;
   GroupGeom G;
   group_geom(g, d.nc, d.ng, G);
   group_prologue(v, d, G, S);
@@ -1787,10 +1905,16 @@ __device__ __forceinline__ void particle_epilogue(const View &v, const SysDesc &
   v.fx[i] = fx;
   v.fy[i] = fy;
   v.fz[i] = fz;
-  if (mode != 2) {
+  if (mode < 2) {
     const double vx0 = v.vx[i], vy0 = v.vy[i], vz0 = v.vz[i];
     double px = vx0, py = vy0, pz = vz0;
-    if (mode == 0 && d.thermostat != 3) {
+    if (mode == 0 && d.thermostat == 5 && st.ramp_left == 0) {
+      // Nose-Hoover NPT second half kick p f1 + f2 F dt/2 (U2PropagatorNPT)
+      const double f1 = st.u2[0], f2 = st.u2[1];
+      px = __dadd_rn(__dmul_rn(vx0, f1), __dmul_rn(__dmul_rn(f2, fx), d.half_dt));
+      py = __dadd_rn(__dmul_rn(vy0, f1), __dmul_rn(__dmul_rn(f2, fy), d.half_dt));
+      pz = __dadd_rn(__dmul_rn(vz0, f1), __dmul_rn(__dmul_rn(f2, fz), d.half_dt));
+    } else if (mode == 0 && d.thermostat != 3) {
       px = __dadd_rn(vx0, __dmul_rn(fx, d.half_dt));
       py = __dadd_rn(vy0, __dmul_rn(fy, d.half_dt));
       pz = __dadd_rn(vz0, __dmul_rn(fz, d.half_dt));
@@ -1850,10 +1974,14 @@ __global__ void __launch_bounds__(BLOCK_G, PREC ? ACG_FORCE_MINB32 : ACG_FORCE_M
   float2 *slo = reinterpret_cast<float2 *>(gsm_raw + 16 * (size_t)gs);
   __shared__ GroupStage S;
   const int2 tile = v.tiles_g[blockIdx.x];
-  const int r = tile.x, g = tile.y;
+  const int r = tile.x;
   const SysState &st = v.st[r];
   if (mode == 1 && !st.prime) return;
   const SysDesc &d = v.desc[r];
+  if (mode == 3 && !npt_due(d, st)) return;
+  // tile.y = group * gsplit + part: this block takes the part-th contiguous
+  // run of the group's centre particles
+  const int g = tile.y / d.gsplit, part = tile.y - g * d.gsplit;
   GroupGeom G;
   group_geom(g, d.nc, d.ng, G);
   group_prologue(v, d, G, S);
@@ -1896,11 +2024,12 @@ __global__ void __launch_bounds__(BLOCK_G, PREC ? ACG_FORCE_MINB32 : ACG_FORCE_M
   const uint16_t *lst = staged ? group_list(v, d, g) : nullptr;
   double pe = 0.0, vir = 0.0, ke = 0.0, va = 0.0;
   const int lane = threadIdx.x % TPP, nper = blockDim.x / TPP;
+  const int run = (M + d.gsplit - 1) / d.gsplit, t_lo = part * run, t_hi = min(M, t_lo + run);
   // rounds over the centre particles: TPP threads per particle, all threads of
   // a round take part in the shuffle reduction
-  for (int t0 = 0; t0 < M; t0 += nper) {
+  for (int t0 = t_lo; t0 < t_hi; t0 += nper) {
     const int t = t0 + threadIdx.x / TPP;
-    const bool valid = t < M;
+    const bool valid = t < t_hi;
     int kc = 0, i = 0, qs = 0;
     if (valid) group_centre(S, t, kc, i, qs);
     const double4 pi = valid ? v.pos[i] : make_double4(0, 0, 0, 0);
@@ -1998,7 +2127,7 @@ __global__ void __launch_bounds__(BLOCK_G, PREC ? ACG_FORCE_MINB32 : ACG_FORCE_M
     if (!valid || lane != 0) continue;
     particle_epilogue(v, d, st, i, mode, a, pe, vir, ke, va);
   }
-  end_force_block(v, r, g, mode, pe, vir, ke, va);
+  end_force_block(v, r, tile.y, mode, pe, vir, ke, va);
 }
 
 // ---------------------------------------------------------------------------
@@ -2667,6 +2796,7 @@ __global__ void __launch_bounds__(BLOCK_X) k_force_box(View v, int mode) {
   const SysState &st = v.st[r];
   if (mode == 1 && !st.prime) return;
   const SysDesc &d = v.desc[r];
+  if (mode == 3 && !npt_due(d, st)) return;
   const int n = d.n, nce = d.ncell;
   box_stage_force<PREC>(v, d, xsm);
   const int ca = b * d.cpb, cb = min(nce, ca + d.cpb);

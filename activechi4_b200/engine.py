@@ -227,6 +227,12 @@ class Engine:
         pe = _f64(p_eta, (3,))
         check(self._lib.acg_set_nhc(self.h, sys, _ptr(e), _ptr(pe)))
 
+    def set_barostat(self, sys: int, eta_baro, p_eta_baro, p_eps: float):
+        """Barostat chain and p_eps of a Nose-Hoover NPT system (thermostat 5)."""
+        e = _f64(eta_baro, (3,))
+        pe = _f64(p_eta_baro, (3,))
+        check(self._lib.acg_set_barostat(self.h, sys, _ptr(e), _ptr(pe), float(p_eps)))
+
     def set_temperature(self, sys: int, T: float):
         check(self._lib.acg_set_temperature(self.h, sys, float(T)))
 
@@ -256,7 +262,7 @@ class Engine:
         t = acg_thermo()
         rc = self._lib.acg_get_thermo(self.h, sys, C.byref(t))
         out = {f: getattr(t, f) for f, _ in acg_thermo._fields_}
-        for f in ("eta", "p_eta", "q"):
+        for f in ("eta", "p_eta", "q", "eta_baro", "p_eta_baro"):
             out[f] = np.array(list(out[f]))
         check(rc)
         return out

@@ -36,6 +36,8 @@ extern "C" {
 #define ACG_ERR_NOMEM (-3)      /* device allocation failed / footprint too large */
 #define ACG_ERR_NONFINITE (-4)  /* a system's kinetic energy became NaN/inf */
 #define ACG_ERR_STATE (-5)      /* call not valid in the handle's current state */
+#define ACG_ERR_BOX (-6)        /* a constant-pressure system's box left the cell grid it was
+                                   created with ((int)((int)L / Cell_cut) changed) */
 
 #define ACG_PREC_FP64 0 /* pair forces in FP64 (the reference's arithmetic) */
 #define ACG_PREC_FP32 1 /* pair forces in FP32; positions, velocities, thermostat,
@@ -64,7 +66,19 @@ typedef struct acg_params {
                              3: Gaussian isokinetic, each half kick p = f1 (p + f2 F)
                                 with f1, f2 from sum p.F, sum F^2, sum p^2
                                 (AdvanceTimeNVTGaussOSM, MDcode/time_evolve.c:351-470);
-                                T is not used and acg_start_ramp is refused */
+                                T is not used and acg_start_ramp is refused;
+                             4: Berendsen NPT: before each step the box is scaled by
+                                chi_P = (1 + dt (pressure - P)/tau_P)^(1/3), pressure =
+                                DENSITY inst_T + virial/L^3, and the forces recomputed;
+                                then the Berendsen NVT step (advance_time_NPT,
+                                MDcode/time_evolve.c:258-348, with UpdateBoxForNPT :823-850).
+                                The box keeps the cell count it was created with
+                                (ACG_ERR_BOX when the reference's count would change);
+                             5: Nose-Hoover NPT: particle and barostat chains, p_eps and
+                                L = L0 exp(eps) (AdvanceTimeNPTNoseHoover with
+                                U1..U4PropagatorNPT, MDcode/time_evolve.c:654-822); the
+                                barostat state comes from acg_set_barostat; same cell-grid
+                                rule as 4.  Ramps (acg_start_ramp) are refused for 3 and 5 */
   int shuffle;            /* re-randomise the active directions every tau_p_steps steps
                              (ShuffleActDirec cadence, MDcode/main.c:245-247):
                              1: on the device in the reference's order (per component,
@@ -83,6 +97,8 @@ typedef struct acg_params {
   int drift_every;        /* remove the mean momentum (fixDrift, MDcode/initialise.c:104-138)
                              after every step whose index is a multiple of this, as run()
                              does every 100000 steps (MDcode/main.c:261); 0 = never */
+  double P;               /* target pressure of the Berendsen barostat (thermostat 4;
+                             para_file line 4, MDcode/main.c:422) */
 } acg_params;
 
 /* Scalars of one system at the last step boundary. */
@@ -99,7 +115,11 @@ typedef struct acg_thermo {
   int64_t rebuilds;/* cell/neighbour list rebuilds so far */
   int overflow;    /* particles that overflowed the neighbour-list capacity at the
                       last rebuild (served from the cell list instead) */
-  int status;      /* 0 or ACG_ERR_NONFINITE */
+  int status;      /* 0, ACG_ERR_NONFINITE or ACG_ERR_BOX */
+  double L;        /* current box length (changes under thermostats 4 and 5) */
+  double pressure; /* DENSITY inst_T + virial/L^3 at the last box update (thermostat 4) */
+  double eps, p_eps;                 /* barostat (thermostat 5): L = L0 exp(eps) */
+  double eta_baro[3], p_eta_baro[3]; /* barostat chain (thermostat 5) */
 } acg_thermo;
 
 typedef struct acg_engine acg_engine;
@@ -191,6 +211,12 @@ int acg_set_lattice(acg_engine *e, int sys, const int *site, const int *type, co
 /* Thermostat chain state (InitialiseNoseHoover, MDcode/time_evolve.c:476-493:
  * eta = 0, p_eta drawn by the caller).  q follows from T and n. */
 int acg_set_nhc(acg_engine *e, int sys, const double *eta3, const double *p_eta3);
+/* Barostat state of a Nose-Hoover NPT system (thermostat 5) at the step
+ * boundary: chain eta_baro[3], p_eta_baro[3] and p_eps (InitialiseNoseHooverNPT,
+ * MDcode/time_evolve.c:614-652, draws them; eps starts at 0 with L0 = the
+ * creation length).  The next step's first half is recomputed. */
+int acg_set_barostat(acg_engine *e, int sys, const double *eta_baro3, const double *p_eta_baro3, double p_eps);
+
 /* Change a system's thermostat temperature (and with it q). */
 int acg_set_temperature(acg_engine *e, int sys, double T);
 

@@ -262,6 +262,13 @@ class Reference(_Common):
             lib.ref_run_berendsen.argtypes = [C.c_int]
             lib.ref_run_gauss.restype = C.c_int
             lib.ref_run_gauss.argtypes = [C.c_int]
+            lib.ref_run_npt.restype = C.c_int
+            lib.ref_run_npt.argtypes = [C.c_int, C.c_double]
+            lib.ref_get_box.argtypes = [_dp]
+            lib.ref_set_npt.argtypes = [_dp, _dp, _dp, _dp, C.c_double]
+            lib.ref_run_nhc_npt.restype = C.c_int
+            lib.ref_run_nhc_npt.argtypes = [C.c_int, C.c_double]
+            lib.ref_get_npt.argtypes = [_dp]
             lib.ref_adjust_temp.restype = C.c_double
             lib.ref_adjust_temp.argtypes = [C.c_double]
             lib.ref_coldstart.argtypes = [C.c_double, C.c_double]
@@ -316,6 +323,34 @@ class Reference(_Common):
         """AdvanceTimeNVTGaussOSM nsteps times (the reference's own build)."""
         if self.lib.ref_run_gauss(int(nsteps)):
             raise RuntimeError("this build has no AdvanceTimeNVTGaussOSM")
+
+    def run_npt(self, nsteps, P):
+        """advance_time_NPT nsteps times at target pressure P (the reference's own build)."""
+        if self.lib.ref_run_npt(int(nsteps), float(P)):
+            raise RuntimeError("this build has no advance_time_NPT")
+
+    def set_npt(self, eta, p_eta, eta_baro, p_eta_baro, p_eps):
+        """Nose-Hoover NPT state (InitialiseNoseHooverNPT with the momenta given)."""
+        f = lambda a: np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(3))  # noqa: E731
+        self.lib.ref_set_npt(f(eta), f(p_eta), f(eta_baro), f(p_eta_baro), float(p_eps))
+
+    def run_nhc_npt(self, nsteps, P):
+        """AdvanceTimeNPTNoseHoover nsteps times at target pressure P."""
+        if self.lib.ref_run_nhc_npt(int(nsteps), float(P)):
+            raise RuntimeError("this build has no AdvanceTimeNPTNoseHoover")
+
+    def npt_state(self):
+        """eps, p_eps, eta_baro, p_eta_baro, eta, p_eta of the program's globals."""
+        out = np.zeros(14)
+        self.lib.ref_get_npt(out)
+        return {"eps": out[0], "p_eps": out[1], "eta_baro": out[2:5], "p_eta_baro": out[5:8],
+                "eta": out[8:11], "p_eta": out[11:14]}
+
+    def box(self):
+        """(L, inv_L, DENSITY) of the program's globals."""
+        out = np.zeros(3)
+        self.lib.ref_get_box(out)
+        return tuple(float(v) for v in out)
 
     def run_berendsen(self, nsteps):
         """advance_time_NVT_Berendsen nsteps times (the reference's own build)."""

@@ -208,6 +208,67 @@ int ref_run_gauss(int nsteps) {
   return 0;
 }
 
+/* advance_time_NPT (MDcode/time_evolve.c:258-348), nsteps times at target
+ * pressure Pset; weak like the Berendsen step */
+void advance_time_NPT(void) __attribute__((weak));
+int ref_run_npt(int nsteps, double Pset) {
+  if (!advance_time_NPT) return -1;
+  P = Pset;
+  for (int i = 0; i < nsteps; i++) advance_time_NPT();
+  return 0;
+}
+
+/* Nose-Hoover NPT state as InitialiseNoseHooverNPT (MDcode/time_evolve.c:614-652)
+ * leaves it, with the chain momenta given instead of drawn: tau = 0.2,
+ * tau_baro = 2, L0 = L, eps = 0, the masses from T */
+void ref_set_npt(const double *eta_in, const double *p_eta_in, const double *eta_baro_in,
+                 const double *p_eta_baro_in, double p_eps_in) {
+  tau = .20;
+  tau_baro = 2.0;
+  L0 = L;
+  w_eps = DOF * T * tau_baro * tau_baro;
+  eps = 0.0;
+  for (int i = 0; i < M; i++) {
+    q[i] = T * tau * tau;
+    eta[i] = eta_in[i];
+    p_eta[i] = p_eta_in[i];
+    q_baro[i] = T * tau_baro * tau_baro;
+    eta_baro[i] = eta_baro_in[i];
+    p_eta_baro[i] = p_eta_baro_in[i];
+  }
+  q[0] = DOF * T * tau * tau;
+  p_eps = p_eps_in;
+}
+
+/* AdvanceTimeNPTNoseHoover (MDcode/time_evolve.c:654-696), nsteps times at
+ * target pressure Pset */
+void AdvanceTimeNPTNoseHoover(void) __attribute__((weak));
+int ref_run_nhc_npt(int nsteps, double Pset) {
+  if (!AdvanceTimeNPTNoseHoover) return -1;
+  P = Pset;
+  for (int i = 0; i < nsteps; i++) AdvanceTimeNPTNoseHoover();
+  return 0;
+}
+
+/* out: eps, p_eps, eta_baro[3], p_eta_baro[3], eta[3], p_eta[3] */
+void ref_get_npt(double *out) {
+  out[0] = eps;
+  out[1] = p_eps;
+  for (int i = 0; i < 3; i++) {
+    out[2 + i] = eta_baro[i];
+    out[5 + i] = p_eta_baro[i];
+    out[8 + i] = eta[i];
+    out[11 + i] = p_eta[i];
+  }
+}
+
+/* out: L, inv_L, DENSITY */
+void ref_get_box(double *out) {
+  out[0] = L;
+  out[1] = inv_L;
+  out[2] = DENSITY;
+}
+
 /* one NVT step composed from the propagators, as AdvanceTimeNVTNoseHoover's
  * body does (MDcode/time_evolve.c:495-526) */
 void ref_step_propagators(void) {

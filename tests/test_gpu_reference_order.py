@@ -240,3 +240,87 @@ def test_gaussian_isokinetic_drift_and_graph_match_eager(cuda_lib, g1000):
     assert np.abs(p.sum(axis=0)).max() < 1e-9 * np.abs(p).sum()
     with pytest.raises(AcgError):
         a.start_ramp(0, 0.2, 0.45, 0.1)
+
+
+def _npt_target(ref, st):
+    """A target pressure 0.3 above the starting state's (so the box shrinks)."""
+    L0, _, rho0 = ref.box()
+    inst = (st.p ** 2).sum() / (3.0 * st.n - 3.0)
+    return rho0 * inst + ref.scalars()["virial"] / L0 ** 3 + 0.3
+
+
+def test_berendsen_npt_matches_reference(cuda_lib, g1000):
+    """thermostat = 4: the reference's advance_time_NPT (box rescaled by the
+    Berendsen barostat and forces recomputed before each Berendsen NVT step)
+    for 50 steps, against the reference program itself: positions, momenta,
+    energies and the box length."""
+    from oracle import Reference, reference_available
+    if not reference_available(1000):
+        pytest.skip("reference library not built")
+    st = golden_state(g1000)
+    ref = Reference(1000)
+    ref.setup(st, 0.45, 1.0)
+    P = _npt_target(ref, st)
+    ref.run_npt(50, P)
+    e = engine_for(st, shuffle=0, drift_every=0, thermostat=4, P=P, L=st.L)
+    e.step(50)
+    x, xu, p, F = e.get_state()
+    xr, xur, pr, Fr = ref.get_state()
+    Lr = ref.box()[0]
+    th, sr = e.thermo(), ref.scalars()
+    assert abs(th["L"] - Lr) < 1e-12 * Lr and th["L"] < st.L * (1 - 1e-4)
+    assert np.abs(xu - xur).max() < 1e-9
+    assert np.abs(p - pr).max() / np.sqrt((pr ** 2).sum(axis=1).mean()) < 1e-9
+    assert abs(th["ke"] - sr["ke"]) < 1e-9 * sr["ke"] and abs(th["pe"] - sr["pe"]) < 1e-9 * abs(sr["pe"])
+
+
+def test_berendsen_npt_graph_eager_and_reconfiguration(cuda_lib, g1000):
+    """The constant-pressure step in the CUDA graph equals the kernel-by-kernel
+    launches bit for bit, also across a change of the launch shape (which
+    uploads the descriptors again and must keep the device's box length)."""
+    st = golden_state(g1000)
+    a = engine_for(st, shuffle=0, drift_every=0, thermostat=4, P=5.3, L=st.L)
+    b = engine_for(st, shuffle=0, drift_every=0, thermostat=4, P=5.3, L=st.L)
+    a.step(30)
+    b.step_eager(30)
+    cells = a.get_box_cells()
+    a.set_box_cells(1 if cells != 1 else 2)
+    b.set_box_cells(1 if cells != 1 else 2)
+    a.step(20)
+    b.step_eager(20)
+    for u, w in zip(a.get_state(), b.get_state()):
+        assert np.array_equal(u, w)
+    assert a.thermo()["L"] == b.thermo()["L"] < st.L
+
+
+def test_nose_hoover_npt_matches_reference(cuda_lib, g1000):
+    """thermostat = 5: the reference's AdvanceTimeNPTNoseHoover (particle and
+    barostat chains, p_eps, L = L0 exp(eps), U1..U4PropagatorNPT) for 50
+    steps from the same chain and barostat state, against the reference
+    program itself: positions, momenta, energies, box, eps, p_eps and both
+    chains."""
+    from oracle import Reference, reference_available
+    if not reference_available(1000):
+        pytest.skip("reference library not built")
+    st = golden_state(g1000)
+    p_eta, p_eta_b, p_eps, P = g1000["p_eta0"], np.array([0.1, -0.05, 0.02]), 20.0, 5.3
+    ref = Reference(1000)
+    ref.setup(st, 0.45, 1.0)
+    ref.set_npt(np.zeros(3), p_eta, np.zeros(3), p_eta_b, p_eps)
+    ref.run_nhc_npt(50, P)
+    e = engine_for(st, shuffle=0, drift_every=0, thermostat=5, P=P, L=st.L)
+    e.set_nhc(0, np.zeros(3), p_eta)
+    e.set_barostat(0, np.zeros(3), p_eta_b, p_eps)
+    e.step(25)
+    e.step(25)
+    x, xu, p, F = e.get_state()
+    xr, xur, pr, Fr = ref.get_state()
+    th, sr, nr = e.thermo(), ref.scalars(), ref.npt_state()
+    Lr = ref.box()[0]
+    assert abs(th["L"] - Lr) < 1e-12 * Lr and th["L"] < st.L * (1 - 1e-4)
+    assert abs(th["eps"] - nr["eps"]) < 1e-12 and abs(th["p_eps"] - nr["p_eps"]) < 1e-9 * abs(nr["p_eps"])
+    assert np.allclose(th["p_eta_baro"], nr["p_eta_baro"], rtol=1e-9, atol=1e-12)
+    assert np.allclose(th["p_eta"], nr["p_eta"], rtol=1e-9, atol=1e-12)
+    assert np.abs(xu - xur).max() < 1e-9
+    assert np.abs(p - pr).max() / np.sqrt((pr ** 2).sum(axis=1).mean()) < 1e-9
+    assert abs(th["ke"] - sr["ke"]) < 1e-9 * sr["ke"] and abs(th["pe"] - sr["pe"]) < 1e-9 * abs(sr["pe"])
