@@ -139,6 +139,7 @@ struct SysState {
   double eta_baro_end[NHC_M], p_eta_baro_end[NHC_M], eta_baro_cur[NHC_M], p_eta_baro_cur[NHC_M];
   double p_eps_end, p_eps_cur, eps_end, eps_cur;
   double u2[2];
+  double brown_m[3];         // active Brownian (thermostat 6): mean random force of this step
 };
 
 // In-place observables of one system (set by acg_obs_configure): events of the
@@ -312,6 +313,45 @@ __device__ inline void npt_u2prime(double &p_eps, double ksum, double virial, do
   const double alpha = 1.0 + 3.0 / dof;
   const double PV = alpha * (ksum) / (3.00) + virial;
   p_eps += 3.00 * (PV - P * L * L * L) * half_dt;
+}
+
+// Philox4x32-10 (Salmon, Moraes, Dror and Shaw, SC'11): ten rounds of two
+// 32x32->64 multiplies on a 128-bit counter under a 64-bit key bumped by the
+// Weyl constants after every round
+struct Philox4 {
+  unsigned int x, y, z, w;
+};
+__host__ __device__ inline Philox4 philox4x32(Philox4 c, unsigned int k0, unsigned int k1) {
+  for (int r = 0; r < 10; r++) {
+    const unsigned long long p0 = 0xD2511F53ull * (unsigned long long)c.x;
+    const unsigned long long p1 = 0xCD9E8D57ull * (unsigned long long)c.z;
+    const unsigned int hi0 = (unsigned int)(p0 >> 32), lo0 = (unsigned int)p0;
+    const unsigned int hi1 = (unsigned int)(p1 >> 32), lo1 = (unsigned int)p1;
+    c = Philox4{hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0};
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return c;
+}
+
+// uniform in (0, 1) from 53 bits of two words
+__host__ __device__ inline double u53(unsigned int a, unsigned int b) {
+  const unsigned long long m = ((((unsigned long long)a) << 32) | b) >> 11;
+  return ((double)m + 0.5) * (1.0 / 9007199254740992.0);
+}
+
+// three standard normals of particle `id` at step `step` of stream `seed`
+// (Box-Muller on two Philox draws: counters {id, step lo, step hi, 0 | 1})
+__device__ inline void normals3(unsigned long long seed, long long step, int id, double g[3]) {
+  const unsigned int k0 = (unsigned int)seed, k1 = (unsigned int)(seed >> 32);
+  const unsigned int s0 = (unsigned int)(unsigned long long)step, s1 = (unsigned int)((unsigned long long)step >> 32);
+  const Philox4 a = philox4x32(Philox4{(unsigned int)id, s0, s1, 0u}, k0, k1);
+  const Philox4 b = philox4x32(Philox4{(unsigned int)id, s0, s1, 1u}, k0, k1);
+  const double r1 = sqrt(-2.0 * log(u53(a.x, a.y))), t1 = 6.283185307179586 * u53(a.z, a.w);
+  const double r2 = sqrt(-2.0 * log(u53(b.x, b.y))), t2 = 6.283185307179586 * u53(b.z, b.w);
+  g[0] = r1 * cos(t1);
+  g[1] = r1 * sin(t1);
+  g[2] = r2 * cos(t2);
 }
 
 // MT19937 (Matsumoto & Nishimura 1998): seeding by their 2002 initialisation

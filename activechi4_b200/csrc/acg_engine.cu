@@ -98,7 +98,7 @@ int resolve(const acg_params &p, SysDesc &d) {
   d.seed = p.seed;
   if (p.dt <= 0 || p.skin <= 0 || p.rebuild_factor <= 0)
     return fail(ACG_ERR_INVALID, "dt, skin and rebuild_factor must be positive");
-  if (p.thermostat < 0 || p.thermostat > 5) return fail(ACG_ERR_INVALID, "thermostat must be 0 to 5");
+  if (p.thermostat < 0 || p.thermostat > 6) return fail(ACG_ERR_INVALID, "thermostat must be 0 to 6");
   if (p.thermostat && !(p.T > 0)) return fail(ACG_ERR_INVALID, "thermostat needs T > 0");
   if (p.shuffle < 0 || p.shuffle > 2) return fail(ACG_ERR_INVALID, "shuffle must be 0, 1 or 2");
   if (p.shuffle && p.tau_p_steps <= 0) return fail(ACG_ERR_INVALID, "shuffle needs tau_p_steps > 0");
@@ -248,6 +248,7 @@ struct acg_engine {
   bool any_gauss = false;  // a system runs the Gaussian isokinetic integrator (thermostat 3)
   bool any_npt = false;    // a system runs the Berendsen barostat (thermostat 4)
   bool any_box = false;    // a system's box length changes on the device (thermostats 4 and 5)
+  bool any_brown = false;  // a system runs active Brownian dynamics (thermostat 6)
   bool desc_live = false;  // the descriptors on the device are the current ones
   cudaGraphExec_t gexec = nullptr;
   cudaGraph_t graph = nullptr;
@@ -517,16 +518,21 @@ void launch_gauss(acg_engine *e, bool with_sum) {
   k_gauss_apply<<<e->ntiles_a, BLOCK_A, 0, e->stream>>>(e->v);
 }
 
-// constant pressure: the box update, then the forces at the new length
-int launch_npt(acg_engine *e) {
-  if (!e->any_npt) return ACG_OK;
-  k_npt_box<<<1, 32, 0, e->stream>>>(e->v);
+// before the kick: the Berendsen barostat's box update and the Brownian
+// random forces and predictor, then the forces of those systems (mode 3)
+int launch_pre(acg_engine *e) {
+  if (!e->any_npt && !e->any_brown) return ACG_OK;
+  if (e->any_npt) k_npt_box<<<1, 32, 0, e->stream>>>(e->v);
+  if (e->any_brown) {
+    k_brown_noise<<<e->ntiles_a, BLOCK_A, 0, e->stream>>>(e->v);
+    k_brown_predict<<<e->ntiles_a, BLOCK_A, 0, e->stream>>>(e->v);
+  }
   CK(cudaGetLastError());
   return launch_force(e, 3);
 }
 
 int launch_step_eager(acg_engine *e) {
-  int rc0 = launch_npt(e);
+  int rc0 = launch_pre(e);
   if (rc0) return rc0;
   k_kick_drift<<<e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, 0, e->stream>>>(e->v, 0, 0, 0);
   k_shuffle_ref<<<3 * e->lay.nsys, BLOCK_SHUF, shuffle_smem(e->lay), e->stream>>>(e->v, -1);
@@ -598,11 +604,24 @@ int add_steps(acg_engine *e, cudaGraph_t g, int K, cudaGraphNode_t *prev_io) {
     CK(cudaGraphConditionalHandleCreate(&ho, g, 0, cudaGraphCondAssignDefault));
     cudaGraphNode_t na, nc, nb;
     int rc;
-    if (e->any_npt) {  // constant pressure: box update, forces at the new length
+    if (e->any_npt || e->any_brown) {
+      // Berendsen barostat box update; Brownian random forces and predictor;
+      // then the forces of those systems (mode 3)
       void *va0[] = {&v};
-      rc = add_kernel(g, prev ? &prev : nullptr, prev ? 1 : 0, &nb, (void *)k_npt_box, 1, 32, va0);
-      if (rc) return rc;
-      prev = nb;
+      if (e->any_npt) {
+        rc = add_kernel(g, prev ? &prev : nullptr, prev ? 1 : 0, &nb, (void *)k_npt_box, 1, 32, va0);
+        if (rc) return rc;
+        prev = nb;
+      }
+      if (e->any_brown) {
+        rc = add_kernel(g, prev ? &prev : nullptr, prev ? 1 : 0, &nb, (void *)k_brown_noise, e->ntiles_a, BLOCK_A,
+                        va0);
+        if (rc) return rc;
+        prev = nb;
+        rc = add_kernel(g, &prev, 1, &nb, (void *)k_brown_predict, e->ntiles_a, BLOCK_A, va0);
+        if (rc) return rc;
+        prev = nb;
+      }
       int mode3 = 3;
       if (e->ntiles_g) {
         void *ga[] = {&v, &mode3};
@@ -880,6 +899,7 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
     e->any_gauss |= e->lay.desc[r].thermostat == 3;
     e->any_npt |= e->lay.desc[r].thermostat == 4;
     e->any_box |= e->lay.desc[r].thermostat == 4 || e->lay.desc[r].thermostat == 5;
+    e->any_brown |= e->lay.desc[r].thermostat == 6;
   }
   cudaError_t ce = cudaSetDevice(device);
   if (ce != cudaSuccess) {
@@ -1297,8 +1317,9 @@ int acg_start_ramp(acg_engine *e, int sys, double T_start, double T_end, double 
   if (!(T_start > 0) || !(T_end > 0) || !(rate > 0) || !std::isfinite(T_start) || !std::isfinite(T_end))
     return fail(ACG_ERR_INVALID, "ramp temperatures and rate must be positive");
   const SysDesc &d = e->lay.desc[sys];
-  if (d.thermostat == 3 || d.thermostat == 5)
-    return fail(ACG_ERR_INVALID, "temperature ramps are refused for Gaussian isokinetic and Nose-Hoover NPT systems");
+  if (d.thermostat == 3 || d.thermostat >= 5)
+    return fail(ACG_ERR_INVALID,
+                "temperature ramps are refused for Gaussian isokinetic, Nose-Hoover NPT and Brownian systems");
   double T0 = 0;
   rc = acg_adjust_temperature(e, sys, T_start, &T0);
   if (rc) return rc;
@@ -1914,8 +1935,10 @@ int acg_bench_steps(acg_engine *e, int64_t nsteps, size_t flush_bytes, double *m
   // events the three kernels of that branch (the node lists of add_steps);
   // with a Gaussian isokinetic system two more per step and one more per branch
   const long long nforce = (e->ntiles_g > 0) + (e->ntiles_x > 0) + (e->ntiles_b > 0);
-  // (constant pressure: the box update and a second force pass every step)
-  const long long per_step = 1 + nforce + 2 * e->any_gauss + e->any_npt * (1 + nforce);
+  // (Berendsen barostat: the box update, Brownian: the random forces and the
+  // predictor, and for either a second force pass every step)
+  const long long per_step = 1 + nforce + 2 * e->any_gauss + e->any_npt + 2 * e->any_brown +
+                             (e->any_npt || e->any_brown) * nforce;
   const long long per_rebuild = 5 + (e->lay.box_m3max > 0) + 2 * (e->ntiles_x > 0) + (e->ntiles_g > 0) +
                                 (e->ntiles_l > 0);
   long long steps_with_rebuild = 0, shuffles = 0, posts = 0;

@@ -232,6 +232,75 @@ __global__ void k_mt_flip(View v, int r) {
 }
 
 // ---------------------------------------------------------------------------
+// systems whose step starts with a force pass of their own (force mode 3):
+// the Berendsen barostat's box change (thermostat 4) and the active Brownian
+// predictor (thermostat 6); none during a ramp
+__device__ __forceinline__ bool pre_due(const SysDesc &d, const SysState &st) {
+  return (d.thermostat == 4 || d.thermostat == 6) && st.ramp_left == 0;
+}
+
+// active Brownian constants with D0 = 1 (MDcode/global.h:50, initialise.c:
+// 287-291): D0ByT = D0/T, TByD0 = T/D0, expFactor = exp(-dt TByD0); the
+// displacement dx = D0ByT ((1 - e) p + c f) with c = D0ByT (TByD0 dt - (1 - e))
+struct BrownConst {
+  double d0t, e, ome, c, cp;
+  __device__ __forceinline__ explicit BrownConst(const SysDesc &d) {
+    d0t = 1.0 / d.T;
+    const double t0 = d.T / 1.0;
+    e = exp(-d.dt * t0);
+    ome = 1.0 - e;
+    c = d0t * (t0 * d.dt - ome);
+    cp = d0t * ome;
+  }
+  __device__ __forceinline__ double dx(double p, double f) const {
+    return __dmul_rn(d0t, __dadd_rn(__dmul_rn(ome, p), __dmul_rn(c, f)));
+  }
+};
+
+// the system's Brownian scratch in the upload staging area (free while it
+// steps): random force, position before the predictor, force before it
+__device__ __forceinline__ double *brown_scratch(const View &v, const SysDesc &d) {
+  return v.stage_d + 9 * (size_t)d.poff;
+}
+
+// advance_time_ActiveBrown_PC's corrector for one particle (MDcode/
+// time_evolve.c:915-946): back to the position before the predictor, the
+// mean of the two forces plus the random force, x and x_u moved, p updated;
+// returns |x_u - x_old|^2 (reduced units) for the rebuild test
+__device__ __forceinline__ double brown_correct_one(const View &v, const SysDesc &d, int i) {
+  const BrownConst B(d);
+  const int n = d.n, loc = i - d.poff;
+  const double *s = brown_scratch(v, d);
+  const double il = d.invL;
+  const double fr[3] = {s[3 * loc], s[3 * loc + 1], s[3 * loc + 2]};
+  const double ro[3] = {s[3 * n + 3 * loc], s[3 * n + 3 * loc + 1], s[3 * n + 3 * loc + 2]};
+  const double fo[3] = {s[6 * n + 3 * loc], s[6 * n + 3 * loc + 1], s[6 * n + 3 * loc + 2]};
+  const double F[3] = {v.fx[i], v.fy[i], v.fz[i]};
+  double *pv[3] = {v.vx + i, v.vy + i, v.vz + i};
+  double *uv[3] = {v.ux + i, v.uy + i, v.uz + i};
+  const double *ov[3] = {v.ox + i, v.oy + i, v.oz + i};
+  double4 pos = v.pos[i];
+  double xo[3], e2 = 0.0;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const double f = __dadd_rn(fr[k], __dmul_rn(0.5, __dadd_rn(F[k], fo[k])));
+    const double p = *pv[k];
+    const double dd = B.dx(p, f);
+    const double step = __dmul_rn(dd, il);
+    xo[k] = wrap_unit(__dadd_rn(ro[k], step));
+    const double u = __dadd_rn(*uv[k], step);
+    *uv[k] = u;
+    *pv[k] = __dadd_rn(__dmul_rn(B.e, p), __dmul_rn(B.cp, f));
+    const double ex = __dadd_rn(u, -*ov[k]);
+    e2 = __dadd_rn(e2, __dmul_rn(ex, ex));
+  }
+  pos.x = xo[0];
+  pos.y = xo[1];
+  pos.z = xo[2];
+  v.pos[i] = pos;
+  return e2;
+}
+
 // U3 U2 (pending thermostat scales and the half kick) and U1 for one
 // particle, in the reference's order of roundings; returns |x_u - x_old|^2
 // (reduced units) for the rebuild test
@@ -333,7 +402,10 @@ __global__ void __launch_bounds__(BLOCK_A) k_kick_drift(View v, int use_cond, cu
     const SysDesc &d = v.desc[r];
     int loc = t.y + threadIdx.x;
     if (loc < d.n) {
-      mymax = kick_drift_one(v, d, v.st[r], d.poff + loc);
+      if (d.thermostat == 6 && v.st[r].ramp_left == 0)
+        mymax = brown_correct_one(v, d, d.poff + loc);
+      else
+        mymax = kick_drift_one(v, d, v.st[r], d.poff + loc);
     }
     // per-system block max (a tile never straddles systems)
     for (int o = 16; o > 0; o >>= 1) mymax = fmax(mymax, __shfl_down_sync(0xffffffffu, mymax, o));
@@ -1217,6 +1289,89 @@ __global__ void __launch_bounds__(BLOCK_A) k_gauss_apply(View v) {
 }
 
 // ---------------------------------------------------------------------------
+// active Brownian dynamics, predictor-corrector (thermostat 6,
+// advance_time_ActiveBrown_PC, MDcode/time_evolve.c:855-974).  Random forces
+// SqrtVariance N(0,1) per component with SqrtVariance = sqrt(2 T^2 / (dt D0))
+// (initialise.c:287), the reference's GSL draws replaced by a counter-based
+// stream (Philox4x32-10 keyed by the system's seed, counter = particle id and
+// step), minus their mean; k_brown_predict moves the particles to the
+// predicted positions, force mode 3 evaluates the forces there, and the
+// corrector runs in k_kick_drift.
+__global__ void __launch_bounds__(BLOCK_A) k_brown_noise(View v) {
+  __shared__ double sh[BLOCK_A / 32];
+  __shared__ int s_last;
+  const int2 t = v.tiles_a[blockIdx.x];
+  const int r = t.x;
+  const SysDesc &d = v.desc[r];
+  SysState &st = v.st[r];
+  if (d.thermostat != 6 || st.ramp_left != 0) return;
+  const int loc = t.y + threadIdx.x;
+  double g[3] = {0.0, 0.0, 0.0};
+  if (loc < d.n) {
+    const int i = d.poff + loc;
+    normals3(d.seed ^ 0x5DEECE66DULL, st.step, v.id[i], g);
+    const double sv = sqrt(2.0 * d.T * d.T / (d.dt * 1.0));
+    double *s = brown_scratch(v, d);
+    for (int k = 0; k < 3; k++) {
+      g[k] = sv * g[k];
+      s[3 * loc + k] = g[k];
+    }
+  }
+  double *part = v.part_o + (size_t)blockIdx.x * OBS_EMAX * OBS_NV;
+  for (int k = 0; k < 3; k++) {
+    const double b = block_sum<BLOCK_A / 32>(g[k], sh);
+    if (threadIdx.x == 0) part[k] = b;
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(&st.counter_g, 1u) == (unsigned)(d.ntile_a - 1);
+  }
+  __syncthreads();
+  if (!s_last || threadIdx.x != 0) return;
+  __threadfence();
+  double m[3] = {0.0, 0.0, 0.0};
+  for (int b = 0; b < d.ntile_a; b++) {
+    const double *pb = v.part_o + (size_t)(d.tile0_a + b) * OBS_EMAX * OBS_NV;
+    for (int k = 0; k < 3; k++) m[k] += __ldcg(pb + k);
+  }
+  for (int k = 0; k < 3; k++) st.brown_m[k] = m[k] / (double)d.n;
+  __threadfence();
+  st.counter_g = 0;
+}
+
+// the random forces minus their mean; position and force before the predictor
+// kept; predicted positions x + D0ByT ((1 - e) p + c (F_random + F)) / L
+// (MDcode/time_evolve.c:885-912, x_u untouched)
+__global__ void __launch_bounds__(BLOCK_A) k_brown_predict(View v) {
+  const int2 t = v.tiles_a[blockIdx.x];
+  const int r = t.x;
+  const SysDesc &d = v.desc[r];
+  const SysState &st = v.st[r];
+  if (d.thermostat != 6 || st.ramp_left != 0) return;
+  const int loc = t.y + threadIdx.x;
+  if (loc >= d.n) return;
+  const int i = d.poff + loc, n = d.n;
+  const BrownConst B(d);
+  double *s = brown_scratch(v, d);
+  double4 pos = v.pos[i];
+  const double F[3] = {v.fx[i], v.fy[i], v.fz[i]};
+  const double P[3] = {v.vx[i], v.vy[i], v.vz[i]};
+  double x[3] = {pos.x, pos.y, pos.z};
+  for (int k = 0; k < 3; k++) {
+    const double fr = __dadd_rn(s[3 * loc + k], -st.brown_m[k]);
+    s[3 * loc + k] = fr;
+    s[3 * n + 3 * loc + k] = x[k];
+    s[6 * n + 3 * loc + k] = F[k];
+    const double dd = B.dx(P[k], __dadd_rn(fr, F[k]));
+    x[k] = wrap_unit(__dadd_rn(x[k], __dmul_rn(dd, d.invL)));
+  }
+  pos.x = x[0];
+  pos.y = x[1];
+  pos.z = x[2];
+  v.pos[i] = pos;
+}
+
+// ---------------------------------------------------------------------------
 // Berendsen NPT (thermostat 4, advance_time_NPT, MDcode/time_evolve.c:258-348):
 // at the start of each step (not during a ramp) the box is rescaled and the
 // forces recomputed at the new length (force mode 3) before the kick.
@@ -1364,7 +1519,7 @@ __global__ void __launch_bounds__(512) k_force_kick(View v, int mode, int tile_b
   SysState &st = v.st[r];
   if (mode == 1 && !st.prime) return;
   const SysDesc &d = v.desc[r];
-  if (mode == 3 && !npt_due(d, st)) return;
+  if (mode == 3 && !pre_due(d, st)) return;
   const int grp = threadIdx.x / TPP, lane = threadIdx.x % TPP;
   const int loc = t.y + grp;
   const bool valid = loc < d.n;
@@ -1450,7 +1605,8 @@ __global__ void __launch_bounds__(512) k_force_kick(View v, int mode, int tile_b
     double px, py, pz;
     if (mode >= 2) {
       px = py = pz = 0.0;
-    } else if (mode == 0 && d.thermostat == 3) {  // Gaussian: the kick waits for k_gauss_sum
+    } else if (mode == 0 && (d.thermostat == 3 || (d.thermostat == 6 && st.ramp_left == 0))) {
+      // Gaussian: the kick waits for k_gauss_sum; Brownian: no kick
       px = v.vx[i];
       py = v.vy[i];
       pz = v.vz[i];
@@ -1914,7 +2070,7 @@ __device__ __forceinline__ void particle_epilogue(const View &v, const SysDesc &
       px = __dadd_rn(__dmul_rn(vx0, f1), __dmul_rn(__dmul_rn(f2, fx), d.half_dt));
       py = __dadd_rn(__dmul_rn(vy0, f1), __dmul_rn(__dmul_rn(f2, fy), d.half_dt));
       pz = __dadd_rn(__dmul_rn(vz0, f1), __dmul_rn(__dmul_rn(f2, fz), d.half_dt));
-    } else if (mode == 0 && d.thermostat != 3) {
+    } else if (mode == 0 && d.thermostat != 3 && !(d.thermostat == 6 && st.ramp_left == 0)) {
       px = __dadd_rn(vx0, __dmul_rn(fx, d.half_dt));
       py = __dadd_rn(vy0, __dmul_rn(fy, d.half_dt));
       pz = __dadd_rn(vz0, __dmul_rn(fz, d.half_dt));
@@ -1924,8 +2080,9 @@ __device__ __forceinline__ void particle_epilogue(const View &v, const SysDesc &
       py = __dmul_rn(vy0, s2);
       pz = __dmul_rn(vz0, s2);
     }
-    // (Gaussian isokinetic step: the second half kick waits for k_gauss_sum)
-    if (mode != 0 || d.thermostat != 3) {
+    // (Gaussian isokinetic step: the second half kick waits for k_gauss_sum;
+    // active Brownian step: no kick after the forces)
+    if (mode != 0 || (d.thermostat != 3 && !(d.thermostat == 6 && st.ramp_left == 0))) {
       v.vx[i] = px;
       v.vy[i] = py;
       v.vz[i] = pz;
@@ -1978,7 +2135,7 @@ __global__ void __launch_bounds__(BLOCK_G, PREC ? ACG_FORCE_MINB32 : ACG_FORCE_M
   const SysState &st = v.st[r];
   if (mode == 1 && !st.prime) return;
   const SysDesc &d = v.desc[r];
-  if (mode == 3 && !npt_due(d, st)) return;
+  if (mode == 3 && !pre_due(d, st)) return;
   // tile.y = group * gsplit + part: this block takes the part-th contiguous
   // run of the group's centre particles
   const int g = tile.y / d.gsplit, part = tile.y - g * d.gsplit;
@@ -2796,7 +2953,7 @@ __global__ void __launch_bounds__(BLOCK_X) k_force_box(View v, int mode) {
   const SysState &st = v.st[r];
   if (mode == 1 && !st.prime) return;
   const SysDesc &d = v.desc[r];
-  if (mode == 3 && !npt_due(d, st)) return;
+  if (mode == 3 && !pre_due(d, st)) return;
   const int n = d.n, nce = d.ncell;
   box_stage_force<PREC>(v, d, xsm);
   const int ca = b * d.cpb, cb = min(nce, ca + d.cpb);

@@ -78,7 +78,14 @@ typedef struct acg_params {
                                 L = L0 exp(eps) (AdvanceTimeNPTNoseHoover with
                                 U1..U4PropagatorNPT, MDcode/time_evolve.c:654-822); the
                                 barostat state comes from acg_set_barostat; same cell-grid
-                                rule as 4.  Ramps (acg_start_ramp) are refused for 3 and 5 */
+                                rule as 4;
+                             6: active Brownian dynamics, predictor-corrector with random
+                                forces sqrt(2 T^2/dt) N(0,1) minus their mean
+                                (advance_time_ActiveBrown_PC, MDcode/time_evolve.c:855-974,
+                                D0 = 1); the normals come from a counter-based stream
+                                (Philox4x32-10 keyed by `seed`, counter = particle and step)
+                                in place of the reference's GSL draws.
+                             Ramps (acg_start_ramp) are refused for 3, 5 and 6 */
   int shuffle;            /* re-randomise the active directions every tau_p_steps steps
                              (ShuffleActDirec cadence, MDcode/main.c:245-247):
                              1: on the device in the reference's order (per component,

@@ -269,6 +269,8 @@ class Reference(_Common):
             lib.ref_run_nhc_npt.restype = C.c_int
             lib.ref_run_nhc_npt.argtypes = [C.c_int, C.c_double]
             lib.ref_get_npt.argtypes = [_dp]
+            lib.ref_run_brown.restype = C.c_int
+            lib.ref_run_brown.argtypes = [C.c_int, _dp]
             lib.ref_adjust_temp.restype = C.c_double
             lib.ref_adjust_temp.argtypes = [C.c_double]
             lib.ref_coldstart.argtypes = [C.c_double, C.c_double]
@@ -345,6 +347,13 @@ class Reference(_Common):
         self.lib.ref_get_npt(out)
         return {"eps": out[0], "p_eps": out[1], "eta_baro": out[2:5], "p_eta_baro": out[5:8],
                 "eta": out[8:11], "p_eta": out[11:14]}
+
+    def run_brown(self, noise):
+        """advance_time_ActiveBrown_PC once per noise[step] ([steps][N][3]
+        standard normals by particle) in place of the program's draws."""
+        noise = np.ascontiguousarray(noise, dtype=np.float64)
+        if self.lib.ref_run_brown(int(noise.shape[0]), noise.reshape(-1)):
+            raise RuntimeError("this build has no advance_time_ActiveBrown_PC")
 
     def box(self):
         """(L, inv_L, DENSITY) of the program's globals."""

@@ -262,6 +262,40 @@ void ref_get_npt(double *out) {
   }
 }
 
+/* advance_time_ActiveBrown_PC (MDcode/time_evolve.c:855-974) with the
+ * random forces given instead of drawn: the library is linked with
+ * --wrap=normal, so normal() as called from time_evolve.c returns the step's
+ * value for particle InBlock[node][k/3], component k%3 (k = the call count
+ * within the step) from noise[step][particle][3]; without a buffer it draws
+ * as the program does.  The constants are initializeOverDampedBD's
+ * (MDcode/initialise.c:287-291). */
+double __real_normal(double mean, double sigma);
+static const double *noise_buf;
+static long noise_k, noise_step;
+double __wrap_normal(double mean, double sigma) {
+  if (!noise_buf) return __real_normal(mean, sigma);
+  const long k = noise_k++;
+  const int part = InBlock[node][k / 3];
+  return mean + sigma * noise_buf[((size_t)noise_step * N + part) * 3 + k % 3];
+}
+void advance_time_ActiveBrown_PC(void) __attribute__((weak));
+int ref_run_brown(int nsteps, const double *noise) {
+  if (!advance_time_ActiveBrown_PC) return -1;
+  SqrtVariance = sqrt(2.0 * T * T / (time_step * D0));
+  InvD0 = 1.0 / D0;
+  D0ByT = D0 / T;
+  TByD0 = T / D0;
+  expFactor = exp(-time_step * TByD0);
+  noise_buf = noise;
+  for (int s = 0; s < nsteps; s++) {
+    noise_k = 0;
+    noise_step = s;
+    advance_time_ActiveBrown_PC();
+  }
+  noise_buf = NULL;
+  return 0;
+}
+
 /* out: L, inv_L, DENSITY */
 void ref_get_box(double *out) {
   out[0] = L;

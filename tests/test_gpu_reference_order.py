@@ -324,3 +324,41 @@ def test_nose_hoover_npt_matches_reference(cuda_lib, g1000):
     assert np.abs(xu - xur).max() < 1e-9
     assert np.abs(p - pr).max() / np.sqrt((pr ** 2).sum(axis=1).mean()) < 1e-9
     assert abs(th["ke"] - sr["ke"]) < 1e-9 * sr["ke"] and abs(th["pe"] - sr["pe"]) < 1e-9 * abs(sr["pe"])
+
+
+def test_active_brownian_matches_reference(cuda_lib, g1000):
+    """thermostat = 6: the reference's advance_time_ActiveBrown_PC
+    (predictor-corrector with random forces minus their mean) for 30 steps,
+    against the reference program itself fed the engine's random stream
+    (restated on the host in tests/brown_noise.py) in place of its GSL draws."""
+    from brown_noise import normals
+    from oracle import Reference, reference_available
+    if not reference_available(1000):
+        pytest.skip("reference library not built")
+    st = golden_state(g1000)
+    seed, nsteps = 2024, 30
+    ref = Reference(1000)
+    ref.setup(st, 0.45, 1.0)
+    ref.run_brown(np.stack([normals(seed, s, st.n) for s in range(nsteps)]))
+    e = engine_for(st, shuffle=0, drift_every=0, thermostat=6, seed=seed, rebuild_factor=2.5)
+    e.step(10)
+    e.step(nsteps - 10)
+    x, xu, p, F = e.get_state()
+    xr, xur, pr, Fr = ref.get_state()
+    assert np.abs(xu - xur).max() < 1e-9
+    assert np.abs(p - pr).max() / np.sqrt((pr ** 2).sum(axis=1).mean()) < 1e-9
+    th, sr = e.thermo(), ref.scalars()
+    assert abs(th["pe"] - sr["pe"]) < 1e-9 * abs(sr["pe"])
+    assert np.abs(xu - st.xu).max() * st.L > 0.05  # the particles moved
+
+
+def test_active_brownian_graph_equals_eager(cuda_lib, g1000):
+    """The Brownian step in the CUDA graph equals the kernel-by-kernel
+    launches bit for bit (same random stream by particle and step)."""
+    st = golden_state(g1000)
+    a = engine_for(st, shuffle=1, drift_every=11, thermostat=6, seed=5)
+    b = engine_for(st, shuffle=1, drift_every=11, thermostat=6, seed=5)
+    a.step(40)
+    b.step_eager(40)
+    for u, w in zip(a.get_state(), b.get_state()):
+        assert np.array_equal(u, w)
