@@ -35,8 +35,22 @@ constexpr int MAX_UNION = 64;     // 4 x 4 x 4 union cells of a 2 x 2 x 2 group
 constexpr int BLOCK_X = 256;      // threads of the whole-box kernels
 constexpr int BOX_CELLS = 8;      // most cells per whole-box block
 constexpr int LIST_SPLIT = 4;     // blocks sharing a whole-box tile in the list build
+constexpr int BOX_WARP_MAX = 16384;  // whole-box particles up to which lists are built one warp per particle
 constexpr int GSPLIT_MAX = 8;     // most force blocks per cell group (small boxes)
-constexpr int GSPLIT_BLOCKS = 296;  // cell-group force blocks aimed at per system (2 per SM)
+// measured on B200 (FP32, T = 0.45, step latency of one system alone):
+// N = 4505 43-47 us per step on the per-particle kernels against 53 us on
+// split cell groups, N = 11154 54 us against 59 us; N = 30000 68 us either way
+#ifndef ACG_GSPLIT_BLOCKS
+#define ACG_GSPLIT_BLOCKS 296
+#endif
+#ifndef ACG_PARTICLE_MAX
+#define ACG_PARTICLE_MAX 20000
+#endif
+constexpr int GSPLIT_BLOCKS = ACG_GSPLIT_BLOCKS;  // cell-group force blocks aimed at per system (2 per SM)
+// systems of up to this many particles take the per-particle kernels (lists
+// of global slots, no staging, one warp per particle in the list build) even
+// where cell groups would apply
+constexpr int PARTICLE_MAX = ACG_PARTICLE_MAX;
 constexpr int BLOCK_SORT = 1024;   // threads of the per-system sub-cell sort
 constexpr int BLOCK_COMPACT = 1024; // threads of the rebuild-list compaction (one block)
 constexpr int MAX_BOX_NC = 4;     // whole-box mode for 2..4 cells per side
@@ -184,6 +198,7 @@ struct View {
   int *stage_i;     // [2n] type, act
   double *stage_f;  // [3n] forces
   int ntiles_a, ntiles_b, ntiles_l, ntiles_c, ntiles_g, ntiles_x, nsys, maxnb;
+  int box_warp;     // whole-box lists built one warp per particle (few such particles), else per brick
   int gcap;         // staged-particle capacity of a cell group (shared memory)
 };
 

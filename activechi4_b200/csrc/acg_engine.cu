@@ -124,7 +124,7 @@ int plan(const acg_params *params, int nsys, Layout &lay, int nsm) {
     d.coff = lay.ncells;
     d.aoff = lay.nact;
     d.box = d.nc >= 2 && d.nc <= MAX_BOX_NC && d.n <= MAX_BOX_N;
-    d.ng = d.nc >= 3 && !d.box ? (d.nc + 1) / 2 : 0;
+    d.ng = d.nc >= 3 && !d.box && d.n > PARTICLE_MAX ? (d.nc + 1) / 2 : 0;
     d.goff = lay.ngroups;
     lay.ngroups += d.ng * d.ng * d.ng;
     // force blocks per cell group: a small box has few groups, each split over
@@ -980,6 +980,15 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   v.tiles_x = tx;
   v.nsys = nsys;
   v.maxnb = L.maxnb;
+  {
+    // whole-box lists: one warp per particle while the sub-cell systems hold
+    // few particles in all (a lone small system: latency), else one lane per
+    // particle over bricks (a batch: fewer instructions)
+    long long nsub_particles = 0;
+    for (int r = 0; r < nsys; r++)
+      if (L.desc[r].box && L.desc[r].msub >= 5) nsub_particles += L.desc[r].n;
+    v.box_warp = nsub_particles <= BOX_WARP_MAX;
+  }
 
   std::vector<int2> h_a, h_l, h_c, h_g;
   for (int r = 0; r < nsys; r++) {

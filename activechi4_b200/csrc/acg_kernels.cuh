@@ -870,7 +870,7 @@ __device__ __forceinline__ void pair_fp32(PairAcc &a, const double4 &pi, int ti,
 
 // finish one system after its last force block: fixed-order sums, then the
 // thermostat chain (runs in a single block)
-__device__ void finalize_sums(const SysDesc &d, SysState &st, int mode, double pe, double vir, double ke, double va);
+__device__ __noinline__ void finalize_sums(const SysDesc &d, SysState &st, int mode, double pe, double vir, double ke, double va);
 
 __device__ void finalize_system(const View &v, int r, int mode) {
   __shared__ double sh[32];
@@ -904,7 +904,7 @@ __device__ void finalize_system(const View &v, int r, int mode) {
 // (MDcode/time_evolve.c:499-501), a ramp step's rescale to the ramp target
 // (adjustInitialTemp, MDcode/initialise.c:141-151, with inst_T of
 // calculate_temp, :153-164), or none (NVE)
-__device__ void next_first_half(const SysDesc &d, SysState &st, double kb) {
+__device__ __noinline__ void next_first_half(const SysDesc &d, SysState &st, double kb) {
   if (st.ramp_left > 0) {
     const double inst = 2.0 * (kb * 0.5) / d.dof;
     st.s1 = sqrt(st.ramp_T / inst);
@@ -970,7 +970,7 @@ __device__ void next_first_half(const SysDesc &d, SysState &st, double kb) {
   }
 }
 
-__device__ void finalize_sums(const SysDesc &d, SysState &st, int mode, double pe, double vir, double ke, double va) {
+__device__ __noinline__ void finalize_sums(const SysDesc &d, SysState &st, int mode, double pe, double vir, double ke, double va) {
   st.pe = 0.5 * pe;
   st.virial = (0.5 * vir) / 3.0;
   st.vir_act = va;
@@ -1668,6 +1668,18 @@ struct GroupStage {
   int cpre[9];               // centre offset of each centre cell
 };
 
+// the union cell holding staged index q: the last u with pre[u] <= q (pre is a
+// non-decreasing prefix over n cells in shared memory)
+__device__ __forceinline__ int union_of(const int *pre, int n, int q) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (pre[mid] <= q) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
 __device__ void group_prologue(const View &v, const SysDesc &d, const GroupGeom &G, GroupStage &S) {
   const int nc = d.nc;
   const int nux = G.nu[0], nuy = G.nu[1], nuz = G.nu[2];
@@ -1790,12 +1802,18 @@ struct ListWriter {
   }
 };
 
-// one warp per centre cell, one lane per particle of that cell: every lane
-// tests the same staged candidate (a shared-memory broadcast).  Each union
-// cell's staged run is padded to a multiple of four with far-away dummies so
-// the candidate loop reads four entries without bounds tests; the staged .w
-// holds the list code (unpadded staged index | type << 15).  Each lane packs
-// its entries into a 64-bit register and stores whole 4-entry chunks.
+// Lists of a cell group: the neighbour cells in (dz, dy, dx) order, each
+// cell's particles in staged order.  Each union cell's staged run is padded
+// to a multiple of four with far-away dummies; the staged .w holds the list
+// code (unpadded staged index | type << 15).  The last chunk of four entries
+// is padded with the force kernel's far-away slot (index gcap).  The force
+// tiles split a small system's groups into gsplit contiguous runs of centre
+// particles; each run's block stages the union and builds the lists of its
+// run with one warp per particle (the lanes test 32 candidates at a time and
+// a ballot appends the accepted ones: a short chain per particle, for the
+// latency of a few blocks).  An unsplit group (a large system, whose blocks
+// fill the GPU) takes one lane per particle, which issues fewer instructions
+// in all.
 __global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
   extern __shared__ float4 stg[];
   __shared__ GroupStage S;
@@ -1804,15 +1822,14 @@ __global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
   const int r = tile.x;
   if (!v.st[r].rebuild) return;
   const SysDesc &d = v.desc[r];
-  // the force tiles split a group; its list is built by the first of them
-  if (tile.y % d.gsplit) return;
-  const int g = tile.y / d.gsplit;
+  const int g = tile.y / d.gsplit, part = tile.y - g * d.gsplit;
   GroupGeom G;
   group_geom(g, d.nc, d.ng, G);
   group_prologue(v, d, G, S);
   const int Q = S.Q, M = S.M, nux = G.nu[0], nuy = G.nu[1];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int maxnb = v.maxnb;
+  const int run = (M + d.gsplit - 1) / d.gsplit, t_lo = part * run, t_hi = min(M, t_lo + run);
   if (Q <= v.gcap) {
     if (threadIdx.x == 0) {
       int m = 0;
@@ -1824,67 +1841,84 @@ __global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
     }
     __syncthreads();
     const double L = d.L;
-    for (int u = warp; u < S.nU; u += nwarps) {
-      const int q0 = S.upre[u], m = S.upre[u + 1] - q0, j0 = S.ustart[u], p0 = pre4[u];
-      const int m4 = pre4[u + 1] - p0;
-      for (int k = lane; k < m4; k += 32) {
+    // padded staged index q over the whole union, two loads in flight per
+    // thread; each union cell's run is padded to a multiple of four
+    const int P4 = pre4[S.nU];
+    for (int q0 = threadIdx.x; q0 < P4; q0 += 2 * blockDim.x) {
+      double4 p[2];
+      int uu[2], kk[2];
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        const int q = q0 + e * blockDim.x;
+        uu[e] = -1;
+        kk[e] = 0;
+        if (q < P4) {
+          const int u = union_of(pre4, S.nU, q);
+          const int k = q - pre4[u];
+          uu[e] = u;
+          kk[e] = k;
+          if (k < S.upre[u + 1] - S.upre[u]) p[e] = v.pos_s[S.ustart[u] + k];
+        }
+      }
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        const int u = uu[e], k = kk[e], q = q0 + e * blockDim.x;
+        if (u < 0) continue;
         float4 f;
-        if (k < m) {
-          const double4 p = v.pos_s[j0 + k];
-          f.x = (float)staged_coord(S, G, u, 0, p.x, L);
-          f.y = (float)staged_coord(S, G, u, 1, p.y, L);
-          f.z = (float)staged_coord(S, G, u, 2, p.z, L);
-          f.w = __int_as_float((q0 + k) | ((int)p.w << 15));
+        if (k < S.upre[u + 1] - S.upre[u]) {
+          f.x = (float)staged_coord(S, G, u, 0, p[e].x, L);
+          f.y = (float)staged_coord(S, G, u, 1, p[e].y, L);
+          f.z = (float)staged_coord(S, G, u, 2, p[e].z, L);
+          f.w = __int_as_float((S.upre[u] + k) | ((int)p[e].w << 15));
         } else {
           f = make_float4(1e18f, 1e18f, 1e18f, __int_as_float(0));
         }
-        stg[p0 + k] = f;
+        stg[q] = f;
       }
     }
     __syncthreads();
-    float lc[3];
-    for (int k = 0; k < 3; k++) lc[k] = (float)(lcut2_of(d, k) * (1.0 + 1e-5));
-    const bool one_cut = lc[0] == lc[1] && lc[1] == lc[2];
-    uint2 *lst = reinterpret_cast<uint2 *>(group_list(v, d, g));
-    for (int kc = warp; kc < S.nC; kc += nwarps) {
-      const int cu = S.cu[kc];
-      const int m = S.cpre[kc + 1] - S.cpre[kc];
-      const int ux = cu % nux, uy = (cu / nux) % nuy, uz = cu / (nux * nuy);
-      for (int w0 = 0; w0 < m; w0 += 32) {
-        const int w = w0 + lane;
-        const bool valid = w < m;
-        const int t = S.cpre[kc] + w, ps = pre4[cu] + w;
-        const float4 fi = valid ? stg[ps] : make_float4(-1e18f, -1e18f, -1e18f, __int_as_float(0));
+    if (d.gsplit > 1) {
+      float lc[3];
+      for (int k = 0; k < 3; k++) lc[k] = (float)(lcut2_of(d, k) * (1.0 + 1e-5));
+      uint16_t *lst = group_list(v, d, g);
+      const unsigned pad = (unsigned)v.gcap;
+      for (int t = t_lo + warp; t < t_hi; t += nwarps) {
+        int kc, i, qs;
+        group_centre(S, t, kc, i, qs);
+        const int cu = S.cu[kc];
+        const int ux = cu % nux, uy = (cu / nux) % nuy, uz = cu / (nux * nuy);
+        const int ps = pre4[cu] + (t - S.cpre[kc]);
+        const float4 fi = stg[ps];
         const int ti = __float_as_int(fi.w) >> 15;
         // cut for a partner of type 0 / 1 (the sum of the two types indexes lc)
         const float c0 = ti == 0 ? lc[0] : lc[1], c1 = ti == 0 ? lc[1] : lc[2];
-        ListWriter lw;
+        int n = 0;
         for (int dz = -1; dz <= 1; dz++)
           for (int dy = -1; dy <= 1; dy++)
             for (int dx = -1; dx <= 1; dx++) {
               const int u2 = (ux + dx) + (uy + dy) * nux + (uz + dz) * nux * nuy;
               const int q1 = pre4[u2 + 1];
-              for (int q = pre4[u2]; q < q1; q += 4) {
-                int code[4];
-                bool ok[4];
-#pragma unroll
-                for (int e = 0; e < 4; e++) {
-                  const float4 fj = stg[q + e];
+              for (int qb = pre4[u2]; qb < q1; qb += 32) {
+                const int q = qb + lane;
+                bool ok = false;
+                int code = 0;
+                if (q < q1) {
+                  const float4 fj = stg[q];
                   const float ex = fi.x - fj.x, ey = fi.y - fj.y, ez = fi.z - fj.z;
                   const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
-                  code[e] = __float_as_int(fj.w);
-                  const float cut = one_cut ? c0 : ((code[e] >> 15) ? c1 : c0);
-                  ok[e] = valid && r2 < cut && q + e != ps;
+                  code = __float_as_int(fj.w);
+                  ok = r2 < ((code >> 15) ? c1 : c0) && q != ps;
                 }
-#pragma unroll
-                for (int e = 0; e < 4; e++)
-                  if (ok[e]) lw.add((unsigned)code[e] & 0xffffu, lst, M, t, maxnb);
+                const unsigned bal = __ballot_sync(0xffffffffu, ok);
+                if (ok) {
+                  const int k = n + __popc(bal & ((1u << lane) - 1u));
+                  if (k < maxnb) lst[group_entry(k, t, M)] = (uint16_t)(code & 0xffff);
+                }
+                n += __popc(bal);
               }
             }
-        if (valid) {
-          lw.finish(lst, M, t, maxnb, (unsigned)v.gcap);
-          const int n = lw.n;
-          const int i = S.ustart[cu] + w;
+        if (n <= maxnb && lane < ((4 - (n & 3)) & 3)) lst[group_entry(n + lane, t, M)] = (uint16_t)pad;
+        if (lane == 0) {
           if (n > maxnb) {
             v.nbn[i] = -1;
             atomicAdd(&v.st[r].overflow, 1);
@@ -1893,10 +1927,68 @@ __global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
           }
         }
       }
+    } else {
+      // an unsplit group (many groups per system): one warp per centre cell,
+      // one lane per particle, every lane testing the same staged candidate
+      // (a shared-memory broadcast); each lane packs its entries into a 64-bit
+      // register and stores whole 4-entry chunks (the same lists: cells in
+      // (dz, dy, dx) order, staged order inside a cell)
+      float lc[3];
+      for (int k = 0; k < 3; k++) lc[k] = (float)(lcut2_of(d, k) * (1.0 + 1e-5));
+      const bool one_cut = lc[0] == lc[1] && lc[1] == lc[2];
+      uint2 *lst = reinterpret_cast<uint2 *>(group_list(v, d, g));
+      for (int kc = warp; kc < S.nC; kc += nwarps) {
+        const int cu = S.cu[kc];
+        const int m = S.cpre[kc + 1] - S.cpre[kc];
+        const int ux = cu % nux, uy = (cu / nux) % nuy, uz = cu / (nux * nuy);
+        for (int w0 = 0; w0 < m; w0 += 32) {
+          const int w = w0 + lane;
+          const bool valid = w < m;
+          const int t = S.cpre[kc] + w, ps = pre4[cu] + w;
+          const float4 fi = valid ? stg[ps] : make_float4(-1e18f, -1e18f, -1e18f, __int_as_float(0));
+          const int ti = __float_as_int(fi.w) >> 15;
+          // cut for a partner of type 0 / 1 (the sum of the two types indexes lc)
+          const float c0 = ti == 0 ? lc[0] : lc[1], c1 = ti == 0 ? lc[1] : lc[2];
+          ListWriter lw;
+          for (int dz = -1; dz <= 1; dz++)
+            for (int dy = -1; dy <= 1; dy++)
+              for (int dx = -1; dx <= 1; dx++) {
+                const int u2 = (ux + dx) + (uy + dy) * nux + (uz + dz) * nux * nuy;
+                const int q1 = pre4[u2 + 1];
+                for (int q = pre4[u2]; q < q1; q += 4) {
+                  int code[4];
+                  bool ok[4];
+#pragma unroll
+                  for (int e = 0; e < 4; e++) {
+                    const float4 fj = stg[q + e];
+                    const float ex = fi.x - fj.x, ey = fi.y - fj.y, ez = fi.z - fj.z;
+                    const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+                    code[e] = __float_as_int(fj.w);
+                    const float cut = one_cut ? c0 : ((code[e] >> 15) ? c1 : c0);
+                    ok[e] = valid && r2 < cut && q + e != ps;
+                  }
+#pragma unroll
+                  for (int e = 0; e < 4; e++)
+                    if (ok[e]) lw.add((unsigned)code[e] & 0xffffu, lst, M, t, maxnb);
+                }
+              }
+          if (valid) {
+            lw.finish(lst, M, t, maxnb, (unsigned)v.gcap);
+            const int n = lw.n;
+            const int i = S.ustart[cu] + w;
+            if (n > maxnb) {
+              v.nbn[i] = -1;
+              atomicAdd(&v.st[r].overflow, 1);
+            } else {
+              v.nbn[i] = n;
+            }
+          }
+        }
+      }
     }
   } else {
     // the union does not fit in shared memory: the force kernel scans cells
-    for (int t = threadIdx.x; t < M; t += blockDim.x) {
+    for (int t = t_lo + threadIdx.x; t < t_hi; t += blockDim.x) {
       int kc, i, qs;
       group_centre(S, t, kc, i, qs);
       v.nbn[i] = -1;
@@ -1904,7 +1996,7 @@ __global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
     }
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < M; t += blockDim.x) {
+  for (int t = t_lo + threadIdx.x; t < t_hi; t += blockDim.x) {
     int kc, i, qs;
     group_centre(S, t, kc, i, qs);
     copy_back(v, i);
@@ -2062,31 +2154,31 @@ __device__ __forceinline__ void particle_epilogue(const View &v, const SysDesc &
   v.fy[i] = fy;
   v.fz[i] = fz;
   if (mode < 2) {
-    const double vx0 = v.vx[i], vy0 = v.vy[i], vz0 = v.vz[i];
-    double px = vx0, py = vy0, pz = vz0;
-    if (mode == 0 && d.thermostat == 5 && st.ramp_left == 0) {
-      // Nose-Hoover NPT second half kick p f1 + f2 F dt/2 (U2PropagatorNPT)
-      const double f1 = st.u2[0], f2 = st.u2[1];
-      px = __dadd_rn(__dmul_rn(vx0, f1), __dmul_rn(__dmul_rn(f2, fx), d.half_dt));
-      py = __dadd_rn(__dmul_rn(vy0, f1), __dmul_rn(__dmul_rn(f2, fy), d.half_dt));
-      pz = __dadd_rn(__dmul_rn(vz0, f1), __dmul_rn(__dmul_rn(f2, fz), d.half_dt));
-    } else if (mode == 0 && d.thermostat != 3 && !(d.thermostat == 6 && st.ramp_left == 0)) {
-      px = __dadd_rn(vx0, __dmul_rn(fx, d.half_dt));
-      py = __dadd_rn(vy0, __dmul_rn(fy, d.half_dt));
-      pz = __dadd_rn(vz0, __dmul_rn(fz, d.half_dt));
-    } else if (mode != 0) {
-      const double s2 = st.s2;
-      px = __dmul_rn(vx0, s2);
-      py = __dmul_rn(vy0, s2);
-      pz = __dmul_rn(vz0, s2);
+    // p = a v + b F: the second half kick U2 (a = 1, b = dt/2,
+    // MDcode/time_evolve.c:558-567), U2PropagatorNPT (a = f1, b = f2 dt/2,
+    // :721-735), none (Gaussian isokinetic: after k_gauss_sum; Brownian), or
+    // the pending thermostat scale (mode 1: a = s2, b = 0)
+    // (the force term is left out where b = 0, so a non-finite force of a
+    // system that holds no state yet does not reach its momenta)
+    double a = 1.0, b = d.half_dt;
+    if (mode == 1) {
+      a = st.s2;
+      b = 0.0;
+    } else if (d.thermostat == 3 || d.thermostat == 6) {
+      b = 0.0;
+    } else if (d.thermostat == 5 && st.ramp_left == 0) {
+      a = st.u2[0];
+      b = st.u2[1] * d.half_dt;
     }
-    // (Gaussian isokinetic step: the second half kick waits for k_gauss_sum;
-    // active Brownian step: no kick after the forces)
-    if (mode != 0 || (d.thermostat != 3 && !(d.thermostat == 6 && st.ramp_left == 0))) {
-      v.vx[i] = px;
-      v.vy[i] = py;
-      v.vz[i] = pz;
+    double px = __dmul_rn(v.vx[i], a), py = __dmul_rn(v.vy[i], a), pz = __dmul_rn(v.vz[i], a);
+    if (b != 0.0) {
+      px = __dadd_rn(px, __dmul_rn(fx, b));
+      py = __dadd_rn(py, __dmul_rn(fy, b));
+      pz = __dadd_rn(pz, __dmul_rn(fz, b));
     }
+    v.vx[i] = px;
+    v.vy[i] = py;
+    v.vz[i] = pz;
     ke += px * px + py * py + pz * pz;
   }
   pe += a.pe;
@@ -2156,23 +2248,36 @@ __global__ void __launch_bounds__(BLOCK_G, PREC ? ACG_FORCE_MINB32 : ACG_FORCE_M
         slo[v.gcap] = make_float2(0.0f, 0.0f);
       }
     }
-    // one warp per union cell: coalesced loads, no search
-    const int wl = threadIdx.x & 31, nw = blockDim.x >> 5;
-    for (int u = threadIdx.x >> 5; u < S.nU; u += nw) {
-      const int q0 = S.upre[u], m = S.upre[u + 1] - q0, j0 = S.ustart[u];
-      for (int k = wl; k < m; k += 32) {
-        const double4 p = v.pos[j0 + k];
-        const double cx = staged_coord(S, G, u, 0, p.x, L);
-        const double cy = staged_coord(S, G, u, 1, p.y, L);
-        const double cz = staged_coord(S, G, u, 2, p.z, L);
+    // staged index q over the whole union, two loads in flight per thread
+    // (the union's cells are runs of consecutive slots)
+    for (int q0 = threadIdx.x; q0 < Q; q0 += 2 * blockDim.x) {
+      double4 p[2];
+      int uu[2];
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        const int q = q0 + e * blockDim.x;
+        uu[e] = -1;
+        if (q < Q) {
+          const int u = union_of(S.upre, S.nU, q);
+          uu[e] = u;
+          p[e] = v.pos[S.ustart[u] + (q - S.upre[u])];
+        }
+      }
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        const int u = uu[e], q = q0 + e * blockDim.x;
+        if (u < 0) continue;
+        const double cx = staged_coord(S, G, u, 0, p[e].x, L);
+        const double cy = staged_coord(S, G, u, 1, p[e].y, L);
+        const double cz = staged_coord(S, G, u, 2, p[e].z, L);
         if (PREC == 0) {
-          sx[q0 + k] = cx;
-          sy[q0 + k] = cy;
-          sz[q0 + k] = cz;
+          sx[q] = cx;
+          sy[q] = cy;
+          sz[q] = cz;
         } else {
           const float hx = (float)cx, hy = (float)cy, hz = (float)cz;
-          shi[q0 + k] = make_float4(hx, hy, hz, (float)(cx - (double)hx));
-          slo[q0 + k] = make_float2((float)(cy - (double)hy), (float)(cz - (double)hz));
+          shi[q] = make_float4(hx, hy, hz, (float)(cx - (double)hx));
+          slo[q] = make_float2((float)(cy - (double)hy), (float)(cz - (double)hz));
         }
       }
     }
@@ -2538,8 +2643,8 @@ __device__ __forceinline__ void box_list_group(const View &v, const SysDesc &d, 
 // the 27 reference cells of a small box.
 //
 // k_sort_sub puts each rebuilding system in sub-cell order (in memory); the
-// warps of the list blocks take bricks of 2 x 2 x d.bz sub-cells, one lane per
-// particle, and scan the union of the brick's neighbourhoods.
+// warps of the list blocks take one particle each (engines with few such
+// particles) or bricks of 2 x 2 x d.bz sub-cells, one lane per particle.
 __device__ __forceinline__ int subcell_of(double x, int m) { return min(max((int)(x * (double)m), 0), m - 1); }
 
 // lists of the particles of brick B (2 x 2 x d.bz sub-cells), one lane per
@@ -2639,6 +2744,89 @@ __device__ __forceinline__ void box_list_brick(const View &v, const SysDesc &d, 
   }
 }
 
+// One warp per particle of a whole-box system with list sub-cells: the
+// particle at position ps of the sub-cell order scans the sub-cells within two
+// of its own (5 x 5 x 5 with m >= 5 per side: each once), rows in (z, y)
+// order and each row's x range in increasing unwrapped x (periodic images
+// split it into runs), 32 candidates per ballot; the accepted ones are
+// appended in that order.  List entries are system-local slots | type << 15,
+// in 4-entry chunks at uint2 index chunk * n + slot.
+__device__ __forceinline__ void box_list_particle(const View &v, const SysDesc &d, int r, const float4 *xs,
+                                                  const int *sst, int ps, int lane) {
+  const int m = d.msub, n = d.n;
+  // the particle's sub-cell: the last c with sst[c] <= ps
+  int lo = 0, hi = m * m * m - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (sst[mid] <= ps) lo = mid;
+    else hi = mid - 1;
+  }
+  const int sx = lo % m, sy = (lo / m) % m, sz = lo / (m * m);
+  const double iL2 = 1.0 / (d.L * d.L);
+  float lc[3];
+  for (int k = 0; k < 3; k++) lc[k] = (float)(lcut2_of(d, k) * iL2 * (1.0 + 1e-5));
+  uint16_t *lst = reinterpret_cast<uint16_t *>(box_list(v, d));
+  const int maxnb = v.maxnb;
+  const float4 fi = xs[ps];
+  const int codei = __float_as_int(fi.w);
+  const int sl = codei & 0x7fff, ti = codei >> 15;
+  const float c0 = ti == 0 ? lc[0] : lc[1], c1 = ti == 0 ? lc[1] : lc[2];
+  int cnt = 0;
+  auto run = [&](int q0, int q1, float xi, float yi, float zi) {
+    for (int qb = q0; qb < q1; qb += 32) {
+      const int q = qb + lane;
+      bool ok = false;
+      int code = 0;
+      if (q < q1) {
+        const float4 fj = __ldg(xs + q);
+        const float ex = xi - fj.x, ey = yi - fj.y, ez = zi - fj.z;
+        const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+        code = __float_as_int(fj.w);
+        ok = r2 < ((code >> 15) ? c1 : c0) && q != ps;
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, ok);
+      if (ok) {
+        const int k = cnt + __popc(bal & ((1u << lane) - 1u));
+        if (k < maxnb) lst[(((size_t)(k >> 2) * n + sl) << 2) + (k & 3)] = (uint16_t)(code & 0xffff);
+      }
+      cnt += __popc(bal);
+    }
+  };
+  for (int zz = sz - 2; zz <= sz + 2; zz++) {
+    const int wz = zz < 0 ? -1 : (zz >= m ? 1 : 0), az = zz - wz * m;
+    for (int yy = sy - 2; yy <= sy + 2; yy++) {
+      const int wy = yy < 0 ? -1 : (yy >= m ? 1 : 0), ay = yy - wy * m;
+      const int row = m * (ay + m * az);
+      // candidate image x_j + w: compare x_i - w with x_j
+      const float yi = fi.y - (float)wy, zi = fi.z - (float)wz;
+      int xa = sx - 2;
+      const int xb = sx + 3;
+      if (xa < 0) {
+        run(sst[row + m + xa], sst[row + m], fi.x + 1.0f, yi, zi);
+        xa = 0;
+      }
+      if (xb > m) {
+        run(sst[row + xa], sst[row + m], fi.x, yi, zi);
+        run(sst[row], sst[row + xb - m], fi.x - 1.0f, yi, zi);
+      } else {
+        run(sst[row + xa], sst[row + xb], fi.x, yi, zi);
+      }
+    }
+  }
+  // the rest of the last chunk written as 0 (the force loop stops at the count)
+  if (cnt <= maxnb && lane < ((4 - (cnt & 3)) & 3))
+    lst[(((size_t)((cnt + lane) >> 2) * n + sl) << 2) + ((cnt + lane) & 3)] = 0;
+  if (lane == 0) {
+    const int i = d.poff + sl;
+    if (cnt > maxnb) {
+      v.nbn[i] = -1;
+      atomicAdd(&v.st[r].overflow, 1);
+    } else {
+      v.nbn[i] = cnt;
+    }
+  }
+}
+
 // one block per whole-box system with list sub-cells (rebuilding systems
 // only): the system in sub-cell order into xsub (reduced x, y, z as float, the
 // list code slot | type << 15) with the sub-cell starts in ssub.  A counting
@@ -2711,6 +2899,7 @@ __global__ void __launch_bounds__(BLOCK_SORT) k_sort_sub(View v) {
   for (int k = threadIdx.x; k <= M3; k += blockDim.x) gst[k] = sst[k];
 }
 
+
 // list bricks of a whole-box system with list sub-cells
 __device__ __forceinline__ int bricks_of(const SysDesc &d) {
   const int nbx = (d.msub + 1) >> 1;
@@ -2718,9 +2907,9 @@ __device__ __forceinline__ int bricks_of(const SysDesc &d) {
 }
 
 // one block: the whole-box systems with list sub-cells that rebuild this step,
-// in system order, with the running count of their bricks, so the list build
-// can spread all their bricks evenly over its warps: rbs[0] systems, rbs[1]
-// bricks, then (system, first brick) pairs
+// in system order, with the running count of their work items (particles
+// with box_warp, else bricks), so the list build can spread them evenly over
+// its warps: rbs[0] systems, rbs[1] items, then (system, first item) pairs
 __global__ void __launch_bounds__(BLOCK_COMPACT) k_rebuild_compact(View v) {
   __shared__ int wk[32], wb[32];
   __shared__ int base_k, base_b;
@@ -2734,7 +2923,7 @@ __global__ void __launch_bounds__(BLOCK_COMPACT) k_rebuild_compact(View v) {
       const SysDesc &d = v.desc[r];
       if (v.st[r].rebuild && d.box && d.msub >= 5) {
         f = 1;
-        nb = bricks_of(d);
+        nb = v.box_warp ? d.n : bricks_of(d);
       }
     }
     // block-wide exclusive scans of the flags and brick counts
@@ -2812,8 +3001,10 @@ __global__ void __launch_bounds__(BLOCK_X) k_build_list_box(View v) {
     const int stride = LIST_SPLIT * blockDim.x;
     for (int sl = cst[ca] + part * blockDim.x + threadIdx.x; sl < cst[cb]; sl += stride) copy_back(v, d.poff + sl);
   }
-  // the bricks of all rebuilding systems with list sub-cells, spread over the
-  // warps of the whole grid: global warp w takes bricks w, w + W, ...
+  // the work items of all rebuilding systems with list sub-cells, spread over
+  // the warps of the whole grid: global warp w takes items w, w + W, ...
+  // (one particle each for few particles in all, else a brick each: per
+  // particle the chains are shorter, per brick the instructions fewer)
   const int K = v.rbs[0], T = v.rbs[1], Wg = gridDim.x * nw;
   for (int it = blockIdx.x * nw + warp; it < T; it += Wg) {
     int lo = 0, hi = K - 1;  // the last system whose first brick is <= it
@@ -2824,7 +3015,10 @@ __global__ void __launch_bounds__(BLOCK_X) k_build_list_box(View v) {
     }
     const int rs = v.rbs[2 + 2 * lo];
     const SysDesc &ds = v.desc[rs];
-    box_list_brick(v, ds, rs, v.xsub + ds.poff, v.ssub + ds.soff, it - v.rbs[3 + 2 * lo], lane);
+    if (v.box_warp)
+      box_list_particle(v, ds, rs, v.xsub + ds.poff, v.ssub + ds.soff, it - v.rbs[3 + 2 * lo], lane);
+    else
+      box_list_brick(v, ds, rs, v.xsub + ds.poff, v.ssub + ds.soff, it - v.rbs[3 + 2 * lo], lane);
   }
 }
 
@@ -2946,7 +3140,7 @@ __device__ __forceinline__ PairAcc box_pairs(const View &v, const SysDesc &d, co
 // reduced coordinates, separation = wrapped integer difference x L/2^32 (one
 // rounding); FP64: staged reduced coordinates, minimum image d - rint(d).
 template <int TPP, int PREC>
-__global__ void __launch_bounds__(BLOCK_X) k_force_box(View v, int mode) {
+__global__ void __launch_bounds__(BLOCK_X, 4) k_force_box(View v, int mode) {
   extern __shared__ __align__(16) unsigned char xsm[];
   const int2 tile = v.tiles_x[blockIdx.x];
   const int r = tile.x, b = tile.y;

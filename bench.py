@@ -197,7 +197,10 @@ def make_engine(n, precision, seed, device, equil):
     from activechi4_b200 import Engine, default_params
     from activechi4_b200.init import lattice_state
     prec = 1 if precision == "fp32" else 0
-    p = default_params(n, T=2.0, f0=1.0, tau_p_steps=200, precision=prec, seed=seed)
+    # per-type list cut 2.5 sigma_ab + skin (list_mode 1): the same pairs
+    # interact as with the reference's one cut of 2.85 for all pairs (both are
+    # parity-tested), with ~25% fewer list entries to test
+    p = default_params(n, T=2.0, f0=1.0, tau_p_steps=200, precision=prec, seed=seed, list_mode=1)
     e = Engine(p, device=device)
     st = lattice_state(n, 2.0, seed=seed)
     e.set_state(0, st)
@@ -217,7 +220,8 @@ def e2e_run(e, st, nsteps):
     """Through the public C ABI with host buffers: load the state from pinned
     host memory, run nsteps steps in calls of up to 32 steps reading the
     thermodynamic scalars back after every call (the reference prints them at
-    its frame cadence), read the final state back."""
+    its frame cadence), read the final state back.  The graphs are built and
+    launched once before the timed region."""
     import numpy as np
     import torch
     n = st.n
@@ -233,6 +237,12 @@ def e2e_run(e, st, nsteps):
     from activechi4_b200 import _abi
     lib = _abi.lib()
     ptr = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    # the step graphs are built and launched once before the timed region (a
+    # one-time set-up, as for `value`): both copies of the loop graph the
+    # engine alternates between, and the remainder graph
+    e.prepare()
+    for k in (32, 32, 1):
+        e.step(k)
     e.sync()
     ncalls = 0
     t0 = time.perf_counter()
@@ -471,7 +481,8 @@ def run_ours(args):
             "dtype": "f64" if args.precision == "fp64" else "f32-pair/f64-state",
             "data": "synthetic: seeded random lattice melted on the device (T=2.0 then 0.45)",
             "config": {"workload": f"plain KA active glass, N={n} one system, rho=1.2, T=0.45, f0=1.0, "
-                                   f"tau_p=200 steps, dt=0.005, NHC NVT, {args.precision} pair forces",
+                                   f"tau_p=200 steps, dt=0.005, NHC NVT, {args.precision} pair forces, "
+                                   "neighbour lists cut at 2.5 sigma_ab + skin 0.35",
                        "n": n, "systems_per_gpu": 1, "parallelism": f"replicas x{world}",
                        "l2": "256 MiB write before every timed graph launch (cold L2 each launch)"},
             "e2e": {"value": e2e_val, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
