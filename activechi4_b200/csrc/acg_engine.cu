@@ -244,6 +244,10 @@ struct acg_engine {
   int2 *d_tiles_b = nullptr;
   int2 *d_tiles_x = nullptr;
   std::vector<int> dirty;  // systems whose forces/lists must be recomputed
+  // the host's copy of each system's step counter and ramp steps left (the
+  // device's st.step / st.ramp_left), to schedule drift removals between
+  // graph launches
+  std::vector<long long> hstep, hramp;
   bool any_dirty = false;
   bool any_gauss = false;  // a system runs the Gaussian isokinetic integrator (thermostat 3)
   bool any_npt = false;    // a system runs the Berendsen barostat (thermostat 4)
@@ -430,8 +434,9 @@ void drop_graphs(acg_engine *e) {
 // memory) and can be updated in place instead of instantiated anew
 std::string graph_shape(const acg_engine *e, int K) {
   char b[160];
-  snprintf(b, sizeof(b), "K%d g%d x%d b%d l%d p%d t%d/%d/%d/%d", K, e->ntiles_g > 0, e->ntiles_x > 0,
-           e->ntiles_b > 0, e->ntiles_l > 0, e->lay.desc[0].precision, e->tpp, e->gtpp, e->btpp, e->block);
+  snprintf(b, sizeof(b), "K%d g%d x%d b%d l%d p%d t%d/%d/%d/%d i%d%d%d", K, e->ntiles_g > 0, e->ntiles_x > 0,
+           e->ntiles_b > 0, e->ntiles_l > 0, e->lay.desc[0].precision, e->tpp, e->gtpp, e->btpp, e->block,
+           e->any_gauss, e->any_npt, e->any_brown);
   return b;
 }
 
@@ -518,6 +523,58 @@ void launch_gauss(acg_engine *e, bool with_sum) {
   k_gauss_apply<<<e->ntiles_a, BLOCK_A, 0, e->stream>>>(e->v);
 }
 
+// ---- drift removal between graph launches ----------------------------------
+// The step graphs hold no drift removal (fixDrift after every drift_every-th
+// step, MDcode/main.c:261): the host keeps a copy of each system's step
+// counter and ramp steps left, launches graphs up to a step after which a
+// removal is due, then the removal kernels (they act on the systems whose
+// kick flagged st.drift), then the rest.
+// Steps from now up to and including the first one after which some system
+// removes its drift (step index % drift_every == 0, not a ramp step); 0 =
+// none within `limit`.
+long long steps_to_drift(const Layout &lay, const std::vector<long long> &hstep,
+                         const std::vector<long long> &hramp, long long limit) {
+  long long best = 0;
+  for (int r = 0; r < lay.nsys; r++) {
+    const long long de = lay.desc[r].drift_every;
+    if (de <= 0) continue;
+    const long long s0 = hstep[r];
+    const long long off = hramp[r] + ((s0 + de - 1) / de * de - s0);
+    if (off < limit && (best == 0 || off + 1 < best)) best = off + 1;
+  }
+  return best;
+}
+
+void advance_steps(std::vector<long long> &hstep, std::vector<long long> &hramp, long long k) {
+  for (size_t r = 0; r < hstep.size(); r++) {
+    const long long ramp = std::min(hramp[r], k);
+    hramp[r] -= ramp;
+    hstep[r] += k - ramp;
+  }
+}
+
+// k steps cut where drift removals are due: (steps, removal after them)
+std::vector<std::pair<long long, bool>> drift_pieces(const acg_engine *e, std::vector<long long> &hstep,
+                                                     std::vector<long long> &hramp, long long k) {
+  std::vector<std::pair<long long, bool>> out;
+  while (k > 0) {
+    const long long m = steps_to_drift(e->lay, hstep, hramp, k);
+    const long long n = m ? m : k;
+    out.push_back({n, m != 0});
+    advance_steps(hstep, hramp, n);
+    k -= n;
+  }
+  return out;
+}
+
+int launch_drift(acg_engine *e) {
+  k_drift_sum<<<e->ntiles_a, BLOCK_A, 0, e->stream>>>(e->v);
+  k_drift_apply<<<e->ntiles_a, BLOCK_A, 0, e->stream>>>(e->v);
+  launch_gauss(e, false);
+  CK(cudaGetLastError());
+  return ACG_OK;
+}
+
 // before the kick: the Berendsen barostat's box update and the Brownian
 // random forces and predictor, then the forces of those systems (mode 3)
 int launch_pre(acg_engine *e) {
@@ -534,7 +591,7 @@ int launch_pre(acg_engine *e) {
 int launch_step_eager(acg_engine *e) {
   int rc0 = launch_pre(e);
   if (rc0) return rc0;
-  k_kick_drift<<<e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, 0, e->stream>>>(e->v, 0, 0, 0);
+  k_kick_drift<<<e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, 0, e->stream>>>(e->v, 0, 0);
   k_shuffle_ref<<<3 * e->lay.nsys, BLOCK_SHUF, shuffle_smem(e->lay), e->stream>>>(e->v, -1);
   CK(cudaGetLastError());
   int rc = launch_rebuild(e);
@@ -595,13 +652,12 @@ int add_steps(acg_engine *e, cudaGraph_t g, int K, cudaGraphNode_t *prev_io) {
   GroupFn xf = box_fn(e->btpp, prec);
   int mode0 = 0, use_cond = 1, tbase = e->ntiles_g + e->ntiles_x;
   for (int s = 0; s < K; s++) {
-    // per step: kick/drift, then one device-decided switch (the list rebuild,
-    // the reference-order direction shuffle, both side by side, or nothing),
-    // the force kernels, and one device-decided branch after them (drift
-    // removal, observables)
-    cudaGraphConditionalHandle h, ho;
-    CK(cudaGraphConditionalHandleCreate(&h, g, 3, cudaGraphCondAssignDefault));
-    CK(cudaGraphConditionalHandleCreate(&ho, g, 0, cudaGraphCondAssignDefault));
+    // per step: kick/drift, then one device-decided switch (any of the list
+    // rebuild, the reference-order direction shuffle and the observable
+    // events, or nothing), the force kernels (drift removals are launched by
+    // the host between graphs)
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, g, 7, cudaGraphCondAssignDefault));
     cudaGraphNode_t na, nc, nb;
     int rc;
     if (e->any_npt || e->any_brown) {
@@ -642,7 +698,7 @@ int add_steps(acg_engine *e, cudaGraph_t g, int K, cudaGraphNode_t *prev_io) {
         prev = nb;
       }
     }
-    void *aa[] = {&v, &use_cond, &h, &ho};
+    void *aa[] = {&v, &use_cond, &h};
     rc = add_kernel(g, prev ? &prev : nullptr, prev ? 1 : 0, &na, (void *)k_kick_drift,
                     e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, aa);
     if (rc) return rc;
@@ -650,7 +706,7 @@ int add_steps(acg_engine *e, cudaGraph_t g, int K, cudaGraphNode_t *prev_io) {
     cp.type = cudaGraphNodeTypeConditional;
     cp.conditional.handle = h;
     cp.conditional.type = cudaGraphCondTypeSwitch;
-    cp.conditional.size = 3;
+    cp.conditional.size = 7;
     CK(cudaGraphAddNode(&nc, g, &na, 1, &cp));
     void *va[] = {&v};
     struct {
@@ -670,10 +726,11 @@ int add_steps(acg_engine *e, cudaGraph_t g, int K, cudaGraphNode_t *prev_io) {
               {(void *)k_build_list, e->ntiles_l, BLOCK_L, 0}};
     int all = -1;
     void *sa[] = {&v, &all};
-    for (int c = 0; c < 3; c++) {
+    for (int c = 0; c < 7; c++) {
+      const int bits = c + 1;
       cudaGraph_t body = cp.conditional.phGraph_out[c];
-      if (c != 1) {  // the rebuild chain
-        cudaGraphNode_t bp = nullptr;
+      cudaGraphNode_t bp = nullptr;
+      if (bits & 1) {  // the rebuild chain
         for (auto &k : rb) {
           if (k.grid == 0) continue;
           cudaGraphNode_t nn;
@@ -682,10 +739,15 @@ int add_steps(acg_engine *e, cudaGraph_t g, int K, cudaGraphNode_t *prev_io) {
           bp = nn;
         }
       }
-      if (c != 0) {  // the shuffle, independent of the rebuild chain
+      if (bits & 2) {  // the shuffle, independent of the rebuild chain
         cudaGraphNode_t nk;
         rc = add_kernel(body, nullptr, 0, &nk, (void *)k_shuffle_ref, 3 * e->lay.nsys, BLOCK_SHUF, sa,
                         shuffle_smem(e->lay));
+        if (rc) return rc;
+      }
+      if (bits & 4) {  // observables, after the rebuild chain (which reorders the slots)
+        cudaGraphNode_t nk;
+        rc = add_kernel(body, bp ? &bp : nullptr, bp ? 1 : 0, &nk, (void *)k_observe, e->ntiles_a, BLOCK_A, va);
         if (rc) return rc;
       }
     }
@@ -726,29 +788,7 @@ int add_steps(acg_engine *e, cudaGraph_t g, int K, cudaGraphNode_t *prev_io) {
       if (rc) return rc;
       last = nb;
     }
-    // after the step: drift removal and observables at the scheduled steps
-    // (device-decided, like the rebuild)
-    cudaGraphNodeParams op = {};
-    op.type = cudaGraphNodeTypeConditional;
-    op.conditional.handle = ho;
-    op.conditional.type = cudaGraphCondTypeIf;
-    op.conditional.size = 1;
-    cudaGraphNode_t no, nk0, nk1, nk2;
-    CK(cudaGraphAddNode(&no, g, dep, ndep, &op));
-    cudaGraph_t ob = op.conditional.phGraph_out[0];
-    rc = add_kernel(ob, nullptr, 0, &nk0, (void *)k_drift_sum, e->ntiles_a, BLOCK_A, va);
-    if (rc) return rc;
-    rc = add_kernel(ob, &nk0, 1, &nk1, (void *)k_drift_apply, e->ntiles_a, BLOCK_A, va);
-    if (rc) return rc;
-    if (e->any_gauss) {  // the first half after a drift removal
-      cudaGraphNode_t nkg;
-      rc = add_kernel(ob, &nk1, 1, &nkg, (void *)k_gauss_apply, e->ntiles_a, BLOCK_A, va);
-      if (rc) return rc;
-      nk1 = nkg;
-    }
-    rc = add_kernel(ob, &nk1, 1, &nk2, (void *)k_observe, e->ntiles_a, BLOCK_A, va);
-    if (rc) return rc;
-    prev = no;
+    prev = last;
   }
   *prev_io = prev;
   return ACG_OK;
@@ -1099,6 +1139,8 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   rc = build_tiles_b(e);
   if (rc) return cleanup_fail(rc);
   e->dirty.assign(nsys, 1);
+  e->hstep.assign(nsys, 0);
+  e->hramp.assign(nsys, 0);
   e->obs_bufs.assign(nsys, {});
   e->obs_offsets.assign(nsys, {});
   e->obs_events.assign(nsys, {});
@@ -1197,6 +1239,7 @@ int acg_set_state(acg_engine *e, int sys, const double *x, const double *xu, con
   CK(cudaMemcpyAsync(&e->v.st[sys].s2, &one, sizeof(double), cudaMemcpyHostToDevice, e->stream));
   CK(cudaMemcpyAsync(&e->v.st[sys].ramp_left, &zero_ll, sizeof(long long), cudaMemcpyHostToDevice, e->stream));
   CK(cudaStreamSynchronize(e->stream));  // host buffers may be freed on return
+  e->hramp[sys] = 0;
   e->dirty[sys] = 1;
   e->any_dirty = true;
   return ACG_OK;
@@ -1349,6 +1392,7 @@ int acg_start_ramp(acg_engine *e, int sys, double T_start, double T_end, double 
   rc = launch_rebuild(e);
   if (rc) return rc;
   k_ramp_begin<<<1, 32, 0, e->stream>>>(e->v, sys, T0, heat ? dT : -dT, T_end, K);
+  e->hramp[sys] = K;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(e->stream));
   if (steps) *steps = K;
@@ -1360,6 +1404,7 @@ int acg_extend_ramp(acg_engine *e, int sys, int64_t total_steps) {
   if (rc) return rc;
   CK(cudaSetDevice(e->device));
   k_ramp_extend<<<1, 32, 0, e->stream>>>(e->v, sys, (long long)total_steps);
+  if (e->hramp[sys] > 0 && (long long)total_steps > e->hramp[sys]) e->hramp[sys] = total_steps;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(e->stream));
   return ACG_OK;
@@ -1400,6 +1445,7 @@ int acg_set_lattice(acg_engine *e, int sys, const int *site, const int *type, co
   CK(cudaMemcpyAsync(&e->v.st[sys].s2, &one, sizeof(double), cudaMemcpyHostToDevice, e->stream));
   CK(cudaMemcpyAsync(&e->v.st[sys].ramp_left, &zero_ll, sizeof(long long), cudaMemcpyHostToDevice, e->stream));
   CK(cudaStreamSynchronize(e->stream));
+  e->hramp[sys] = 0;
   e->dirty[sys] = 1;
   e->any_dirty = true;
   return ACG_OK;
@@ -1494,12 +1540,9 @@ int acg_compute_forces(acg_engine *e) {
   return ACG_OK;
 }
 
-int acg_step(acg_engine *e, int nsteps) {
-  if (!e) return fail(ACG_ERR_INVALID, "null engine");
-  if (nsteps < 0) return fail(ACG_ERR_INVALID, "nsteps < 0");
-  CK(cudaSetDevice(e->device));
-  int rc = prime(e);
-  if (rc) return rc;
+// nsteps steps in graph launches (no drift removal due inside them)
+int step_graphs(acg_engine *e, int nsteps) {
+  int rc;
   if (!e->no_while) {
     // device loop: one launch for the GRAPH_STEPS-step blocks, one for the rest
     const long long q = nsteps / GRAPH_STEPS, r = nsteps % GRAPH_STEPS;
@@ -1541,6 +1584,23 @@ int acg_step(acg_engine *e, int nsteps) {
   return ACG_OK;
 }
 
+int acg_step(acg_engine *e, int nsteps) {
+  if (!e) return fail(ACG_ERR_INVALID, "null engine");
+  if (nsteps < 0) return fail(ACG_ERR_INVALID, "nsteps < 0");
+  CK(cudaSetDevice(e->device));
+  int rc = prime(e);
+  if (rc) return rc;
+  for (const auto &pc : drift_pieces(e, e->hstep, e->hramp, nsteps)) {
+    rc = step_graphs(e, (int)pc.first);
+    if (rc) return rc;
+    if (pc.second) {
+      rc = launch_drift(e);
+      if (rc) return rc;
+    }
+  }
+  return ACG_OK;
+}
+
 int acg_prepare(acg_engine *e) {
   if (!e) return fail(ACG_ERR_INVALID, "null engine");
   CK(cudaSetDevice(e->device));
@@ -1560,9 +1620,10 @@ int acg_step_eager(acg_engine *e, int nsteps) {
   int rc = prime(e);
   if (rc) return rc;
   for (int s = 0; s < nsteps; s++) {
-    rc = launch_step_eager(e);
+    rc = launch_step_eager(e);  // its drift kernels act on the kick's st.drift flags
     if (rc) return rc;
   }
+  advance_steps(e->hstep, e->hramp, nsteps);
   return ACG_OK;
 }
 
@@ -1738,7 +1799,7 @@ int acg_time_stage(acg_engine *e, int stage, int reps, double *ms) {
   CK(cudaEventRecord(a, e->stream));
   for (int i = 0; i < reps; i++) {
     if (stage == 0) {
-      k_kick_drift<<<e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, 0, e->stream>>>(e->v, 0, 0, 0);
+      k_kick_drift<<<e->ntiles_a + 3 * e->lay.nsys, BLOCK_A, 0, e->stream>>>(e->v, 0, 0);
     } else if (stage == 1) {
       rc = launch_force(e, 2);
     } else {
@@ -1899,14 +1960,23 @@ int acg_bench_steps(acg_engine *e, int64_t nsteps, size_t flush_bytes, double *m
     for (int64_t k = 0; k < nsteps / GRAPH_STEPS; k++) plan.push_back(GRAPH_STEPS);
     if (nsteps % GRAPH_STEPS) plan.push_back((int)(nsteps % GRAPH_STEPS));
   }
-  for (int K : plan) {
-    if (e->bench.count(K)) continue;
-    cudaGraph_t g;
-    cudaGraphExec_t x;
-    rc = build_graph(e, K, &g, &x);
-    if (rc) return rc;
-    e->bench[K] = {g, x};
+  // each timed region in pieces cut where drift removals are due (launched
+  // between the pieces, inside the region)
+  std::vector<std::vector<std::pair<long long, bool>>> pieces;
+  {
+    std::vector<long long> hs = e->hstep, hr = e->hramp;
+    for (int K : plan) pieces.push_back(drift_pieces(e, hs, hr, K));
   }
+  for (const auto &reg : pieces)
+    for (const auto &pc : reg) {
+      const int K = (int)pc.first;
+      if (e->bench.count(K)) continue;
+      cudaGraph_t g;
+      cudaGraphExec_t x;
+      rc = build_graph(e, K, &g, &x);
+      if (rc) return rc;
+      e->bench[K] = {g, x};
+    }
   if (flush_bytes > e->flush_bytes) {
     if (e->flush) cudaFree(e->flush);
     e->flush = nullptr;
@@ -1917,15 +1987,28 @@ int acg_bench_steps(acg_engine *e, int64_t nsteps, size_t flush_bytes, double *m
   const int nsys = e->lay.nsys;
   std::vector<SysState> st0(nsys), st1(nsys);
   CK(cudaMemcpyAsync(st0.data(), e->v.st, sizeof(SysState) * nsys, cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  for (int r = 0; r < nsys; r++)
+    if (st0[r].step != e->hstep[r] || st0[r].ramp_left != e->hramp[r])
+      return fail(ACG_ERR_STATE, "system " + std::to_string(r) + ": the host's step counter disagrees with the device's");
   const size_t nl = plan.size();
   std::vector<cudaEvent_t> ev(2 * nl);
   for (auto &x : ev) CK(cudaEventCreate(&x));
+  long long ndrift = 0;
   for (size_t c = 0; c < nl; c++) {
     if (flush_bytes) CK(cudaMemsetAsync(e->flush, (int)(c & 0xff), flush_bytes, e->stream));
     CK(cudaEventRecord(ev[2 * c], e->stream));
-    CK(cudaGraphLaunch(e->bench[plan[c]].second, e->stream));
+    for (const auto &pc : pieces[c]) {
+      CK(cudaGraphLaunch(e->bench[(int)pc.first].second, e->stream));
+      if (pc.second) {
+        rc = launch_drift(e);
+        if (rc) return rc;
+        ndrift++;
+      }
+    }
     CK(cudaEventRecord(ev[2 * c + 1], e->stream));
   }
+  advance_steps(e->hstep, e->hramp, nsteps);
   CK(cudaStreamSynchronize(e->stream));
   double tot = 0;
   for (size_t c = 0; c < nl; c++) {
@@ -1937,35 +2020,34 @@ int acg_bench_steps(acg_engine *e, int64_t nsteps, size_t flush_bytes, double *m
   CK(cudaMemcpy(st1.data(), e->v.st, sizeof(SysState) * nsys, cudaMemcpyDeviceToHost));
   *ms = tot;
   if (!launches) return ACG_OK;
-  // kernels launched in the timed graphs: every step the kick/drift kernel
-  // and each force kernel in use; a step whose rebuild branch is taken the
-  // rebuild kernels with a non-empty grid; a step with a reference-order
-  // shuffle the shuffle kernel; a step with a drift removal or observable
-  // events the three kernels of that branch (the node lists of add_steps);
-  // with a Gaussian isokinetic system two more per step and one more per branch
+  // kernels launched in the timed region: every step the kick/drift kernel
+  // and each force kernel in use; a step whose switch takes the rebuild the
+  // rebuild kernels with a non-empty grid, the shuffle the shuffle kernel,
+  // observable events the observable kernel (the node lists of add_steps);
+  // each drift removal its two kernels (and a Gaussian one).  A Gaussian
+  // isokinetic system adds two kernels per step; the Berendsen barostat the
+  // box update, Brownian dynamics the random forces and the predictor, and
+  // either a second force pass every step.
   const long long nforce = (e->ntiles_g > 0) + (e->ntiles_x > 0) + (e->ntiles_b > 0);
-  // (Berendsen barostat: the box update, Brownian: the random forces and the
-  // predictor, and for either a second force pass every step)
   const long long per_step = 1 + nforce + 2 * e->any_gauss + e->any_npt + 2 * e->any_brown +
                              (e->any_npt || e->any_brown) * nforce;
   const long long per_rebuild = 5 + (e->lay.box_m3max > 0) + 2 * (e->ntiles_x > 0) + (e->ntiles_g > 0) +
                                 (e->ntiles_l > 0);
-  long long steps_with_rebuild = 0, shuffles = 0, posts = 0;
+  long long steps_with_rebuild = 0, shuffles = 0, obs_steps = 0;
   for (int r = 0; r < nsys; r++) steps_with_rebuild = std::max(steps_with_rebuild, st1[r].rebuilds - st0[r].rebuilds);
   for (long long k = 0; k < nsteps; k++) {
-    bool shuf = false, post = false;
-    for (int r = 0; r < nsys && !(shuf && post); r++) {
+    bool shuf = false, obs = false;
+    for (int r = 0; r < nsys && !(shuf && obs); r++) {
       const SysDesc &d = e->lay.desc[r];
       const long long step = st0[r].step + k;
       if (d.shuffle == 1 && d.nact > 0 && d.tau_p > 0 && step % d.tau_p == 0) shuf = true;
-      if (d.drift_every > 0 && step % d.drift_every == 0) post = true;
       const auto &evs = e->obs_events[r];
-      if (!post && std::binary_search(evs.begin(), evs.end(), step)) post = true;
+      if (!obs && std::binary_search(evs.begin(), evs.end(), step)) obs = true;
     }
     shuffles += shuf;
-    posts += post;
+    obs_steps += obs;
   }
-  *launches = per_step * nsteps + per_rebuild * steps_with_rebuild + shuffles + (3 + e->any_gauss) * posts;
+  *launches = per_step * nsteps + per_rebuild * steps_with_rebuild + shuffles + obs_steps + (2 + e->any_gauss) * ndrift;
   return ACG_OK;
 }
 

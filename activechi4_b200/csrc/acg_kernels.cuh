@@ -386,11 +386,13 @@ __device__ __forceinline__ bool shuffle_due(const SysDesc &d, const SysState &st
 }
 
 // stage 1: kick + drift (+ uniform-shuffle blocks) + rebuild decision
-// The last block sets the step's two graph branches: h_pre (a switch before
-// the forces: 0 = list rebuild, 1 = reference-order shuffle, 2 = both, 3 =
-// neither) and h_obs (after the forces: drift removal and observables).
-__global__ void __launch_bounds__(BLOCK_A) k_kick_drift(View v, int use_cond, cudaGraphConditionalHandle h_pre,
-                                                        cudaGraphConditionalHandle h_obs) {
+// The last block sets the step's graph branch h_pre, a switch before the
+// forces over the work due in some system: bit 0 list rebuild, bit 1
+// reference-order shuffle, bit 2 observable events (the positions of the step
+// are final after the drift); value = bits - 1, or 7 for none.  The drift
+// removal after the step (st.drift) is scheduled by the host between graph
+// launches, or run by the kernel-by-kernel step.
+__global__ void __launch_bounds__(BLOCK_A) k_kick_drift(View v, int use_cond, cudaGraphConditionalHandle h_pre) {
   __shared__ double sm[BLOCK_A / 32];
   __shared__ int s_last;
   const int b = blockIdx.x;
@@ -429,7 +431,7 @@ __global__ void __launch_bounds__(BLOCK_A) k_kick_drift(View v, int use_cond, cu
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-  int any = 0, any_post = 0, any_shuf = 0;
+  int any = 0, any_obs = 0, any_shuf = 0;
   for (int s = threadIdx.x; s < v.nsys; s += blockDim.x) {
     const SysDesc &d = v.desc[s];
     SysState &st = v.st[s];
@@ -445,16 +447,16 @@ __global__ void __launch_bounds__(BLOCK_A) k_kick_drift(View v, int use_cond, cu
     } else {
       st.obs_lo = st.obs_hi = 0;
     }
-    any_post |= ob | st.drift;
+    any_obs |= ob;
   }
   any = __syncthreads_or(any);
-  any_post = __syncthreads_or(any_post);
+  any_obs = __syncthreads_or(any_obs);
   any_shuf = __syncthreads_or(any_shuf);
   if (threadIdx.x == 0) {
     *v.counter_a = 0;
     if (use_cond) {
-      cudaGraphSetConditional(h_pre, any ? (any_shuf ? 2u : 0u) : (any_shuf ? 1u : 3u));
-      cudaGraphSetConditional(h_obs, any_post ? 1u : 0u);
+      const unsigned bits = (any ? 1u : 0u) | (any_shuf ? 2u : 0u) | (any_obs ? 4u : 0u);
+      cudaGraphSetConditional(h_pre, bits ? bits - 1u : 7u);
     }
   }
 }
