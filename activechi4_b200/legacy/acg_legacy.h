@@ -34,6 +34,8 @@ acg_engine *acg_legacy_current(void);
 void acg_legacy_push(acg_engine *e);
 /* device -> host sphere[] and the scalar globals of the step */
 void acg_legacy_pull(acg_engine *e);
+/* list rebuilds so far of the engine that holds the state */
+long long acg_legacy_rebuilds(void);
 /* print the library's last error and exit, as the reference does on errors */
 void acg_legacy_die(const char *where, int rc);
 /* refresh sphere[] and the step's globals from the device when it is ahead

@@ -312,7 +312,8 @@ void InitialiseNoseHoover() {
 }
 
 /* one step of the whole system on the device with engine `kind`; sphere[]
- * follows at the next sync point */
+ * and the step's scalars (pe, ke, virial, maxmaxD, the chain) follow at the
+ * next sync point, so a run of steps queues on the device without a wait */
 static void legacy_step(int kind) {
   acg_engine *e = acg_legacy_engine(kind);
   acg_legacy_push(e);
@@ -322,9 +323,17 @@ static void legacy_step(int kind) {
 #ifdef ACG_LEGACY_EAGER
   acg_legacy_pull(e);
 #else
-  pull_scalars(e);
   host_stale = 1;
 #endif
+}
+
+/* list rebuilds of the engine that holds the state (for test harnesses, which
+ * would otherwise read maxmaxD after every step) */
+long long acg_legacy_rebuilds(void) {
+  acg_thermo th;
+  int rc = acg_get_thermo(acg_legacy_current(), 0, &th);
+  if (rc) acg_legacy_die("acg_get_thermo", rc);
+  return (long long)th.rebuilds;
 }
 
 /* AdvanceTimeNVTNoseHoover (MDcode/time_evolve.c:495-526): one NHC step of

@@ -164,6 +164,7 @@ void ref_set_nhc(const double *eta_in, const double *p_eta_in) {
   }
 }
 void ref_get_nhc(double *out) {
+  mirror_read();
   for (int i = 0; i < M; i++) {
     out[i] = eta[i];
     out[M + i] = p_eta[i];
@@ -176,14 +177,20 @@ void ref_get_nhc(double *out) {
  * every 100000th step.  Returns the number of steps that rebuilt the
  * cell/neighbour lists, i.e. took the 3*maxmaxD > skin^2 branch
  * (MDcode/time_evolve.c:508). */
+/* the drop-in build's count of list rebuilds (its step leaves maxmaxD and the
+ * other scalars to the next sync point); weak, absent from the reference build */
+long long acg_legacy_rebuilds(void) __attribute__((weak));
+
 int ref_run(long start, int nsteps, int do_shuffle, int do_drift) {
   int rebuilds = 0;
+  const long long r0 = acg_legacy_rebuilds ? acg_legacy_rebuilds() : 0;
   for (long i = start; i < start + nsteps; i++) {
     if (do_shuffle && !(i % TAU_per)) ShuffleActDirec();
     AdvanceTimeNVTNoseHoover();
-    if (3.0 * maxmaxD > skin * skin) rebuilds++;
+    if (!acg_legacy_rebuilds && 3.0 * maxmaxD > skin * skin) rebuilds++;
     if (do_drift && i % 100000 == 0) fixDrift();
   }
+  if (acg_legacy_rebuilds) rebuilds = (int)(acg_legacy_rebuilds() - r0);
   return rebuilds;
 }
 
@@ -403,6 +410,7 @@ void ref_get_state(double *x, double *xu, double *p, double *F) {
 
 /* out: peblk, ke, virialblk, vir_actblk, inst_T, maxmaxD */
 void ref_get_scalars(double *out) {
+  mirror_read();
   out[0] = peblk;
   out[1] = ke;
   out[2] = virialblk;
