@@ -1508,12 +1508,96 @@ __global__ void k_lattice(View v, int r, int troot) {
   }
 }
 
+// 1/x for x in the pair range (0.3 < x < 7): the hardware estimate
+// (rcp.approx.ftz.f64) refined by two Newton-Raphson steps y += y (1 - x y),
+// each squaring the relative error, to within an ulp of the rounded quotient
+__device__ __forceinline__ double rcp_nr(double x) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  return fma(y, e, y);
+}
+
+// 1/x in FP32 from the hardware estimate (a Newton step on it changed the
+// measured force error by nothing: the FP32 rounding of r^2 dominates)
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+struct PairAccF {
+  float fx, fy, fz, pe, vir;
+};
+
+// the sums of one list chunk (at most two FP32 terms in each of fa, fb) moved
+// into the FP64 sums: the per-particle force is a sum of large terms of both
+// signs, whose FP32 rounding would otherwise grow with the list; and the FP64
+// sum of these chunk values is exact in practice, so it does not depend on how
+// the chunks are split over threads
+__device__ __forceinline__ void flush_chunk(PairAccF &fa, PairAccF &fb, PairAcc &a) {
+  a.fx += (double)(fa.fx + fb.fx);
+  a.fy += (double)(fa.fy + fb.fy);
+  a.fz += (double)(fa.fz + fb.fz);
+  a.pe += (double)(fa.pe + fb.pe);
+  a.vir += (double)(fa.vir + fb.vir);
+  fa = PairAccF{0.f, 0.f, 0.f, 0.f, 0.f};
+  fb = PairAccF{0.f, 0.f, 0.f, 0.f, 0.f};
+}
+
+// FP32 pair constants of particle i against a partner of type 0 and of type 1:
+// 1/sigma^2, 4 eps and 8 eps/sigma^2 (MDcode/cell_list+forces.c:19-20)
+struct PairParamsF {
+  float is2[2], e4[2], ge[2];
+  __device__ __forceinline__ explicit PairParamsF(int ti) {
+#pragma unroll
+    for (int tj = 0; tj < 2; tj++) {
+      const int tp = ti + tj;
+      is2[tj] = tp == 0 ? 1.0f : (tp == 1 ? 1.5625f : (float)(1.0 / (0.88 * 0.88)));
+      e4[tj] = tp == 0 ? 4.0f : (tp == 1 ? 6.0f : 2.0f);
+      ge[tj] = 2.0f * e4[tj] * is2[tj];
+    }
+  }
+  // for separations counted in units of u: 1/sigma^2 u^2 and 8 eps/sigma^2 u,
+  // so forces come out in absolute units and the virial in units of 1/u
+  __device__ __forceinline__ PairParamsF(int ti, float u) : PairParamsF(ti) {
+#pragma unroll
+    for (int tj = 0; tj < 2; tj++) {
+      is2[tj] *= u * u;
+      ge[tj] *= u;
+    }
+  }
+};
+
+// FP32 pair term: U = 4 eps (s^12 - s^6) + C0 + C2 (r/sigma)^2 and its radial
+// force factor, written as s6 (s6 - 1) and s6 (6 s6 - 3) s2
+__device__ __forceinline__ void pair_f32(PairAccF &a, float dx, float dy, float dz, const PairParamsF &P,
+                                         bool tj) {
+  const float is2 = tj ? P.is2[1] : P.is2[0];
+  const float dr2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  const float rs2 = dr2 * is2;
+  // evaluated for every entry and masked (no divergent branch): beyond the cut
+  // the factors are zero and each sum gains exactly nothing
+  const bool in = rs2 < (float)KA_RC2;
+  const float e4 = in ? (tj ? P.e4[1] : P.e4[0]) : 0.0f, ge = in ? (tj ? P.ge[1] : P.ge[0]) : 0.0f;
+  const float s2 = rcp_approx(rs2);
+  const float s6 = s2 * s2 * s2;
+  a.pe = fmaf(e4, fmaf(s6, s6, -s6) + fmaf((float)KA_C2, rs2, (float)KA_C0), a.pe);
+  const float g = ge * fmaf(s6 * fmaf(6.0f, s6, -3.0f), s2, -(float)KA_C2);
+  a.fx = fmaf(g, dx, a.fx);
+  a.fy = fmaf(g, dy, a.fy);
+  a.fz = fmaf(g, dz, a.fz);
+  a.vir = fmaf(g, dr2, a.vir);
+}
+
 // stage 2: forces + second kick.  mode 0 = step; 1 = prime (forces at the
 // current positions for systems flagged `prime`, pending velocity scale
 // applied, thermostat first half recomputed); 2 = forces only, velocities and
 // thermostat untouched (calculate_forces)
 template <int TPP, int PREC>
-__global__ void __launch_bounds__(512) k_force_kick(View v, int mode, int tile_base) {
+__global__ void __launch_bounds__(512, 2) k_force_kick(View v, int mode, int tile_base) {
   __shared__ double sh[32];
   __shared__ int s_last;
   const int2 t = v.tiles_b[blockIdx.x];
@@ -1531,6 +1615,7 @@ __global__ void __launch_bounds__(512) k_force_kick(View v, int mode, int tile_b
   if (valid) {
     const double4 pi = v.pos[i];
     const int ti = (int)pi.w;
+    const PairParamsF PF(ti);
     const int nn = v.nbn[i];
     if (nn >= 0) {
       // four list entries per lane per iteration (one 16-byte load; rows are
@@ -1551,10 +1636,23 @@ __global__ void __launch_bounds__(512) k_force_kick(View v, int mode, int tile_b
           if (v2) pair_fp64(a, pi, ti, p2, L, L2);
           if (v3) pair_fp64(a, pi, ti, p3, L, L2);
         } else {
-          pair_fp32(a, pi, ti, p0, L, L2);
-          if (v1) pair_fp32(a, pi, ti, p1, L, L2);
-          if (v2) pair_fp32(a, pi, ti, p2, L, L2);
-          if (v3) pair_fp32(a, pi, ti, p3, L, L2);
+          // separations from the FP64 minimum image, the pair terms in FP32
+          // summed per chunk of four and moved into the FP64 sums (as the
+          // cell-group and whole-box kernels do); an unused entry (past nn)
+          // is the particle itself at separation zero, masked by the cut test
+          const float Lf = (float)L;
+          PairAccF fa = {0.f, 0.f, 0.f, 0.f, 0.f}, fb = {0.f, 0.f, 0.f, 0.f, 0.f};
+          const double4 pj[4] = {p0, p1, p2, p3};
+#pragma unroll
+          for (int e = 0; e < 4; e++) {
+            const float dx = (float)min_image(pi.x - pj[e].x) * Lf;
+            const float dy = (float)min_image(pi.y - pj[e].y) * Lf;
+            const float dz = (float)min_image(pi.z - pj[e].z) * Lf;
+            const float dr2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            // separation zero (the particle itself in an unused entry) gains nothing
+            if (dr2 > 0.0f) pair_f32(e & 1 ? fb : fa, dx, dy, dz, PF, (int)pj[e].w != 0);
+          }
+          flush_chunk(fa, fb, a);
         }
       }
     } else {
@@ -2003,90 +2101,6 @@ __global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
     group_centre(S, t, kc, i, qs);
     copy_back(v, i);
   }
-}
-
-// 1/x for x in the pair range (0.3 < x < 7): the hardware estimate
-// (rcp.approx.ftz.f64) refined by two Newton-Raphson steps y += y (1 - x y),
-// each squaring the relative error, to within an ulp of the rounded quotient
-__device__ __forceinline__ double rcp_nr(double x) {
-  double y;
-  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-  double e = fma(-x, y, 1.0);
-  y = fma(y, e, y);
-  e = fma(-x, y, 1.0);
-  return fma(y, e, y);
-}
-
-// 1/x in FP32 from the hardware estimate (a Newton step on it changed the
-// measured force error by nothing: the FP32 rounding of r^2 dominates)
-__device__ __forceinline__ float rcp_approx(float x) {
-  float y;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-
-struct PairAccF {
-  float fx, fy, fz, pe, vir;
-};
-
-// the sums of one list chunk (at most two FP32 terms in each of fa, fb) moved
-// into the FP64 sums: the per-particle force is a sum of large terms of both
-// signs, whose FP32 rounding would otherwise grow with the list; and the FP64
-// sum of these chunk values is exact in practice, so it does not depend on how
-// the chunks are split over threads
-__device__ __forceinline__ void flush_chunk(PairAccF &fa, PairAccF &fb, PairAcc &a) {
-  a.fx += (double)(fa.fx + fb.fx);
-  a.fy += (double)(fa.fy + fb.fy);
-  a.fz += (double)(fa.fz + fb.fz);
-  a.pe += (double)(fa.pe + fb.pe);
-  a.vir += (double)(fa.vir + fb.vir);
-  fa = PairAccF{0.f, 0.f, 0.f, 0.f, 0.f};
-  fb = PairAccF{0.f, 0.f, 0.f, 0.f, 0.f};
-}
-
-// FP32 pair constants of particle i against a partner of type 0 and of type 1:
-// 1/sigma^2, 4 eps and 8 eps/sigma^2 (MDcode/cell_list+forces.c:19-20)
-struct PairParamsF {
-  float is2[2], e4[2], ge[2];
-  __device__ __forceinline__ explicit PairParamsF(int ti) {
-#pragma unroll
-    for (int tj = 0; tj < 2; tj++) {
-      const int tp = ti + tj;
-      is2[tj] = tp == 0 ? 1.0f : (tp == 1 ? 1.5625f : (float)(1.0 / (0.88 * 0.88)));
-      e4[tj] = tp == 0 ? 4.0f : (tp == 1 ? 6.0f : 2.0f);
-      ge[tj] = 2.0f * e4[tj] * is2[tj];
-    }
-  }
-  // for separations counted in units of u: 1/sigma^2 u^2 and 8 eps/sigma^2 u,
-  // so forces come out in absolute units and the virial in units of 1/u
-  __device__ __forceinline__ PairParamsF(int ti, float u) : PairParamsF(ti) {
-#pragma unroll
-    for (int tj = 0; tj < 2; tj++) {
-      is2[tj] *= u * u;
-      ge[tj] *= u;
-    }
-  }
-};
-
-// FP32 pair term: U = 4 eps (s^12 - s^6) + C0 + C2 (r/sigma)^2 and its radial
-// force factor, written as s6 (s6 - 1) and s6 (6 s6 - 3) s2
-__device__ __forceinline__ void pair_f32(PairAccF &a, float dx, float dy, float dz, const PairParamsF &P,
-                                         bool tj) {
-  const float is2 = tj ? P.is2[1] : P.is2[0];
-  const float dr2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-  const float rs2 = dr2 * is2;
-  // evaluated for every entry and masked (no divergent branch): beyond the cut
-  // the factors are zero and each sum gains exactly nothing
-  const bool in = rs2 < (float)KA_RC2;
-  const float e4 = in ? (tj ? P.e4[1] : P.e4[0]) : 0.0f, ge = in ? (tj ? P.ge[1] : P.ge[0]) : 0.0f;
-  const float s2 = rcp_approx(rs2);
-  const float s6 = s2 * s2 * s2;
-  a.pe = fmaf(e4, fmaf(s6, s6, -s6) + fmaf((float)KA_C2, rs2, (float)KA_C0), a.pe);
-  const float g = ge * fmaf(s6 * fmaf(6.0f, s6, -3.0f), s2, -(float)KA_C2);
-  a.fx = fmaf(g, dx, a.fx);
-  a.fy = fmaf(g, dy, a.fy);
-  a.fz = fmaf(g, dz, a.fz);
-  a.vir = fmaf(g, dr2, a.vir);
 }
 
 // FP64 pair constants of particle i against a partner of type 0 and of type 1:

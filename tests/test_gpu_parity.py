@@ -139,6 +139,29 @@ def test_fp32_pair_forces(cuda_lib, g4000):
     assert rel(th["pe"], g4000["pe0"]) <= 1e-5
 
 
+def test_fp32_pair_forces_all_paths(cuda_lib):
+    """FP32 pair forces against the C restatement (FP64) on each force path:
+    N = 8000 and 16000 take the per-particle kernels (6 and 7 cells per side,
+    N <= 20000), N = 27000 the cell groups split over several blocks; both list
+    cuts; max|dF|/rms|F| and pe within 1e-5."""
+    from activechi4_b200 import Engine, default_params, lattice_state
+    from oracle import Oracle
+    for n, seed, lm in ((8000, 31, 0), (16000, 32, 1), (27000, 33, 1)):
+        st = lattice_state(n, 1.0, seed=seed)
+        o = Oracle.from_state(st, 1.0, 2.0, p_eta=np.array([0.1, 0.2, 0.3]))
+        o.run(40)
+        x, xu, p, _ = o.get_state()
+        st.x, st.xu, st.p = x, xu, p
+        Fo, pe, vir, va = Oracle.from_state(st, 1.0, 2.0).forces()
+        e = Engine(default_params(n, T=1.0, f0=2.0, shuffle=0, precision=1, list_mode=lm))
+        e.set_state(0, st)
+        e.compute_forces()
+        assert force_err(e.get_state()[3], Fo) <= 1e-5, n
+        th = e.thermo()
+        assert rel(th["pe"], pe) <= 1e-5 and rel(th["virial"], vir) <= 1e-5
+        e.close()
+
+
 def test_batch_members_identical_to_alone(cuda_lib, g1000, g4000):
     from activechi4_b200 import Engine, default_params, lattice_state
     st3 = lattice_state(2000, 0.6, seed=9)
