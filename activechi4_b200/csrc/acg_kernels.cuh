@@ -1597,7 +1597,7 @@ __device__ __forceinline__ void pair_f32(PairAccF &a, float dx, float dy, float 
 // applied, thermostat first half recomputed); 2 = forces only, velocities and
 // thermostat untouched (calculate_forces)
 template <int TPP, int PREC>
-__global__ void __launch_bounds__(512, 2) k_force_kick(View v, int mode, int tile_base) {
+__global__ void __launch_bounds__(512) k_force_kick(View v, int mode, int tile_base) {
   __shared__ double sh[32];
   __shared__ int s_last;
   const int2 t = v.tiles_b[blockIdx.x];
