@@ -776,36 +776,60 @@ __global__ void __launch_bounds__(BLOCK_L) k_build_list(View v) {
   const int i = d.poff + loc;
   const double4 pi = v.pos_s[i];
   const int ti = (int)pi.w;
-  const double L = d.L;
   const int nc = d.nc, c = v.cellof[i];
   const int cx = c % nc, cy = (c / nc) % nc, cz = c / (nc * nc);
-  const int lo = stencil_lo(nc), hi = stencil_hi(nc);
+  const int lo = stencil_lo(nc), w = stencil_hi(nc) - lo + 1, ncell = w * w * w;
   const int maxnb = v.maxnb;
   int *row = v.nbl + (size_t)i * maxnb;
+  // the neighbour cells' runs, one cell per lane (27 lanes at most), read at
+  // once; cell q in (oz, oy, ox) order is then broadcast from lane q
+  int my_s0 = 0, my_m = 0;
+  if (lane < ncell) {
+    const int ox = lane % w + lo, oy = (lane / w) % w + lo, oz = lane / (w * w) + lo;
+    const int c2 = wrap_cell(cx + ox, nc) + wrap_cell(cy + oy, nc) * nc + wrap_cell(cz + oz, nc) * nc * nc;
+    my_s0 = d.poff + v.cstart[d.coff + c2];
+    my_m = v.ccount[d.coff + c2];
+  }
+  // the test in FP32 on reduced coordinates with the cut widened by 1e-5
+  // (the lists may hold a few pairs just outside the cut; the force loop tests
+  // every entry): separation error ~1e-7 L against a margin of 1e-5 x 2.85
+  const float L2f = (float)(d.L * d.L);
+  float lc[3];
+  for (int k = 0; k < 3; k++) lc[k] = (float)(lcut2_of(d, k) * (1.0 + 1e-5));
+  const float xi = (float)pi.x, yi = (float)pi.y, zi = (float)pi.z;
   int cnt = 0;
-  for (int oz = lo; oz <= hi; oz++)
-    for (int oy = lo; oy <= hi; oy++)
-      for (int ox = lo; ox <= hi; ox++) {
-        int c2 = wrap_cell(cx + ox, nc) + wrap_cell(cy + oy, nc) * nc + wrap_cell(cz + oz, nc) * nc * nc;
-        const int s0 = d.poff + v.cstart[d.coff + c2], m = v.ccount[d.coff + c2];
-        for (int k0 = 0; k0 < m; k0 += 32) {
-          const int k = k0 + lane;
-          bool ok = false;
-          int j = s0 + k;
-          if (k < m && j != i) {
-            double4 pj = v.pos_s[j];
-            double dx = min_image(pi.x - pj.x), dy = min_image(pi.y - pj.y), dz = min_image(pi.z - pj.z);
-            double dr2 = (dx * dx + dy * dy + dz * dz) * L * L;
-            ok = dr2 < lcut2_of(d, ti + (int)pj.w);
-          }
-          unsigned int mask = __ballot_sync(0xffffffffu, ok);
-          if (ok) {
-            int pos = cnt + __popc(mask & ((1u << lane) - 1u));
-            if (pos < maxnb) row[pos] = j;
-          }
-          cnt += __popc(mask);
-        }
+  // one cell ahead: the next cell's first 32 candidates load while this
+  // cell's are tested
+  int s0 = __shfl_sync(0xffffffffu, my_s0, 0), m = __shfl_sync(0xffffffffu, my_m, 0);
+  double4 cur = lane < m ? v.pos_s[s0 + lane] : make_double4(0, 0, 0, 0);
+  for (int q = 0; q < ncell; q++) {
+    const int qn = q + 1 < ncell ? q + 1 : q;
+    const int s0n = __shfl_sync(0xffffffffu, my_s0, qn), mn = __shfl_sync(0xffffffffu, my_m, qn);
+    const double4 nxt = (q + 1 < ncell && lane < mn) ? v.pos_s[s0n + lane] : make_double4(0, 0, 0, 0);
+    for (int k0 = 0; k0 < m; k0 += 32) {
+      const int k = k0 + lane;
+      const int j = s0 + k;
+      bool ok = false;
+      if (k < m && j != i) {
+        const double4 pj = k0 == 0 ? cur : v.pos_s[j];
+        float dx = xi - (float)pj.x, dy = yi - (float)pj.y, dz = zi - (float)pj.z;
+        dx -= rintf(dx);
+        dy -= rintf(dy);
+        dz -= rintf(dz);
+        const float dr2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) * L2f;
+        ok = dr2 < lc[ti + (int)pj.w];
       }
+      const unsigned int mask = __ballot_sync(0xffffffffu, ok);
+      if (ok) {
+        const int pos = cnt + __popc(mask & ((1u << lane) - 1u));
+        if (pos < maxnb) row[pos] = j;
+      }
+      cnt += __popc(mask);
+    }
+    cur = nxt;
+    s0 = s0n;
+    m = mn;
+  }
   if (lane == 0) {
     if (cnt > maxnb) {
       v.nbn[i] = -1;  // served from the cell list by the force kernel
