@@ -117,7 +117,8 @@ class Server:
     event marks the end of each), so the GPU has work from every run while the
     host admits new requests or builds their graphs."""
 
-    def __init__(self, device=0, hbm_budget=None, max_active=16, chunk_work=2.0e7, depth=2, priority="time"):
+    def __init__(self, device=0, hbm_budget=None, max_active=16, chunk_work=2.0e7, depth=2, priority="time",
+                 max_big=None, big_n=20000):
         self.device = device
         if hbm_budget is None:
             import torch
@@ -132,6 +133,10 @@ class Server:
         # and sets the end of the stream; queued behind the kernels of other
         # runs it ends later still), "size" = larger systems first, "none"
         self.priority = priority
+        # at most max_big runs of more than big_n particles active at once (None:
+        # no limit); a big request waits while smaller ones behind it are admitted
+        self.max_big = max_big
+        self.big_n = big_n
 
     def _level(self, req) -> int:
         if self.priority == "size":
@@ -173,12 +178,20 @@ class Server:
             now = clock() - t0
             while pending and pending[0].arrival <= now:
                 queue.append(pending.pop(0))
-            # admission in arrival order while memory and slots allow
+            # admission in arrival order while memory and slots allow (a big
+            # request over the max_big limit waits; the next in line goes first)
             while queue and len(active) < self.max_active:
-                fp = request_footprint(queue[0])
+                nbig = sum(1 for a in active.values() if a["req"].n > self.big_n)
+                k = 0
+                if self.max_big is not None:
+                    while k < len(queue) and queue[k].n > self.big_n and nbig >= self.max_big:
+                        k += 1
+                    if k == len(queue):
+                        break
+                fp = request_footprint(queue[k])
                 if used + fp > self.budget and active:
                     break
-                req = queue.pop(0)
+                req = queue.pop(k)
                 e = start_run(req, self.device, setup_priority=5)
                 # stepping priority by the policy (`priority`)
                 e.set_priority(self._level(req))
