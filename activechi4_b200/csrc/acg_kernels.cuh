@@ -2151,17 +2151,20 @@ __device__ __forceinline__ void pair_f64(PairAcc &a, double dx, double dy, doubl
   const double is2 = tj ? P.is2[1] : P.is2[0];
   const double dr2 = fma(dx, dx, fma(dy, dy, dz * dz));
   const double rs2 = dr2 * is2;
-  if (rs2 < KA_RC2) {
-    const double e4 = tj ? P.e4[1] : P.e4[0], ge = tj ? P.ge[1] : P.ge[0];
-    const double s2 = rcp_nr(rs2);
-    const double s6 = s2 * s2 * s2;
-    a.pe = fma(e4, fma(s6, s6, -s6) + fma(KA_C2, rs2, KA_C0), a.pe);
-    const double g = ge * fma(s6 * fma(6.0, s6, -3.0), s2, -KA_C2);
-    a.fx = fma(g, dx, a.fx);
-    a.fy = fma(g, dy, a.fy);
-    a.fz = fma(g, dz, a.fz);
-    a.vir = fma(g, dr2, a.vir);
-  }
+  // evaluated for every entry and masked, as the FP32 term: beyond the cut
+  // (s2 <= 0.16, every product finite) the factors are zero and each sum
+  // gains an exact zero, so the sums are those of a branch on the cut; with
+  // no branch the four pairs of a list chunk interleave
+  const bool in = rs2 < KA_RC2;
+  const double e4 = in ? (tj ? P.e4[1] : P.e4[0]) : 0.0, ge = in ? (tj ? P.ge[1] : P.ge[0]) : 0.0;
+  const double s2 = rcp_nr(rs2);
+  const double s6 = s2 * s2 * s2;
+  a.pe = fma(e4, fma(s6, s6, -s6) + fma(KA_C2, rs2, KA_C0), a.pe);
+  const double g = ge * fma(s6 * fma(6.0, s6, -3.0), s2, -KA_C2);
+  a.fx = fma(g, dx, a.fx);
+  a.fy = fma(g, dy, a.fy);
+  a.fz = fma(g, dz, a.fz);
+  a.vir = fma(g, dr2, a.vir);
 }
 
 // launch-bounds occupancy targets of the cell-group force kernel (blocks per
