@@ -1938,6 +1938,49 @@ struct ListWriter {
 // latency of a few blocks).  An unsplit group (a large system, whose blocks
 // fill the GPU) takes one lane per particle, which issues fewer instructions
 // in all.
+// one centre particle's list built by the whole warp (staged index ps, union
+// cell cu, list row t): the lanes test 32 staged candidates at a time over the
+// 27 neighbour cells in (dz, dy, dx) order and a ballot appends the accepted
+// ones in staged order; the last chunk is padded with `pad`.  Returns the
+// entry count (entries past maxnb are not stored).
+__device__ __forceinline__ int warp_list_particle(const float4 *stg, const int *pre4, int nux, int nuy, int cu,
+                                                  int ps, const float lc[3], uint16_t *lst, int t, int M, int maxnb,
+                                                  unsigned pad) {
+  const int lane = threadIdx.x & 31;
+  const int ux = cu % nux, uy = (cu / nux) % nuy, uz = cu / (nux * nuy);
+  const float4 fi = stg[ps];
+  const int ti = __float_as_int(fi.w) >> 15;
+  // cut for a partner of type 0 / 1 (the sum of the two types indexes lc)
+  const float c0 = ti == 0 ? lc[0] : lc[1], c1 = ti == 0 ? lc[1] : lc[2];
+  int n = 0;
+  for (int dz = -1; dz <= 1; dz++)
+    for (int dy = -1; dy <= 1; dy++)
+      for (int dx = -1; dx <= 1; dx++) {
+        const int u2 = (ux + dx) + (uy + dy) * nux + (uz + dz) * nux * nuy;
+        const int q1 = pre4[u2 + 1];
+        for (int qb = pre4[u2]; qb < q1; qb += 32) {
+          const int q = qb + lane;
+          bool ok = false;
+          int code = 0;
+          if (q < q1) {
+            const float4 fj = stg[q];
+            const float ex = fi.x - fj.x, ey = fi.y - fj.y, ez = fi.z - fj.z;
+            const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+            code = __float_as_int(fj.w);
+            ok = r2 < ((code >> 15) ? c1 : c0) && q != ps;
+          }
+          const unsigned bal = __ballot_sync(0xffffffffu, ok);
+          if (ok) {
+            const int k = n + __popc(bal & ((1u << lane) - 1u));
+            if (k < maxnb) lst[group_entry(k, t, M)] = (uint16_t)(code & 0xffff);
+          }
+          n += __popc(bal);
+        }
+      }
+  if (n <= maxnb && lane < ((4 - (n & 3)) & 3)) lst[group_entry(n + lane, t, M)] = (uint16_t)pad;
+  return n;
+}
+
 __global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
   extern __shared__ float4 stg[];
   __shared__ GroupStage S;
@@ -2005,43 +2048,12 @@ __global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
       float lc[3];
       for (int k = 0; k < 3; k++) lc[k] = (float)(lcut2_of(d, k) * (1.0 + 1e-5));
       uint16_t *lst = group_list(v, d, g);
-      const unsigned pad = (unsigned)v.gcap;
       for (int t = t_lo + warp; t < t_hi; t += nwarps) {
         int kc, i, qs;
         group_centre(S, t, kc, i, qs);
         const int cu = S.cu[kc];
-        const int ux = cu % nux, uy = (cu / nux) % nuy, uz = cu / (nux * nuy);
-        const int ps = pre4[cu] + (t - S.cpre[kc]);
-        const float4 fi = stg[ps];
-        const int ti = __float_as_int(fi.w) >> 15;
-        // cut for a partner of type 0 / 1 (the sum of the two types indexes lc)
-        const float c0 = ti == 0 ? lc[0] : lc[1], c1 = ti == 0 ? lc[1] : lc[2];
-        int n = 0;
-        for (int dz = -1; dz <= 1; dz++)
-          for (int dy = -1; dy <= 1; dy++)
-            for (int dx = -1; dx <= 1; dx++) {
-              const int u2 = (ux + dx) + (uy + dy) * nux + (uz + dz) * nux * nuy;
-              const int q1 = pre4[u2 + 1];
-              for (int qb = pre4[u2]; qb < q1; qb += 32) {
-                const int q = qb + lane;
-                bool ok = false;
-                int code = 0;
-                if (q < q1) {
-                  const float4 fj = stg[q];
-                  const float ex = fi.x - fj.x, ey = fi.y - fj.y, ez = fi.z - fj.z;
-                  const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
-                  code = __float_as_int(fj.w);
-                  ok = r2 < ((code >> 15) ? c1 : c0) && q != ps;
-                }
-                const unsigned bal = __ballot_sync(0xffffffffu, ok);
-                if (ok) {
-                  const int k = n + __popc(bal & ((1u << lane) - 1u));
-                  if (k < maxnb) lst[group_entry(k, t, M)] = (uint16_t)(code & 0xffff);
-                }
-                n += __popc(bal);
-              }
-            }
-        if (n <= maxnb && lane < ((4 - (n & 3)) & 3)) lst[group_entry(n + lane, t, M)] = (uint16_t)pad;
+        const int n = warp_list_particle(stg, pre4, nux, nuy, cu, pre4[cu] + (t - S.cpre[kc]), lc, lst, t, M, maxnb,
+                                         (unsigned)v.gcap);
         if (lane == 0) {
           if (n > maxnb) {
             v.nbn[i] = -1;
@@ -2061,12 +2073,15 @@ __global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
       for (int k = 0; k < 3; k++) lc[k] = (float)(lcut2_of(d, k) * (1.0 + 1e-5));
       const bool one_cut = lc[0] == lc[1] && lc[1] == lc[2];
       uint2 *lst = reinterpret_cast<uint2 *>(group_list(v, d, g));
+      // the first 32 particles of each centre cell; a cell's further
+      // particles (a dense cell) are listed below, one warp each, so that no
+      // warp sweeps the 27 cells twice while the others wait at the barrier
       for (int kc = warp; kc < S.nC; kc += nwarps) {
         const int cu = S.cu[kc];
         const int m = S.cpre[kc + 1] - S.cpre[kc];
         const int ux = cu % nux, uy = (cu / nux) % nuy, uz = cu / (nux * nuy);
-        for (int w0 = 0; w0 < m; w0 += 32) {
-          const int w = w0 + lane;
+        {
+          const int w = lane;
           const bool valid = w < m;
           const int t = S.cpre[kc] + w, ps = pre4[cu] + w;
           const float4 fi = valid ? stg[ps] : make_float4(-1e18f, -1e18f, -1e18f, __int_as_float(0));
@@ -2106,6 +2121,30 @@ __global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
             } else {
               v.nbn[i] = n;
             }
+          }
+        }
+      }
+      int nover = 0;
+      for (int k = 0; k < S.nC; k++) nover += max(0, S.cpre[k + 1] - S.cpre[k] - 32);
+      uint16_t *lst16 = group_list(v, d, g);
+      for (int o = warp; o < nover; o += nwarps) {
+        int k = 0, oo = o;
+        for (;;) {
+          const int ex = max(0, S.cpre[k + 1] - S.cpre[k] - 32);
+          if (oo < ex) break;
+          oo -= ex;
+          k++;
+        }
+        const int w = 32 + oo, cu = S.cu[k], t = S.cpre[k] + w;
+        const int n = warp_list_particle(stg, pre4, nux, nuy, cu, pre4[cu] + w, lc, lst16, t, M, maxnb,
+                                         (unsigned)v.gcap);
+        if (lane == 0) {
+          const int i = S.ustart[cu] + w;
+          if (n > maxnb) {
+            v.nbn[i] = -1;
+            atomicAdd(&v.st[r].overflow, 1);
+          } else {
+            v.nbn[i] = n;
           }
         }
       }
@@ -2168,9 +2207,11 @@ __device__ __forceinline__ void pair_f64(PairAcc &a, double dx, double dy, doubl
 }
 
 // launch-bounds occupancy targets of the cell-group force kernel (blocks per
-// SM; measured best: 3 for both precisions, 80 registers without spills)
+// SM).  FP64: 2, no spills (the masked pair term interleaves the four pairs of
+// a chunk; at 4 blocks, 64 registers, it spilled: N = 2.56e5 force 143 -> 129
+// us, N = 1e5 unchanged at 60 us); FP32: 4
 #ifndef ACG_FORCE_MINB64
-#define ACG_FORCE_MINB64 4
+#define ACG_FORCE_MINB64 2
 #endif
 #ifndef ACG_FORCE_MINB32
 #define ACG_FORCE_MINB32 4
@@ -2291,13 +2332,15 @@ __global__ void __launch_bounds__(BLOCK_G, PREC ? ACG_FORCE_MINB32 : ACG_FORCE_M
         slo[v.gcap] = make_float2(0.0f, 0.0f);
       }
     }
-    // staged index q over the whole union, two loads in flight per thread
-    // (the union's cells are runs of consecutive slots)
-    for (int q0 = threadIdx.x; q0 < Q; q0 += 2 * blockDim.x) {
-      double4 p[2];
-      int uu[2];
+    // staged index q over the whole union, SG loads in flight per thread
+    // (the union's cells are runs of consecutive slots; every block of the
+    // grid stages at once at the start, so nothing else hides the latency)
+    constexpr int SG = 4;
+    for (int q0 = threadIdx.x; q0 < Q; q0 += SG * blockDim.x) {
+      double4 p[SG];
+      int uu[SG];
 #pragma unroll
-      for (int e = 0; e < 2; e++) {
+      for (int e = 0; e < SG; e++) {
         const int q = q0 + e * blockDim.x;
         uu[e] = -1;
         if (q < Q) {
@@ -2307,7 +2350,7 @@ __global__ void __launch_bounds__(BLOCK_G, PREC ? ACG_FORCE_MINB32 : ACG_FORCE_M
         }
       }
 #pragma unroll
-      for (int e = 0; e < 2; e++) {
+      for (int e = 0; e < SG; e++) {
         const int u = uu[e], q = q0 + e * blockDim.x;
         if (u < 0) continue;
         const double cx = staged_coord(S, G, u, 0, p[e].x, L);
@@ -2370,12 +2413,14 @@ __global__ void __launch_bounds__(BLOCK_G, PREC ? ACG_FORCE_MINB32 : ACG_FORCE_M
       const PairParamsD P(ti);
       const int nch = (nn + 3) >> 2;
       const uint2 *lp = reinterpret_cast<const uint2 *>(lst) + t;
-      // list chunks are loaded one iteration ahead; two accumulators break
-      // the dependency chains of consecutive pairs
+      // list chunks are loaded two iterations ahead (an L2 round trip is
+      // longer than one chunk's arithmetic); two accumulators break the
+      // dependency chains of consecutive pairs
       PairAcc b = {0.0, 0.0, 0.0, 0.0, 0.0};
       uint2 w = lane < nch ? __ldg(lp + (size_t)lane * M) : make_uint2(0u, 0u);
+      uint2 wn = lane + TPP < nch ? __ldg(lp + (size_t)(lane + TPP) * M) : make_uint2(0u, 0u);
       for (int c = lane; c < nch; c += TPP) {
-        const uint2 wn = c + TPP < nch ? __ldg(lp + (size_t)(c + TPP) * M) : make_uint2(0u, 0u);
+        const uint2 wnn = c + 2 * TPP < nch ? __ldg(lp + (size_t)(c + 2 * TPP) * M) : make_uint2(0u, 0u);
         const int e0 = w.x & 0xffff, e1 = w.x >> 16, e2 = w.y & 0xffff, e3 = w.y >> 16;
         {
           const int q = e0 & 0x7fff;
@@ -2394,6 +2439,7 @@ __global__ void __launch_bounds__(BLOCK_G, PREC ? ACG_FORCE_MINB32 : ACG_FORCE_M
           pair_f64(b, xi - sx[q], yi - sy[q], zi - sz[q], P, e3 >> 15);
         }
         w = wn;
+        wn = wnn;
       }
       a.fx += b.fx;
       a.fy += b.fy;
