@@ -27,6 +27,7 @@ constexpr int NHC_M = 3;
 constexpr int BLOCK_A = 256;    // kick+drift: one thread per particle
 constexpr int BLOCK_L = 256;    // list build: one warp per particle
 constexpr int PART_L = BLOCK_L / 32;
+constexpr int BLOCK_LC = 256;   // list build by cells: one block per cell
 constexpr int BLOCK_R = 256;    // per-slot rebuild kernels (tiles of BLOCK_A)
 constexpr int CELLS_PER_TILE = 8;
 constexpr int BLOCK_SCAN = 512;
@@ -188,6 +189,8 @@ struct View {
   unsigned int *mt; // [nsys][2][MT_WORDS]: two stored MT19937 states per system (current, next)
   int *ccount_b, *cfill, *cstart, *ccount;
   const int2 *tiles_a, *tiles_b, *tiles_l, *tiles_c, *tiles_g, *tiles_x;
+  const int2 *tiles_lc;  // (system, cell): list build by cells (per-particle systems, >= 3 cells per side)
+  int ntiles_lc, lccap;  // lccap: staged candidates of a cell's 27 neighbours (shared memory)
   int *gstart;      // per group: first centre particle (prefix over the system's groups)
   double4 *part_b;
   double4 *pacc;    // whole-box systems: per-particle pe, virial, KE, active virial

@@ -203,7 +203,7 @@ int plan(const acg_params *params, int nsys, Layout &lay, int nsm) {
   for (int k = 0; k < 4; k++) add(4 * Cn);
   add(8 * (S / BLOCK_A + nsys + 1));      // tiles_a
   add(8 * (S / 4 + nsys + 1));            // tiles_b (>= 4 particles per block)
-  add(8 * (S / PART_L + nsys + 1));       // tiles_l
+  add(8 * (S / PART_L + Cn + nsys + 1));  // tiles_lc (one a cell), then tiles_l
   add(8 * (Cn / CELLS_PER_TILE + nsys + 1));
   const size_t Gn = (size_t)lay.ngroups, Gt = (size_t)lay.ngtiles;
   add(8 * (Gt + 1));                      // tiles_g
@@ -240,7 +240,7 @@ struct acg_engine {
   View v{};
   SysDesc *d_desc = nullptr;
   int tpp = 4, block = 128, gtpp = 2, btpp = 2;  // btpp: whole-box kernels
-  int ntiles_a = 0, ntiles_b = 0, ntiles_l = 0, ntiles_c = 0, ntiles_g = 0, ntiles_x = 0;
+  int ntiles_a = 0, ntiles_b = 0, ntiles_l = 0, ntiles_c = 0, ntiles_g = 0, ntiles_x = 0, ntiles_lc = 0;
   int2 *d_tiles_b = nullptr;
   int2 *d_tiles_x = nullptr;
   std::vector<int> dirty;  // systems whose forces/lists must be recomputed
@@ -291,6 +291,7 @@ GroupFn group_fn(int gtpp, int prec) {
 // group force kernel: 24 bytes per staged particle and one dummy slot
 size_t group_smem(int gcap) { return 3 * ((size_t)gcap + 1) * sizeof(double); }
 size_t list_smem(int gcap) { return ((size_t)gcap + 3 * MAX_UNION) * sizeof(float4); }
+size_t list_cells_smem(int lccap) { return (size_t)lccap * sizeof(float4); }
 
 GroupFn box_fn(int gtpp, int prec) {
   switch (gtpp) {
@@ -434,8 +435,8 @@ void drop_graphs(acg_engine *e) {
 // memory) and can be updated in place instead of instantiated anew
 std::string graph_shape(const acg_engine *e, int K) {
   char b[160];
-  snprintf(b, sizeof(b), "K%d g%d x%d b%d l%d p%d t%d/%d/%d/%d i%d%d%d", K, e->ntiles_g > 0, e->ntiles_x > 0,
-           e->ntiles_b > 0, e->ntiles_l > 0, e->lay.desc[0].precision, e->tpp, e->gtpp, e->btpp, e->block,
+  snprintf(b, sizeof(b), "K%d g%d x%d b%d l%d%d p%d t%d/%d/%d/%d i%d%d%d", K, e->ntiles_g > 0, e->ntiles_x > 0,
+           e->ntiles_b > 0, e->ntiles_l > 0, e->ntiles_lc > 0, e->lay.desc[0].precision, e->tpp, e->gtpp, e->btpp, e->block,
            e->any_gauss, e->any_npt, e->any_brown);
   return b;
 }
@@ -499,6 +500,7 @@ int launch_rebuild(acg_engine *e) {
   if (e->ntiles_x) k_rebuild_compact<<<1, BLOCK_COMPACT, 0, s>>>(v);
   if (e->ntiles_g) k_build_list_groups<<<e->ntiles_g, BLOCK_G, list_smem(v.gcap), s>>>(v);
   if (e->ntiles_x) k_build_list_box<<<e->ntiles_x * LIST_SPLIT, BLOCK_X, box_list_smem(e->lay.box_cell_nmax), s>>>(v);
+  if (e->ntiles_lc) k_build_list_cells<<<e->ntiles_lc, BLOCK_LC, list_cells_smem(v.lccap), s>>>(v);
   if (e->ntiles_l) k_build_list<<<e->ntiles_l, BLOCK_L, 0, s>>>(v);
   CK(cudaGetLastError());
   return ACG_OK;
@@ -723,6 +725,7 @@ int add_steps(acg_engine *e, cudaGraph_t g, int K, cudaGraphNode_t *prev_io) {
               {(void *)k_rebuild_compact, e->ntiles_x ? 1 : 0, BLOCK_COMPACT, 0},
               {(void *)k_build_list_groups, e->ntiles_g, BLOCK_G, list_smem(v.gcap)},
               {(void *)k_build_list_box, e->ntiles_x * LIST_SPLIT, BLOCK_X, box_list_smem(e->lay.box_cell_nmax)},
+              {(void *)k_build_list_cells, e->ntiles_lc, BLOCK_LC, list_cells_smem(v.lccap)},
               {(void *)k_build_list, e->ntiles_l, BLOCK_L, 0}};
     int all = -1;
     void *sa[] = {&v, &all};
@@ -993,7 +996,7 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   v.ccount = (int *)take(4 * Cn);
   int2 *ta = (int2 *)take(8 * (S / BLOCK_A + nsys + 1));
   e->d_tiles_b = (int2 *)take(8 * (S / 4 + nsys + 1));
-  int2 *tl = (int2 *)take(8 * (S / PART_L + nsys + 1));
+  int2 *tl = (int2 *)take(8 * (S / PART_L + Cn + nsys + 1));
   int2 *tc = (int2 *)take(8 * (Cn / CELLS_PER_TILE + nsys + 1));
   const size_t Gn = (size_t)L.ngroups, Gt = (size_t)L.ngtiles;
   int2 *tg = (int2 *)take(8 * (Gt + 1));
@@ -1030,7 +1033,7 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
     v.box_warp = nsub_particles <= BOX_WARP_MAX;
   }
 
-  std::vector<int2> h_a, h_l, h_c, h_g;
+  std::vector<int2> h_a, h_l, h_c, h_g, h_lc;
   for (int r = 0; r < nsys; r++) {
     SysDesc &d = e->lay.desc[r];
     d.tile0_a = (int)h_a.size();
@@ -1041,6 +1044,8 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
       for (int g = 0; g < d.ng * d.ng * d.ng * d.gsplit; g++) h_g.push_back(make_int2(r, g));
     else if (d.box)
       continue;  // whole-box tiles: build_tiles_x
+    else if (d.nc >= 3)
+      for (int c = 0; c < d.ncell; c++) h_lc.push_back(make_int2(r, c));
     else
       for (int s = 0; s < d.n; s += PART_L) h_l.push_back(make_int2(r, s));
   }
@@ -1058,6 +1063,10 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   e->d_tiles_x = tx;
   e->ntiles_a = (int)h_a.size();
   e->ntiles_l = (int)h_l.size();
+  e->ntiles_lc = (int)h_lc.size();
+  v.tiles_lc = tl;
+  v.tiles_l = tl + h_lc.size();
+  v.ntiles_lc = e->ntiles_lc;
   e->ntiles_c = (int)h_c.size();
   e->ntiles_g = (int)h_g.size();
   v.ntiles_a = e->ntiles_a;
@@ -1072,6 +1081,15 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
       if (L.desc[r].ng > 0) mean_u = std::max(mean_u, 64.0 * L.desc[r].n / (double)L.desc[r].ncell);
     v.gcap = (int)align_up((size_t)(1.08 * mean_u + 128.0), 32);
     v.gcap = std::min(v.gcap, 8192);
+    // staged candidates of a cell's 27 neighbours (list build by cells):
+    // 1.5x the mean of the densest such system plus margin; a cell above it
+    // leaves its particles to the force kernel's cell scan
+    double mean_c = 0;
+    for (int r = 0; r < nsys; r++) {
+      const SysDesc &dr = L.desc[r];
+      if (!dr.box && dr.ng == 0 && dr.nc >= 3) mean_c = std::max(mean_c, 27.0 * dr.n / (double)dr.ncell);
+    }
+    v.lccap = (int)std::min<size_t>(align_up((size_t)(1.5 * mean_c + 128.0), 32), 8192);
   }
   // the shared-memory limit is a property of the kernel function, shared by
   // every engine of the process: only ever raise it
@@ -1085,6 +1103,7 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
   for (int gt : {1, 2, 4})
     for (int pr : {0, 1}) attr_ok = attr_ok && raise_smem((const void *)group_fn(gt, pr), group_smem(v.gcap));
   attr_ok = attr_ok && raise_smem((const void *)k_build_list_groups, list_smem(v.gcap));
+  attr_ok = attr_ok && raise_smem((const void *)k_build_list_cells, list_cells_smem(v.lccap));
   if (L.box_nmax > 0) {
     if (box_list_smem(L.box_cell_nmax) > 227 * 1024 || box_smem(L.box_nmax, 0) > 227 * 1024) {
       acg_destroy(e);
@@ -1114,9 +1133,12 @@ int acg_create(const acg_params *params, int nsys, int device, acg_engine **out)
       (!h_g.empty() &&
        cudaMemcpyAsync(tg, h_g.data(), h_g.size() * sizeof(int2), cudaMemcpyHostToDevice, e->stream) !=
            cudaSuccess) ||
-      (!h_l.empty() &&
-       cudaMemcpyAsync(tl, h_l.data(), h_l.size() * sizeof(int2), cudaMemcpyHostToDevice, e->stream) !=
+      (!h_lc.empty() &&
+       cudaMemcpyAsync(tl, h_lc.data(), h_lc.size() * sizeof(int2), cudaMemcpyHostToDevice, e->stream) !=
            cudaSuccess) ||
+      (!h_l.empty() &&
+       cudaMemcpyAsync(tl + h_lc.size(), h_l.data(), h_l.size() * sizeof(int2), cudaMemcpyHostToDevice,
+                       e->stream) != cudaSuccess) ||
       build_tiles_x(e) != ACG_OK)
     return cleanup_fail(fail(ACG_ERR_CUDA, "initial upload failed"));
   std::vector<SysState> st(nsys);
@@ -2032,7 +2054,7 @@ int acg_bench_steps(acg_engine *e, int64_t nsteps, size_t flush_bytes, double *m
   const long long per_step = 1 + nforce + 2 * e->any_gauss + e->any_npt + 2 * e->any_brown +
                              (e->any_npt || e->any_brown) * nforce;
   const long long per_rebuild = 5 + (e->lay.box_m3max > 0) + 2 * (e->ntiles_x > 0) + (e->ntiles_g > 0) +
-                                (e->ntiles_l > 0);
+                                (e->ntiles_l > 0) + (e->ntiles_lc > 0);
   long long steps_with_rebuild = 0, shuffles = 0, obs_steps = 0;
   for (int r = 0; r < nsys; r++) steps_with_rebuild = std::max(steps_with_rebuild, st1[r].rebuilds - st0[r].rebuilds);
   for (long long k = 0; k < nsteps; k++) {

@@ -766,6 +766,104 @@ __device__ __forceinline__ void copy_back(const View &v, int i) {
 
 // Neighbour lists for boxes with 2 cells per side (one warp per particle, FP64
 // minimum image per pair: the stencil's shifted frame is ambiguous there).
+// Lists of the per-particle kernels by cells (>= 3 cells per side): one
+// block per cell stages its 27 neighbour cells' particles once (float4 of the
+// FP32 reduced coordinates and slot | type << 30, cells in (oz, oy, ox) order,
+// slots ascending), then each warp lists one centre particle at a time, the
+// lanes testing 32 staged candidates a step and a ballot appending the
+// accepted ones in staged order.  Same test, same order and so the same lists
+// as k_build_list, which reads every candidate of every particle from global
+// memory (27 cells x ~30 candidates x 32 bytes a particle).  A cell whose
+// neighbourhood exceeds lccap staged candidates leaves its particles to the
+// force kernel's cell scan.
+__global__ void __launch_bounds__(BLOCK_LC) k_build_list_cells(View v) {
+  extern __shared__ float4 cstg[];
+  __shared__ int s_pre[28], s_start[27];
+  const int2 t = v.tiles_lc[blockIdx.x];
+  const int r = t.x, c = t.y;
+  if (!v.st[r].rebuild) return;
+  const SysDesc &d = v.desc[r];
+  const int nc = d.nc;
+  const int cx = c % nc, cy = (c / nc) % nc, cz = c / (nc * nc);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  if (warp == 0) {
+    int m = 0;
+    if (lane < 27) {
+      const int ox = lane % 3 - 1, oy = (lane / 3) % 3 - 1, oz = lane / 9 - 1;
+      const int c2 = wrap_cell(cx + ox, nc) + wrap_cell(cy + oy, nc) * nc + wrap_cell(cz + oz, nc) * nc * nc;
+      s_start[lane] = d.poff + v.cstart[d.coff + c2];
+      m = v.ccount[d.coff + c2];
+    }
+    int x = m;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane < 27) s_pre[lane + 1] = x;
+    if (lane == 0) s_pre[0] = 0;
+  }
+  __syncthreads();
+  const int Q = s_pre[27];
+  const int i0 = s_start[13], mc = s_pre[14] - s_pre[13];  // the centre cell (offset 0, 0, 0)
+  const int maxnb = v.maxnb;
+  if (Q <= v.lccap) {
+    for (int q = threadIdx.x; q < Q; q += blockDim.x) {
+      int u = 0;
+      while (s_pre[u + 1] <= q) u++;
+      const int j = s_start[u] + (q - s_pre[u]);
+      const double4 p = v.pos_s[j];
+      cstg[q] = make_float4((float)p.x, (float)p.y, (float)p.z, __int_as_float(j | ((int)p.w << 30)));
+    }
+    __syncthreads();
+    const float L2f = (float)(d.L * d.L);
+    float lc[3];
+    for (int k = 0; k < 3; k++) lc[k] = (float)(lcut2_of(d, k) * (1.0 + 1e-5));
+    for (int w = warp; w < mc; w += nwarps) {
+      const int i = i0 + w;
+      const float4 fi = cstg[s_pre[13] + w];
+      const int ti = __float_as_int(fi.w) >> 30;
+      int *row = v.nbl + (size_t)i * maxnb;
+      int cnt = 0;
+      for (int q0 = 0; q0 < Q; q0 += 32) {
+        const int q = q0 + lane;
+        bool ok = false;
+        int j = 0;
+        if (q < Q) {
+          const float4 fj = cstg[q];
+          const int code = __float_as_int(fj.w);
+          j = code & 0x3fffffff;
+          float dx = fi.x - fj.x, dy = fi.y - fj.y, dz = fi.z - fj.z;
+          dx -= rintf(dx);
+          dy -= rintf(dy);
+          dz -= rintf(dz);
+          const float dr2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) * L2f;
+          ok = dr2 < lc[ti + (code >> 30)] && j != i;
+        }
+        const unsigned mask = __ballot_sync(0xffffffffu, ok);
+        if (ok) {
+          const int pos = cnt + __popc(mask & ((1u << lane) - 1u));
+          if (pos < maxnb) row[pos] = j;
+        }
+        cnt += __popc(mask);
+      }
+      if (lane == 0) {
+        if (cnt > maxnb) {
+          v.nbn[i] = -1;  // served from the cell list by the force kernel
+          atomicAdd(&v.st[r].overflow, 1);
+        } else {
+          v.nbn[i] = cnt;
+        }
+      }
+    }
+  } else {
+    for (int w = threadIdx.x; w < mc; w += blockDim.x) {
+      v.nbn[i0 + w] = -1;
+      atomicAdd(&v.st[r].overflow, 1);
+    }
+  }
+  for (int w = threadIdx.x; w < mc; w += blockDim.x) copy_back(v, i0 + w);
+}
+
 __global__ void __launch_bounds__(BLOCK_L) k_build_list(View v) {
   int2 t = v.tiles_l[blockIdx.x];
   const int r = t.x;
@@ -1906,6 +2004,14 @@ __device__ __forceinline__ size_t group_entry(int k, int t, int M) {
 // shift register (the newest entry enters at the top, so after four the
 // first is in the low bits); whole chunks are stored as uint2 at
 // chunk * stride + row
+// the next index of a block-shared counter for the calling warp (lane 0 takes
+// it, the warp shares it)
+__device__ __forceinline__ int warp_next(int &counter) {
+  int o = 0;
+  if ((threadIdx.x & 31) == 0) o = atomicAdd(&counter, 1);
+  return __shfl_sync(0xffffffffu, o, 0);
+}
+
 struct ListWriter {
   unsigned lo = 0u, hi = 0u;
   int n = 0;
@@ -1985,6 +2091,7 @@ __global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
   extern __shared__ float4 stg[];
   __shared__ GroupStage S;
   __shared__ int pre4[MAX_UNION + 1];
+  __shared__ int s_over;  // next overflow particle to hand out
   const int2 tile = v.tiles_g[blockIdx.x];
   const int r = tile.x;
   if (!v.st[r].rebuild) return;
@@ -2005,6 +2112,7 @@ __global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
         m += (S.upre[u + 1] - S.upre[u] + 3) & ~3;
       }
       pre4[S.nU] = m;
+      s_over = 0;
     }
     __syncthreads();
     const double L = d.L;
@@ -2127,7 +2235,9 @@ __global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
       int nover = 0;
       for (int k = 0; k < S.nC; k++) nover += max(0, S.cpre[k + 1] - S.cpre[k] - 32);
       uint16_t *lst16 = group_list(v, d, g);
-      for (int o = warp; o < nover; o += nwarps) {
+      // handed out as warps come free (a particle's list does not depend on
+      // which warp builds it)
+      for (int o = warp_next(s_over); o < nover; o = warp_next(s_over)) {
         int k = 0, oo = o;
         for (;;) {
           const int ex = max(0, S.cpre[k + 1] - S.cpre[k] - 32);
@@ -2158,7 +2268,8 @@ __global__ void __launch_bounds__(BLOCK_G) k_build_list_groups(View v) {
       atomicAdd(&v.st[r].overflow, 1);
     }
   }
-  __syncthreads();
+  // no barrier: the copy reads and writes no shared memory and no list, so a
+  // warp done with its lists starts it while the others finish theirs
   for (int t = t_lo + threadIdx.x; t < t_hi; t += blockDim.x) {
     int kc, i, qs;
     group_centre(S, t, kc, i, qs);
