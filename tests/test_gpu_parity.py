@@ -162,6 +162,32 @@ def test_fp32_pair_forces_all_paths(cuda_lib):
         e.close()
 
 
+def test_list_by_cells_staging_overflow(cuda_lib):
+    """A per-particle system (N = 8000, 6 cells per side) squeezed into x <
+    0.45: cells in the dense slab have more neighbour candidates than the list
+    build by cells stages (~2000 against ~1630), so their particles take the
+    force kernel's cell scan (rows of 512 entries, so that the row capacity is
+    not what overflows).  FP64 forces, pe and virial <= 1e-12 against the C
+    restatement, FP32 pair forces <= 1e-5."""
+    from activechi4_b200 import Engine, default_params, lattice_state
+    from oracle import Oracle
+    n = 8000
+    st = lattice_state(n, 1.0, seed=41)
+    st.x[:, 0] *= 0.45
+    st.xu = st.x.copy()
+    Fo, pe, vir, _ = Oracle.from_state(st, 1.0, 2.0).forces()
+    for prec, tol in ((0, 1e-12), (1, 1e-5)):
+        e = Engine(default_params(n, T=1.0, f0=2.0, shuffle=0, nb_capacity=512, precision=prec))
+        e.set_state(0, st)
+        e.compute_forces()
+        th = e.thermo()
+        assert th["overflow"] > 0
+        err = force_err(e.get_state()[3], Fo)
+        assert err <= tol, (prec, err)
+        assert rel(th["pe"], pe) <= tol and rel(th["virial"], vir) <= tol, prec
+        e.close()
+
+
 def test_batch_members_identical_to_alone(cuda_lib, g1000, g4000):
     from activechi4_b200 import Engine, default_params, lattice_state
     st3 = lattice_state(2000, 0.6, seed=9)
