@@ -167,8 +167,10 @@ def test_list_by_cells_staging_overflow(cuda_lib):
     0.45: cells in the dense slab have more neighbour candidates than the list
     build by cells stages (~2000 against ~1630), so their particles take the
     force kernel's cell scan (rows of 512 entries, so that the row capacity is
-    not what overflows).  FP64 forces, pe and virial <= 1e-12 against the C
-    restatement, FP32 pair forces <= 1e-5."""
+    not what overflows).  Against the C restatement: FP64 forces <= 1e-12,
+    pe and virial <= 1e-11 (here sums of ~1e6 pair terms up to ~1e5 each, the
+    overlapping particles of the squeezed slab, summed in another order), FP32
+    pair forces, pe and virial <= 1e-5."""
     from activechi4_b200 import Engine, default_params, lattice_state
     from oracle import Oracle
     n = 8000
@@ -176,7 +178,7 @@ def test_list_by_cells_staging_overflow(cuda_lib):
     st.x[:, 0] *= 0.45
     st.xu = st.x.copy()
     Fo, pe, vir, _ = Oracle.from_state(st, 1.0, 2.0).forces()
-    for prec, tol in ((0, 1e-12), (1, 1e-5)):
+    for prec, tol, tol_sum in ((0, 1e-12, 1e-11), (1, 1e-5, 1e-5)):
         e = Engine(default_params(n, T=1.0, f0=2.0, shuffle=0, nb_capacity=512, precision=prec))
         e.set_state(0, st)
         e.compute_forces()
@@ -184,7 +186,7 @@ def test_list_by_cells_staging_overflow(cuda_lib):
         assert th["overflow"] > 0
         err = force_err(e.get_state()[3], Fo)
         assert err <= tol, (prec, err)
-        assert rel(th["pe"], pe) <= tol and rel(th["virial"], vir) <= tol, prec
+        assert rel(th["pe"], pe) <= tol_sum and rel(th["virial"], vir) <= tol_sum, prec
         e.close()
 
 
