@@ -40,7 +40,11 @@ constexpr int BOX_WARP_MAX = 16384;  // whole-box particles up to which lists ar
 constexpr int GSPLIT_MAX = 8;     // most force blocks per cell group (small boxes)
 // measured on B200 (FP32, T = 0.45, step latency of one system alone):
 // N = 4505 43-47 us per step on the per-particle kernels against 53 us on
-// split cell groups, N = 11154 54 us against 59 us; N = 30000 68 us either way
+// split cell groups, N = 11154 54 us against 59 us; N = 30000 68 us either way.
+// With the per-particle lists built by cells: N = 30000 forces 43 us against
+// 28 us on cell groups, a rebuild 101 us against 160 us, so the groups stay
+// ahead at T = 0.45 (a rebuild every ~8 steps); N = 88250 134 against 103 us
+// per step
 #ifndef ACG_GSPLIT_BLOCKS
 #define ACG_GSPLIT_BLOCKS 296
 #endif
