@@ -36,6 +36,15 @@ constexpr int MAX_UNION = 64;     // 4 x 4 x 4 union cells of a 2 x 2 x 2 group
 constexpr int BLOCK_X = 256;      // threads of the whole-box kernels
 constexpr int BOX_CELLS = 8;      // most cells per whole-box block
 constexpr int LIST_SPLIT = 4;     // blocks sharing a whole-box tile in the list build
+// expected particles of a 2 x 2 x 2 list brick at most (else 2 x 2 x 1).
+// Measured on the batched workload (256 FP32 replicas at density 1.2, where
+// a 2 x 2 x 2 brick expects 29-51): 28 405 us a step, 48 and 64 650-660 us
+// (the many particles past a brick's 32 lanes, listed one warp each, cost
+// more than the lanes the smaller bricks leave idle)
+#ifndef ACG_BRICK2_MAX
+#define ACG_BRICK2_MAX 28.0
+#endif
+constexpr double BRICK2_MAX = ACG_BRICK2_MAX;
 constexpr int BOX_WARP_MAX = 16384;  // whole-box particles up to which lists are built one warp per particle
 constexpr int GSPLIT_MAX = 8;     // most force blocks per cell group (small boxes)
 // measured on B200 (FP32, T = 0.45, step latency of one system alone):

@@ -147,9 +147,10 @@ int plan(const acg_params *params, int nsys, Layout &lay, int nsm) {
       if (m >= 5 && m * m * m <= MAX_SUB3) {
         d.msub = m;
         // list bricks of 2 x 2 x 2 sub-cells, or 2 x 2 x 1 where that would
-        // hold more than about a warp of particles
+        // hold more than BRICK2_MAX particles (a brick's particles past 32
+        // are listed one warp each)
         const double hs = d.L / m;
-        d.bz = 8.0 * hs * hs * hs * d.n / (d.L * d.L * d.L) > 28.0 ? 1 : 2;
+        d.bz = 8.0 * hs * hs * hs * d.n / (d.L * d.L * d.L) > BRICK2_MAX ? 1 : 2;
         lay.box_m3max = std::max(lay.box_m3max, m * m * m);
         d.soff = lay.nsub;
         lay.nsub += m * m * m + 1;

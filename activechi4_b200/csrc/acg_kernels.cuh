@@ -766,6 +766,18 @@ __device__ __forceinline__ void copy_back(const View &v, int i) {
 
 // Neighbour lists for boxes with 2 cells per side (one warp per particle, FP64
 // minimum image per pair: the stencil's shifted frame is ambiguous there).
+// the union cell holding staged index q: the last u with pre[u] <= q (pre is a
+// non-decreasing prefix over n cells in shared memory)
+__device__ __forceinline__ int union_of(const int *pre, int n, int q) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (pre[mid] <= q) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
 // Lists of the per-particle kernels by cells (>= 3 cells per side): one
 // block per cell stages its 27 neighbour cells' particles once (float4 of the
 // FP32 reduced coordinates and slot | type << 30, cells in (oz, oy, ox) order,
@@ -807,12 +819,25 @@ __global__ void __launch_bounds__(BLOCK_LC) k_build_list_cells(View v) {
   const int i0 = s_start[13], mc = s_pre[14] - s_pre[13];  // the centre cell (offset 0, 0, 0)
   const int maxnb = v.maxnb;
   if (Q <= v.lccap) {
-    for (int q = threadIdx.x; q < Q; q += blockDim.x) {
-      int u = 0;
-      while (s_pre[u + 1] <= q) u++;
-      const int j = s_start[u] + (q - s_pre[u]);
-      const double4 p = v.pos_s[j];
-      cstg[q] = make_float4((float)p.x, (float)p.y, (float)p.z, __int_as_float(j | ((int)p.w << 30)));
+    // staged index q over the 27 cells' runs, four loads in flight a thread
+    for (int q0 = threadIdx.x; q0 < Q; q0 += 4 * blockDim.x) {
+      double4 p[4];
+      int jj[4];
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const int q = q0 + e * blockDim.x;
+        jj[e] = -1;
+        if (q < Q) {
+          const int u = union_of(s_pre, 27, q);
+          jj[e] = s_start[u] + (q - s_pre[u]);
+          p[e] = v.pos_s[jj[e]];
+        }
+      }
+#pragma unroll
+      for (int e = 0; e < 4; e++)
+        if (jj[e] >= 0)
+          cstg[q0 + e * blockDim.x] =
+              make_float4((float)p[e].x, (float)p[e].y, (float)p[e].z, __int_as_float(jj[e] | ((int)p[e].w << 30)));
     }
     __syncthreads();
     const float L2f = (float)(d.L * d.L);
@@ -822,6 +847,8 @@ __global__ void __launch_bounds__(BLOCK_LC) k_build_list_cells(View v) {
       const int i = i0 + w;
       const float4 fi = cstg[s_pre[13] + w];
       const int ti = __float_as_int(fi.w) >> 30;
+      // cut for a partner of type 0 / 1 (the sum of the two types indexes lc)
+      const float c0 = ti == 0 ? lc[0] : lc[1], c1 = ti == 0 ? lc[1] : lc[2];
       int *row = v.nbl + (size_t)i * maxnb;
       int cnt = 0;
       for (int q0 = 0; q0 < Q; q0 += 32) {
@@ -837,7 +864,7 @@ __global__ void __launch_bounds__(BLOCK_LC) k_build_list_cells(View v) {
           dy -= rintf(dy);
           dz -= rintf(dz);
           const float dr2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) * L2f;
-          ok = dr2 < lc[ti + (code >> 30)] && j != i;
+          ok = dr2 < ((code >> 30) ? c1 : c0) && j != i;
         }
         const unsigned mask = __ballot_sync(0xffffffffu, ok);
         if (ok) {
@@ -1890,17 +1917,6 @@ struct GroupStage {
   int cpre[9];               // centre offset of each centre cell
 };
 
-// the union cell holding staged index q: the last u with pre[u] <= q (pre is a
-// non-decreasing prefix over n cells in shared memory)
-__device__ __forceinline__ int union_of(const int *pre, int n, int q) {
-  int lo = 0, hi = n - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (pre[mid] <= q) lo = mid;
-    else hi = mid - 1;
-  }
-  return lo;
-}
 
 __device__ void group_prologue(const View &v, const SysDesc &d, const GroupGeom &G, GroupStage &S) {
   const int nc = d.nc;
@@ -2854,6 +2870,9 @@ __device__ __forceinline__ int subcell_of(double x, int m) { return min(max((int
 // rows of up to 6 sub-cells contiguous in sub-cell order.  Where the union is
 // wider than the box (5 sub-cells per side) a sub-cell comes under two image
 // shifts, of which at most one can be in range (L > 2 x the list cut).
+__device__ __forceinline__ void box_list_particle(const View &v, const SysDesc &d, int r, const float4 *xs,
+                                                  const int *sst, int ps, int lane);
+
 __device__ __forceinline__ void box_list_brick(const View &v, const SysDesc &d, int r, const float4 *xs,
                                                const int *sst, int B, int lane) {
   const int m = d.msub, bz = d.bz, n = d.n;
@@ -2873,9 +2892,12 @@ __device__ __forceinline__ void box_list_brick(const View &v, const SysDesc &d, 
       const int row = m * (y + m * z);
       total += sst[row + x1] - sst[row + x0];
     }
-  for (int k0 = 0; k0 < total; k0 += 32) {
+  // the brick's first 32 particles, one lane each; the others (a dense
+  // brick) one warp each below, so the warp does not sweep the brick's
+  // neighbourhood a second time for a few lanes
+  {
     // this lane's particle: entry k of the brick's runs (z, y) of x0..x1-1
-    int k = k0 + lane, ps = -1;
+    int k = lane, ps = -1;
     for (int z = z0; z < z1; z++)
       for (int y = y0; y < y1; y++) {
         const int row = m * (y + m * z);
@@ -2941,6 +2963,22 @@ __device__ __forceinline__ void box_list_brick(const View &v, const SysDesc &d, 
         v.nbn[i] = lw.n;
       }
     }
+  }
+  // the same lists (the sub-cells within two of the particle's own, rows in
+  // (z, y) order, increasing unwrapped x): the brick's neighbourhood holds
+  // them, and candidates farther than two sub-cells are beyond every cut
+  for (int k1 = 32; k1 < total; k1++) {
+    int k = k1, ps = -1;
+    for (int z = z0; z < z1; z++)
+      for (int y = y0; y < y1; y++) {
+        const int row = m * (y + m * z);
+        const int q0 = sst[row + x0], len = sst[row + x1] - q0;
+        if (ps < 0) {
+          if (k < len) ps = q0 + k;
+          else k -= len;
+        }
+      }
+    box_list_particle(v, d, r, xs, sst, ps, lane);
   }
 }
 
