@@ -181,13 +181,9 @@ class Server:
             # admission in arrival order while memory and slots allow (a big
             # request over the max_big limit waits; the next in line goes first)
             while queue and len(active) < self.max_active:
-                nbig = sum(1 for a in active.values() if a["req"].n > self.big_n)
-                k = 0
-                if self.max_big is not None:
-                    while k < len(queue) and queue[k].n > self.big_n and nbig >= self.max_big:
-                        k += 1
-                    if k == len(queue):
-                        break
+                k = next_admissible(queue, [a["req"].n for a in active.values()], self.max_big, self.big_n)
+                if k < 0:
+                    break
                 fp = request_footprint(queue[k])
                 if used + fp > self.budget and active:
                     break
@@ -267,6 +263,22 @@ def poisson_requests(count, rate=20.0, n_range=(1000, 256000), step_range=(10000
         reqs.append(RunRequest(i, n, max(64, steps), float(rng.choice(T_SET)), float(rng.choice(F0_SET)),
                                int(rng.choice(TAU_SET)), seed=10000 * seed + i, arrival=t, precision=precision))
     return reqs
+
+
+def next_admissible(queue, active_n, max_big=None, big_n=20000) -> int:
+    """Index in `queue` (arrival order) of the next request to admit, or -1:
+    the first one, except that a request of more than `big_n` particles
+    waits while `max_big` such runs are active (sizes `active_n`), and the
+    first smaller request behind it goes instead."""
+    if not queue:
+        return -1
+    if max_big is None:
+        return 0
+    nbig = sum(1 for n in active_n if n > big_n)
+    for k, req in enumerate(queue):
+        if req.n <= big_n or nbig < max_big:
+            return k
+    return -1
 
 
 def latency_stats(results):
