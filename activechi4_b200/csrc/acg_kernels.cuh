@@ -1771,8 +1771,12 @@ __global__ void __launch_bounds__(512) k_force_kick(View v, int mode, int tile_b
       // 16-byte aligned and padded to maxnb, entries past nn are not used)
       const int4 *row4 = reinterpret_cast<const int4 *>(v.nbl + (size_t)i * v.maxnb);
       const int nb4 = (nn + 3) >> 2;
+      // each chunk's slots are loaded one iteration ahead, so the positions it
+      // gathers wait for one L2 round trip, not two
+      int4 jn = lane < nb4 ? __ldg(row4 + lane) : make_int4(0, 0, 0, 0);
       for (int b = lane; b < nb4; b += TPP) {
-        const int4 jj = __ldg(row4 + b);
+        const int4 jj = jn;
+        if (b + TPP < nb4) jn = __ldg(row4 + b + TPP);
         const int k0 = 4 * b;
         const bool v1 = k0 + 1 < nn, v2 = k0 + 2 < nn, v3 = k0 + 3 < nn;
         const double4 p0 = v.pos[jj.x];

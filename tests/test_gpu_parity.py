@@ -190,6 +190,40 @@ def test_list_by_cells_staging_overflow(cuda_lib):
         e.close()
 
 
+def test_batched_bricks_past_32(cuda_lib):
+    """Twelve whole-box replicas (N = 1800 at rho = 0.8: 4 cells and 9 list
+    sub-cells per side, bricks of 2 x 2 x 2 sub-cells with ~20 particles
+    expected; 21600 particles in all, so the engine lists by bricks) with x
+    squeezed into [0, 0.6) in the odd replicas: ~30 bricks of each of those
+    hold more than 32 particles, and their particles past 32 are listed one
+    warp each.  Against the C restatement for every replica: FP64 forces <=
+    1e-12, pe and virial <= 1e-11; FP32 pair forces, pe and virial <= 1e-5."""
+    from activechi4_b200 import Engine, default_params, lattice_state
+    from oracle import Oracle
+    n, rho, nrep = 1800, 0.8, 12
+    sts = []
+    for k in range(nrep):
+        st = lattice_state(n, 1.0, seed=200 + k, density=rho)
+        if k % 2:
+            st.x[:, 0] *= 0.6
+            st.xu = st.x.copy()
+        sts.append(st)
+    ref = [Oracle.from_state(st, 1.0, 2.0).forces() for st in sts]
+    for prec, tol, tol_sum in ((0, 1e-12, 1e-11), (1, 1e-5, 1e-5)):
+        p = default_params(n, T=1.0, f0=2.0, shuffle=0, precision=prec, density=rho)
+        e = Engine([p] * nrep)
+        for k, st in enumerate(sts):
+            e.set_state(k, st)
+        e.compute_forces()
+        for k in range(nrep):
+            Fo, pe, vir, _ = ref[k]
+            err = force_err(e.get_state(k)[3], Fo)
+            assert err <= tol, (prec, k, err)
+            th = e.thermo(k)
+            assert rel(th["pe"], pe) <= tol_sum and rel(th["virial"], vir) <= tol_sum, (prec, k)
+        e.close()
+
+
 def test_batch_members_identical_to_alone(cuda_lib, g1000, g4000):
     from activechi4_b200 import Engine, default_params, lattice_state
     st3 = lattice_state(2000, 0.6, seed=9)
